@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""Benchmark: N=5 10-eigenpair shift-and-invert Lanczos solve on one B200
+(mixed precision form vs plain FP64), one JSON line on stdout.
+
+A step is one complete solve of the 10 smallest eigenpairs of the
+null-space-free reduced Maxwell operator at N=5 (NF = 10^6 modes,
+2*NF = 2e6 complex unknowns; golden-ratio cut matrix, eps = 1 + 12 prod
+(1+cos x_d)/2, q = (0.05,0.04,0.03); Krylov block 40, outer tol 1e-8, inner
+Mhat PCG tol 1e-10).  Setup (mass/basis/operator handles) is outside the
+timed region, as in the reference's timing.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fame|reference]
+
+Multi-GPU runs are replicas (independent solves, one per rank, no data-path
+collective); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "null--space-free-6d-projection-method_b200")
+for p in (ROOT, PKG):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+METRIC = "N=5 10-eigenpair solve s & Yee pts/s, mixed vs FP64 on 1 B200 at 1e-8 resid"
+N_BENCH = 5
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["fame", "reference"], default="fame")
+    ap.add_argument("--N", type=int, default=N_BENCH)
+    return ap.parse_args()
+
+
+def workload_config(N):
+    return {
+        "workload": "N=%d null-space-free Maxwell, NF=%d, 2NF=%d complex unknowns, 10 smallest "
+                    "eigenpairs, shift 0, Krylov block 40, outer tol 1e-8, inner Mhat PCG tol 1e-10"
+                    % (N, (2 * N) ** 6, 2 * (2 * N) ** 6),
+        "material": "eps = 1 + 12*prod_d (1+cos x_d)/2",
+        "cut_matrix": "[I3; diag(phi, 1/phi, phi^2)]",
+        "q": [0.05, 0.04, 0.03],
+        "form": "mixed: complex64 mass + FP32 PCG inside FP64 refinement; FP64 Lanczos",
+        "l2": "Krylov basis (1.28 GB) larger than L2, plus a 256 MB L2 flush between steps",
+        "setup": "excluded (mass/basis/operator handles built before timing)",
+    }
+
+
+# --------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.strip().split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if "Active" in v and "Not" not in v:
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kind):
+    """Per-launch DRAM bytes of the dominant chain from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "mhat_chain_traffic.json")) as f:
+            return json.load(f).get(kind)
+    except Exception:
+        return None
+
+
+# ----------------------------------------------------------------- fame arm
+def run_fame(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import fame_b200 as F
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=600))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    N = args.N
+    NF = (2 * N) ** 6
+    cfg = F.configs
+    S = cfg.SOLVE
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- setup (untimed)
+    E = cfg.material_separable_cos(N, 12.0, device=dev)
+    mass = F.MassBackend(E, N)
+    sysq = F.build_q_system(mass, cfg.P_GOLDEN, cfg.Q_BASELINE)
+    v0 = F.start_vector(cfg.SEED, sysq.nr)
+    ops = {}
+    for prec in ("mixed", "fp64"):
+        ops[prec] = F.make_explicit_krinv_compact(sysq, S["tolCG"], S["maxitCG"], precision=prec)[0]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def solve(prec):
+        return F.Lanczos(ops[prec], None, None, sysq.nr, S["nev"], S["tol"], S["maxRestart"],
+                         S["p"], v0)
+
+    def timed_steps(prec, steps):
+        times, launches = [], 0
+        res = None
+        for _ in range(steps):
+            flush.zero_()
+            barrier()
+            l0 = F.kernel_launches()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            res = solve(prec)
+            e1.record()
+            barrier()
+            launches += F.kernel_launches() - l0
+            times.append(e0.elapsed_time(e1) / 1e3)
+        return times, launches, res
+
+    for _ in range(max(args.warmup, 0)):
+        solve("mixed")
+    solve("fp64")
+    barrier()
+
+    sampler = ClockSampler(dev.index)
+    sampler.start()
+    t_mixed, launches, res_mixed = timed_steps("mixed", args.steps)
+    clocks = sampler.stop()
+    step_s = max_over_ranks(sum(t_mixed) / len(t_mixed))
+    t_fp64, _, res_fp64 = timed_steps("fp64", 1)
+    fp64_s = max_over_ranks(t_fp64[0])
+
+    lam_m = np.sort(1.0 / res_mixed[1])
+    lam_d = np.sort(1.0 / res_fp64[1])
+    lam_err = float(np.max(np.abs(lam_m - lam_d) / np.abs(lam_d)))
+
+    # ---- dominant kernel chain: Mhat (3 fields through passes A/B/C)
+    def chain_time(dtype, reps=40):
+        x = torch.randn(NF, dtype=dtype, device=dev)
+        for _ in range(5):
+            F.apply_Mhat_C_scalar_compact(x, sysq)
+        torch.cuda.synchronize()
+        s = torch.cuda.current_stream()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(reps):
+            F.apply_Mhat_C_scalar_compact(x, sysq)
+        e1.record(s)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / reps
+
+    peak, peak_kind = measured_peaks()
+    bytes32 = 156.0 * NF  # algorithmic bytes per FP32 Mhat chain (3 passes, 3 fields)
+    bytes64 = 312.0 * NF
+    t32 = chain_time(torch.complex64)
+    t64 = chain_time(torch.complex128)
+    ach32 = bytes32 / t32 / 1e9
+    ach64 = bytes64 / t64 / 1e9
+
+    # ---- end to end through the public API from host buffers
+    e2e = None
+    if rank == 0 or world > 1:
+        E_h = E.cpu().pin_memory()
+        v0_h = v0.cpu().pin_memory()
+        torch.cuda.synchronize()
+        reps = max(1, min(args.steps, 2))
+        tot = 0.0
+        for _ in range(reps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            Ed = E_h.to(dev, non_blocking=True)
+            vd = v0_h.to(dev, non_blocking=True)
+            m2 = F.MassBackend(Ed, N)
+            s2 = F.build_q_system(m2, cfg.P_GOLDEN, cfg.Q_BASELINE)
+            op2, _ = F.make_explicit_krinv_compact(s2, S["tolCG"], S["maxitCG"], precision="mixed")
+            Y, theta, _, _ = F.Lanczos(op2, None, None, s2.nr, S["nev"], S["tol"], S["maxRestart"],
+                                       S["p"], vd)
+            Yh = Y.cpu()
+            torch.cuda.synchronize()
+            tot += time.perf_counter() - t0
+            del op2, s2, m2
+        h2d = E_h.numel() * 8 + v0_h.numel() * 16
+        d2h = Yh.numel() * 16 + 8 * len(theta)
+        e2e = {"value": max_over_ranks(tot / reps), "unit": "s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h,
+               "includes": "H2D of eps and v0 from pinned memory, setup, solve, D2H of 10 eigenpairs"}
+
+    # ---- CPU baseline (rank 0, N=1 only)
+    cpu = None
+    if rank == 0 and world == 1:
+        cpu = cpu_baseline(N, steps_in_solve=res_mixed[3]["steps"])
+
+    if world > 1:
+        dist.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(step_s, 6), "unit": "s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_s * 1e3, 3),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c64/f32 mass+PCG, f64 refinement+Lanczos", "data": "synthetic",
+            "config": workload_config(N),
+            "fp64_solve_s": round(fp64_s, 6), "mixed_speedup_vs_fp64": round(fp64_s / step_s, 3),
+            "eig_rel_err_mixed_vs_fp64": lam_err,
+            "lanczos_steps": res_mixed[3]["steps"], "converged": res_mixed[3]["converged"],
+            "solves_per_s_all_gpus": round(world / step_s, 4),
+            "yee_pts_per_s": None,
+            "roofline": {"bound": "hbm", "achieved": round(ach32, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(ach32 / peak, 4), "traffic": ncu_traffic("fp32"),
+                         "kernel": "Mhat chain FP32 (passes A/B/C, 3 fields), %.1f us/launch" % (t32 * 1e6),
+                         "algorithmic_bytes": bytes32, "peak_source": peak_kind,
+                         "fp64_chain": {"achieved": round(ach64, 1), "frac": round(ach64 / peak, 4),
+                                        "us": round(t64 * 1e6, 2), "algorithmic_bytes": bytes64,
+                                        "traffic": ncu_traffic("fp64")}},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    del ops
+    if world > 1:
+        dist.destroy_process_group()
+
+
+# ------------------------------------------------------------ CPU reference
+def cpu_baseline(N, steps_in_solve=40, kind="port"):
+    """Time one explicit K_r^{-1} action of the FP64 oracle on the host cores and
+    extrapolate to a full solve (steps_in_solve actions)."""
+    import numpy as np
+    import oracle as O
+    cores = os.cpu_count() or 1
+    O.set_fft_workers(cores)
+    try:
+        import threadpoolctl  # noqa: F401
+    except ImportError:
+        pass
+    E = O.material_separable_cos(N, 12.0)
+    from fame_b200 import configs as cfg
+    S = O.build_q_system(N, cfg.P_GOLDEN, cfg.Q_BASELINE, E)
+    op, stats = O.make_explicit_krinv_compact(S, 1e-10, 3000)
+    v0 = O.start_vector(cfg.SEED, S.nr)
+    v0 = v0 / np.linalg.norm(v0)
+    t0 = time.perf_counter()
+    op(v0)
+    dt = time.perf_counter() - t0
+    return {"value": round(dt * steps_in_solve, 3), "unit": "s", "cores": cores, "kind": kind,
+            "sample": "one explicit K_r^{-1} action at N=%d (FP64 NumPy/pocketfft oracle, %d threads, "
+                      "%d Mhat PCG iterations, %.2f s) x %d Lanczos steps of the solve"
+                      % (N, cores, stats()["totalMhatIterations"], dt, steps_in_solve)}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    N = args.N
+    vals = []
+    cb = None
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(N)
+        if i >= args.warmup:
+            vals.append(cb["value"])
+    v = sum(vals) / len(vals)
+    cb["value"] = round(v, 3)
+    line = {
+        "metric": METRIC, "value": round(v, 3), "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(v * 1e3, 1), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(N), "impl": "reference", "cpu_baseline": cb,
+        "e2e": {"value": round(v, 3), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "MATLAB/Octave are not installed; the reference path is the NumPy FP64 restatement "
+                "of the reference algorithm (oracle), timed on the host cores",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_fame(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,147 @@
+// Context, status and error plumbing of the C ABI; the shared start-vector
+// generator.
+#include <atomic>
+#include <cstring>
+#include <string>
+#include "internal.cuh"
+
+namespace fame {
+
+static thread_local std::string g_last_error;
+static std::atomic<long long> g_launches{0};
+
+void count_launch(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+void set_last_error(int code, const std::string& msg) {
+  g_last_error = std::string(fame_status_string(code)) + ": " + msg;
+}
+
+int fail(int code, const std::string& msg) {
+  set_last_error(code, msg);
+  return code;
+}
+
+int dalloc(void** p, size_t bytes) {
+  *p = nullptr;
+  if (bytes == 0) return FAME_OK;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return fail(e == cudaErrorMemoryAllocation ? FAME_ERR_OOM : FAME_ERR_CUDA,
+                std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+  }
+  return FAME_OK;
+}
+
+void dfree(void* p) {
+  if (p) cudaFree(p);
+}
+
+int read_back(fame_ctx* ctx, const void* dsrc, void* hdst, size_t bytes) {
+  if (bytes > 4096) return fail(FAME_ERR_INVALID, "read_back larger than staging area");
+  FAME_CUDA_TRY(cudaMemcpyAsync(ctx->pinned, dsrc, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  FAME_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  std::memcpy(hdst, ctx->pinned, bytes);
+  return FAME_OK;
+}
+
+// splitmix64 over the counter; shared with the oracle's start_vector.
+__global__ void k_start_vector(unsigned long long seed, long long n, double2* v) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double u[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      unsigned long long c = 2ull * (unsigned long long)i + h;
+      unsigned long long z = seed + (c + 1ull) * 0x9E3779B97F4A7C15ull;
+      z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+      z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+      z = z ^ (z >> 31);
+      u[h] = 2.0 * ((double)(z >> 11) * 0x1.0p-53) - 1.0;
+    }
+    v[i] = make_double2(u[0], u[1]);
+  }
+}
+
+}  // namespace fame
+
+using namespace fame;
+
+extern "C" {
+
+const char* fame_status_string(int s) {
+  switch (s) {
+    case FAME_OK: return "FAME_OK";
+    case FAME_ERR_INVALID: return "FAME_ERR_INVALID";
+    case FAME_ERR_CUDA: return "FAME_ERR_CUDA";
+    case FAME_ERR_OOM: return "FAME_ERR_OOM";
+    case FAME_ERR_NOT_CONVERGED: return "FAME_ERR_NOT_CONVERGED";
+    case FAME_ERR_NONFINITE: return "FAME_ERR_NONFINITE";
+    case FAME_ERR_BUDGET: return "FAME_ERR_BUDGET";
+    case FAME_ERR_SINGULAR: return "FAME_ERR_SINGULAR";
+    case FAME_ERR_UNSUPPORTED: return "FAME_ERR_UNSUPPORTED";
+    case FAME_ERR_BREAKDOWN: return "FAME_ERR_BREAKDOWN";
+    default: return "FAME_ERR_UNKNOWN";
+  }
+}
+
+const char* fame_last_error(void) { return g_last_error.c_str(); }
+
+int fame_version(void) { return 100; }
+
+long long fame_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int fame_ctx_create(int device, fame_ctx** out) {
+  if (!out) return fail(FAME_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  int count = 0;
+  FAME_CUDA_TRY(cudaGetDeviceCount(&count));
+  if (device < 0 || device >= count) return fail(FAME_ERR_INVALID, "bad device index");
+  FAME_CUDA_TRY(cudaSetDevice(device));
+  fame_ctx* c = new fame_ctx();
+  c->device = device;
+  if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaMallocHost(&c->pinned, 4096) != cudaSuccess) {
+    cudaGetLastError();
+    delete c;
+    return fail(FAME_ERR_CUDA, "context resources");
+  }
+  c->stream = c->own;
+  *out = c;
+  return FAME_OK;
+}
+
+int fame_ctx_destroy(fame_ctx* c) {
+  if (!c) return FAME_OK;
+  cudaStreamSynchronize(c->stream);
+  if (c->pinned) cudaFreeHost(c->pinned);
+  if (c->ev) cudaEventDestroy(c->ev);
+  if (c->own) cudaStreamDestroy(c->own);
+  delete c;
+  return FAME_OK;
+}
+
+int fame_ctx_set_stream(fame_ctx* c, void* stream) {
+  if (!c) return fail(FAME_ERR_INVALID, "ctx is NULL");
+  c->stream = stream ? (cudaStream_t)stream : c->own;
+  return FAME_OK;
+}
+
+int fame_ctx_sync(fame_ctx* c) {
+  if (!c) return fail(FAME_ERR_INVALID, "ctx is NULL");
+  FAME_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return FAME_OK;
+}
+
+int fame_start_vector(fame_ctx* c, unsigned long long seed, long long n, void* v) {
+  if (!c || !v || n <= 0) return fail(FAME_ERR_INVALID, "fame_start_vector arguments");
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 16);
+  k_start_vector<<<blocks, 256, 0, c->stream>>>(seed, n, (double2*)v);
+  ::fame::count_launch();
+  FAME_CUDA_TRY(cudaGetLastError());
+  return FAME_OK;
+}
+
+}  // extern "C"

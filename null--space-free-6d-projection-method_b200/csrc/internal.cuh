@@ -1,0 +1,43 @@
+// Internal handle layouts behind the opaque C ABI types.
+#pragma once
+#include <vector>
+#include "fame_common.cuh"
+
+struct fame_ctx {
+  int device = 0;
+  cudaStream_t own = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev = nullptr;
+  void* pinned = nullptr;  // small host staging area (4 KB)
+  std::vector<void*> allocs;
+};
+
+struct fame_mass {
+  fame_ctx* ctx = nullptr;
+  int N = 0, n = 0;
+  long long NF = 0;
+  double* Es64 = nullptr;  // E / NF, FP64
+  float* Es32 = nullptr;   // E / NF, FP32
+};
+
+struct fame_basis {
+  fame_ctx* ctx = nullptr;
+  int N = 0, n = 0;
+  long long NF = 0;
+  double2 *V[6] = {nullptr};  // V11,V21,V31,V12,V22,V32
+  double2 *det = nullptr, *W1 = nullptr, *W2 = nullptr;
+  double *invC = nullptr, *Qq = nullptr, *q[3] = {nullptr};
+  float2 *W1f = nullptr, *W2f = nullptr;
+  float* invCf = nullptr;
+  void* work = nullptr;  // scratch of fame_apply_Mhat_C_scalar_compact (3 fields)
+  size_t work_bytes = 0;
+  fame_basis_info info{};
+};
+
+namespace fame {
+// device allocation helpers recorded for cleanup by the owner
+int dalloc(void** p, size_t bytes);
+void dfree(void* p);
+// copy a small device struct to host (synchronises the stream)
+int read_back(fame_ctx* ctx, const void* dsrc, void* hdst, size_t bytes);
+}  // namespace fame

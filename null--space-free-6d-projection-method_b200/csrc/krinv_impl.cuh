@@ -1,0 +1,141 @@
+// fame_krinv layout and helpers shared by krinv.cu, nested.cu and lanczos.cu.
+#pragma once
+#include "internal.cuh"
+#include "krylov.cuh"
+
+namespace fame {
+
+template <typename T> struct PcgBuf {
+  C<T>* work = nullptr;  // 3 fields of NF (mass chain)
+  C<T>* x = nullptr;
+  C<T>* r = nullptr;
+  C<T>* p = nullptr;
+  C<T>* Ap = nullptr;
+};
+
+// Outer (K_r) PCG state of the nested realisation.
+struct OuterState {
+  double rho, rho1, beta, pq_re, pq_im, alpha_re, alpha_im, rr, bnorm2, tolb2;
+  int iter, pad;
+};
+
+}  // namespace fame
+
+struct fame_krinv {
+  fame_basis* b = nullptr;
+  fame_mass* m = nullptr;
+  fame_ctx* ctx = nullptr;
+  fame_krinv_opts o{};
+  fame_krinv_stats stats{};
+  long long NF = 0;
+  int n = 0;
+  fame::PcgBuf<double> b64;
+  fame::PcgBuf<float> b32;
+  double2 *mr1 = nullptr, *mr2 = nullptr, *bhat = nullptr;
+  double* partials = nullptr;
+  unsigned* counter = nullptr;
+  fame::PcgState *st64 = nullptr, *st32 = nullptr;
+  int lastIt64 = 0, lastIt32 = 0;
+  // nested (method B) outer vectors, 2NF each
+  double2 *ox = nullptr, *orr = nullptr, *oz = nullptr, *op = nullptr, *oq = nullptr;
+  double* sigma = nullptr;  // |q|^2 (NF), sigma_r = [sigma; sigma]
+  fame::OuterState* ost = nullptr;
+};
+
+namespace fame {
+int nested_alloc(fame_krinv* K);
+void nested_free(fame_krinv* K);
+int krinv_nested_apply_one(fame_krinv* K, const double2* b, double2* x);
+template <typename T> MhatCoef<T> coef_of(fame_basis* b);
+template <typename T> const T* es_of(fame_mass* m);
+}  // namespace fame
+
+namespace fame {
+
+// Operator tags for the generic PCG driver: each launches one PCG matvec
+// chain (search-direction update fused in front, p^H A p reduction behind)
+// and one true-residual chain r = b - A x.
+template <typename T> struct OpMhat {
+  MhatCoef<T> c;
+  const T* Es;
+  static constexpr int nvec = 1;   // vector length in units of NF
+  static constexpr int mass_per_matvec = 3;
+  int matvec(fame_krinv* K, PcgBuf<T>& B, PcgState* st, cudaStream_t s) const {
+    ProPcgMhat<T> pro{c, B.p, B.r, st};
+    EpiPcgMhat<T> epi{c, B.Ap, B.p, st, reinterpret_cast<T*>(K->partials), K->counter};
+    return run_chain<T, 3>(K->n, pro, epi, B.work, Es, (T)1, K->NF, s, Gate{&st->active});
+  }
+  int resid(fame_krinv* K, PcgBuf<T>& B, const C<T>* b, double* out, cudaStream_t s) const {
+    ProResidMhat<T, T, false> pro{c, B.x, nullptr};
+    EpiResidMhat<T> epi{c, b, B.r, out, reinterpret_cast<T*>(K->partials), K->counter};
+    return run_chain<T, 3>(K->n, pro, epi, B.work, Es, (T)1, K->NF, s);
+  }
+};
+
+template <typename T> struct OpM3 {
+  const T* Es;
+  static constexpr int nvec = 3;
+  static constexpr int mass_per_matvec = 3;
+  int matvec(fame_krinv* K, PcgBuf<T>& B, PcgState* st, cudaStream_t s) const {
+    ProPcgM3<T> pro{B.p, B.r, st, K->NF};
+    EpiPcgM3<T> epi{B.Ap, B.p, st, K->NF, reinterpret_cast<T*>(K->partials), K->counter};
+    return run_chain<T, 3>(K->n, pro, epi, B.work, Es, (T)1, K->NF, s, Gate{&st->active});
+  }
+  int resid(fame_krinv* K, PcgBuf<T>& B, const C<T>* b, double* out, cudaStream_t s) const {
+    ProResidM3<T, T, false> pro{B.x, nullptr, K->NF};
+    EpiResidM3<T> epi{b, B.r, out, K->NF, reinterpret_cast<T*>(K->partials), K->counter};
+    return run_chain<T, 3>(K->n, pro, epi, B.work, Es, (T)1, K->NF, s);
+  }
+};
+
+// Queue PCG iterations until the device state stops them; the host reads the
+// state once per chunk (the first chunk is sized from the previous solve's
+// iteration count).  With verify, convergence is confirmed on the true
+// residual as MATLAB pcg does, continuing up to three times if it fails.
+template <typename T, class Op>
+int pcg_iterate(fame_krinv* K, const Op& op, PcgBuf<T>& B, PcgState* st, int& lastIt, PcgState& h,
+                bool verify, const C<T>* b) {
+  cudaStream_t s = K->ctx->stream;
+  T* partials = reinterpret_cast<T*>(K->partials);
+  const long long nlen = (long long)Op::nvec * K->NF;
+  const int every = std::max(1, K->o.checkEvery);
+  int chunk = lastIt > 4 ? lastIt - 2 : every;
+  int queued = 0, moresteps = 0;
+  for (;;) {
+    for (int it = 0; it < chunk; ++it) {
+      FAME_TRY(op.matvec(K, B, st, s));
+      k_pcg_update<T><<<vec_blocks(nlen), 256, 0, s>>>(B.x, B.r, B.p, B.Ap, nlen, st, partials,
+                                                      K->counter);
+      ::fame::count_launch();
+    }
+    FAME_CUDA_TRY(cudaGetLastError());
+    queued += chunk;
+    FAME_TRY(read_back(K->ctx, st, &h, sizeof(PcgState)));
+    if (h.active) {
+      if (queued > h.maxit + 4 * every) return fail(FAME_ERR_CUDA, "PCG state did not stop at maxit");
+      chunk = every;
+      continue;
+    }
+    if (verify && h.conv && h.flag == 0) {
+      FAME_TRY(op.resid(K, B, b, &st->aux, s));
+      K->stats.massApplies += Op::mass_per_matvec;
+      FAME_TRY(read_back(K->ctx, st, &h, sizeof(PcgState)));
+      if (h.aux > h.tolb2) {
+        if (++moresteps < 3 && h.iter < h.maxit) {
+          k_pcg_resume<<<1, 1, 0, s>>>(st);
+          ::fame::count_launch();
+          chunk = every;
+          continue;
+        }
+        h.flag = 3;
+      }
+      h.rho = h.aux;
+    }
+    break;
+  }
+  lastIt = h.iter;
+  K->stats.massApplies += (long long)Op::mass_per_matvec * h.iter;
+  return FAME_OK;
+}
+
+}  // namespace fame

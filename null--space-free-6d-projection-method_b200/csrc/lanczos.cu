@@ -1,0 +1,494 @@
+// Restarted Lanczos (Krylov-Schur thick restart) on K_r^{-1}, restating
+// exp2/Lanczos.m:1-148 with fncB = fncBinv = I.
+//
+// Device side: the basis Q (n x p, FP64 complex) stays in HBM; each step's
+// full reorthogonalisation is classical Gram-Schmidt applied twice (three
+// times right after a restart) as two streaming kernels per pass
+// (c = Q^H w, then w -= Q c with ||w||^2 fused), replacing the reference's
+// column-by-column modified Gram-Schmidt with one host sync per dot
+// (exp2/Lanczos.m:150-155).  The projected (arrowhead + tridiagonal) matrix
+// H is diagonalised on the GPU by a one-CTA parallel cyclic Jacobi method;
+// the thick-restart update Q(:,1:k) = Q*Ukeep is a tall-skinny GEMM.
+// Host side: the restart bookkeeping (sorting, convergence count, k) of
+// exp2/Lanczos.m:92-138 on the p x p data.
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "internal.cuh"
+#include "krinv_impl.cuh"
+
+namespace fame {
+
+constexpr int kGemvThreads = 256;
+constexpr int kGemvRows = 4;  // rows per thread
+constexpr int kMaxCols = 256; // max Krylov dimension p
+
+// partial[b*m + j] = sum over this block's rows of conj(Q[row,j]) w[row]
+__global__ void __launch_bounds__(kGemvThreads) k_gemv_h(const double2* __restrict__ Q, long long ldq,
+                                                         int m, const double2* __restrict__ w, long long n,
+                                                         double2* __restrict__ partial) {
+  __shared__ double2 red[kGemvThreads / 32][kMaxCols];
+  const long long base = (long long)blockIdx.x * kGemvThreads * kGemvRows + threadIdx.x;
+  double2 wr[kGemvRows];
+#pragma unroll
+  for (int r = 0; r < kGemvRows; ++r) {
+    const long long row = base + (long long)r * kGemvThreads;
+    wr[r] = row < n ? w[row] : make_double2(0.0, 0.0);
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int j = 0; j < m; ++j) {
+    const double2* q = Q + ldq * j;
+    double sr = 0.0, si = 0.0;
+#pragma unroll
+    for (int r = 0; r < kGemvRows; ++r) {
+      const long long row = base + (long long)r * kGemvThreads;
+      if (row < n) {
+        const double2 a = q[row];
+        sr += a.x * wr[r].x + a.y * wr[r].y;
+        si += a.x * wr[r].y - a.y * wr[r].x;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sr += __shfl_xor_sync(0xffffffffu, sr, o);
+      si += __shfl_xor_sync(0xffffffffu, si, o);
+    }
+    if (lane == 0) red[wid][j] = make_double2(sr, si);
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < m; j += blockDim.x) {
+    double sr = 0.0, si = 0.0;
+    for (int w2 = 0; w2 < kGemvThreads / 32; ++w2) {
+      sr += red[w2][j].x;
+      si += red[w2][j].y;
+    }
+    partial[(long long)blockIdx.x * m + j] = make_double2(sr, si);
+  }
+}
+
+// coef[j] = sum_b partial[b*m + j] (fixed order); optionally scal[1] = Re coef[m-1]
+__global__ void k_gemv_h_reduce(const double2* partial, int nblk, int m, double2* coef, double* scal,
+                                int write_alpha) {
+  __shared__ double sr[256], si[256];
+  const int j = blockIdx.x;
+  double a = 0.0, b = 0.0;
+  for (int i = threadIdx.x; i < nblk; i += blockDim.x) {
+    const double2 v = partial[(long long)i * m + j];
+    a += v.x;
+    b += v.y;
+  }
+  sr[threadIdx.x] = a;
+  si[threadIdx.x] = b;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      sr[threadIdx.x] += sr[threadIdx.x + s];
+      si[threadIdx.x] += si[threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    coef[j] = make_double2(sr[0], si[0]);
+    if (write_alpha && j == m - 1) scal[1] = sr[0];
+  }
+}
+
+// w -= Q c ; scal[0] = ||w||^2 (fixed-order grid reduction)
+__global__ void __launch_bounds__(256) k_gemv_n_sub(const double2* __restrict__ Q, long long ldq, int m,
+                                                    const double2* __restrict__ coef, double2* w, long long n,
+                                                    double* scal, double* partials, unsigned* counter) {
+  __shared__ double2 c[kMaxCols];
+  for (int j = threadIdx.x; j < m; j += blockDim.x) c[j] = coef[j];
+  __syncthreads();
+  Red<double, 1> acc{};
+  for (long long row = blockIdx.x * (long long)blockDim.x + threadIdx.x; row < n;
+       row += (long long)gridDim.x * blockDim.x) {
+    double2 v = w[row];
+    for (int j = 0; j < m; ++j) {
+      const double2 q = Q[row + ldq * j];
+      v.x -= q.x * c[j].x - q.y * c[j].y;
+      v.y -= q.x * c[j].y + q.y * c[j].x;
+    }
+    w[row] = v;
+    acc.v[0] += v.x * v.x + v.y * v.y;
+  }
+  grid_sum_finalize<double, 1>(acc, partials, counter, [&](const Red<double, 1>& t) { scal[0] = t.v[0]; });
+}
+
+// ||x||^2 -> scal[0]
+__global__ void k_nrm2(const double2* x, long long n, double* scal, double* partials, unsigned* counter) {
+  Red<double, 1> acc{};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    acc.v[0] += cabs2<double>(x[i]);
+  grid_sum_finalize<double, 1>(acc, partials, counter, [&](const Red<double, 1>& t) { scal[0] = t.v[0]; });
+}
+
+// y = x / sqrt(scal[0])
+__global__ void k_scale_inv_sqrt(const double2* x, double2* y, long long n, const double* scal) {
+  const double s = 1.0 / sqrt(scal[0]);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    y[i] = cscale<double>(x[i], s);
+}
+
+// out(:, c0:c0+CT) = Q(:, 0:m) * U(0:m, c0:c0+CT)  (U real, column-major ldU = m)
+constexpr int kRestartCT = 8;
+__global__ void __launch_bounds__(256) k_restart_gemm(const double2* __restrict__ Q, long long ldq, int m,
+                                                      const double* __restrict__ U, int kk,
+                                                      double2* __restrict__ out, long long ldo, long long n) {
+  __shared__ double u[kMaxCols * kRestartCT];
+  const int c0 = blockIdx.y * kRestartCT;
+  const int nc = min(kRestartCT, kk - c0);
+  for (int idx = threadIdx.x; idx < m * kRestartCT; idx += blockDim.x) {
+    const int j = idx % m, c = idx / m;
+    u[c * m + j] = c < nc ? U[(long long)(c0 + c) * m + j] : 0.0;
+  }
+  __syncthreads();
+  for (long long row = blockIdx.x * (long long)blockDim.x + threadIdx.x; row < n;
+       row += (long long)gridDim.x * blockDim.x) {
+    double2 acc[kRestartCT];
+#pragma unroll
+    for (int c = 0; c < kRestartCT; ++c) acc[c] = make_double2(0.0, 0.0);
+    for (int j = 0; j < m; ++j) {
+      const double2 q = Q[row + ldq * j];
+#pragma unroll
+      for (int c = 0; c < kRestartCT; ++c) {
+        acc[c].x += q.x * u[c * m + j];
+        acc[c].y += q.y * u[c * m + j];
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < kRestartCT; ++c)
+      if (c < nc) out[row + ldo * (c0 + c)] = acc[c];
+  }
+}
+
+// One-CTA parallel cyclic Jacobi for a real symmetric m x m matrix (column-
+// major).  Round-robin pair ordering: M/2 disjoint rotations per step.
+// A and V live in shared memory when 2*M*M doubles fit, else in gA/gV.
+__global__ void __launch_bounds__(1024) k_jacobi_eig(const double* H, int m, double* evals, double* U,
+                                                     double* gA, double* gV, int use_smem, int max_sweeps) {
+  extern __shared__ double sh[];
+  const int M = m + (m & 1);
+  double* A = use_smem ? sh : gA;
+  double* V = use_smem ? sh + (size_t)M * M : gV;
+  __shared__ double cs_c[kMaxCols / 2 + 1], cs_s[kMaxCols / 2 + 1];
+  __shared__ int cs_p[kMaxCols / 2 + 1], cs_q[kMaxCols / 2 + 1];
+  __shared__ double red[2][32];
+  __shared__ int stop;
+  for (int idx = threadIdx.x; idx < M * M; idx += blockDim.x) {
+    const int i = idx % M, j = idx / M;
+    A[idx] = (i < m && j < m) ? H[i + (size_t)m * j] : 0.0;
+    V[idx] = (i == j) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  const int pairs = M / 2;
+  for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+    // convergence: off-diagonal mass relative to the total
+    double off = 0.0, tot = 0.0;
+    for (int idx = threadIdx.x; idx < M * M; idx += blockDim.x) {
+      const double a = A[idx];
+      tot += a * a;
+      if (idx % M != idx / M) off += a * a;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      off += __shfl_xor_sync(0xffffffffu, off, o);
+      tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      red[0][threadIdx.x >> 5] = off;
+      red[1][threadIdx.x >> 5] = tot;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double so = 0.0, st = 0.0;
+      for (int w = 0; w < (int)((blockDim.x + 31) / 32); ++w) {
+        so += red[0][w];
+        st += red[1][w];
+      }
+      stop = (so <= 1e-32 * st) ? 1 : 0;
+    }
+    __syncthreads();
+    if (stop) break;
+    for (int r = 0; r < M - 1; ++r) {
+      for (int k = threadIdx.x; k < pairs; k += blockDim.x) {
+        auto P = [&](int i) { return i == 0 ? 0 : ((i - 1 + r) % (M - 1)) + 1; };
+        int p = P(k), q = P(M - 1 - k);
+        if (p > q) { int t = p; p = q; q = t; }
+        const double apq = A[p + (size_t)M * q], app = A[p + (size_t)M * p], aqq = A[q + (size_t)M * q];
+        double c = 1.0, s = 0.0;
+        if (fabs(apq) > 1e-300) {
+          const double theta = (app - aqq) / (2.0 * apq);
+          double t;
+          if (fabs(theta) > 1e150) t = -0.5 / theta;
+          else t = -(theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+          c = 1.0 / sqrt(1.0 + t * t);
+          s = t * c;
+        }
+        cs_c[k] = c; cs_s[k] = s; cs_p[k] = p; cs_q[k] = q;
+      }
+      __syncthreads();
+      for (int w = threadIdx.x; w < pairs * M; w += blockDim.x) {  // rows p,q
+        const int k = w / M, j = w % M;
+        const double c = cs_c[k], s = cs_s[k];
+        const int p = cs_p[k], q = cs_q[k];
+        const double ap = A[p + (size_t)M * j], aq = A[q + (size_t)M * j];
+        A[p + (size_t)M * j] = c * ap - s * aq;
+        A[q + (size_t)M * j] = s * ap + c * aq;
+      }
+      __syncthreads();
+      for (int w = threadIdx.x; w < pairs * M; w += blockDim.x) {  // columns p,q of A and V
+        const int k = w / M, j = w % M;
+        const double c = cs_c[k], s = cs_s[k];
+        const int p = cs_p[k], q = cs_q[k];
+        const double ap = A[j + (size_t)M * p], aq = A[j + (size_t)M * q];
+        A[j + (size_t)M * p] = c * ap - s * aq;
+        A[j + (size_t)M * q] = s * ap + c * aq;
+        const double vp = V[j + (size_t)M * p], vq = V[j + (size_t)M * q];
+        V[j + (size_t)M * p] = c * vp - s * vq;
+        V[j + (size_t)M * q] = s * vp + c * vq;
+      }
+      __syncthreads();
+    }
+  }
+  for (int i = threadIdx.x; i < m; i += blockDim.x) evals[i] = A[i + (size_t)M * i];
+  for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
+    const int i = idx % m, j = idx / m;
+    U[idx] = V[i + (size_t)M * j];
+  }
+}
+
+struct LanczosWs {
+  fame_ctx* ctx = nullptr;
+  long long n = 0;
+  int p = 0;
+  double2 *Q = nullptr, *Q2 = nullptr, *w = nullptr, *v = nullptr, *coef = nullptr, *partial = nullptr;
+  double *scal = nullptr, *partials = nullptr, *H = nullptr, *evals = nullptr, *U = nullptr,
+         *Ukeep = nullptr, *gA = nullptr, *gV = nullptr;
+  unsigned* counter = nullptr;
+  double* hbuf = nullptr;  // pinned
+  int nblk = 0;
+  ~LanczosWs() {
+    if (ctx) cudaStreamSynchronize(ctx->stream);
+    dfree(Q); dfree(Q2); dfree(w); dfree(v); dfree(coef); dfree(partial); dfree(scal);
+    dfree(partials); dfree(H); dfree(evals); dfree(U); dfree(Ukeep); dfree(gA); dfree(gV);
+    dfree(counter);
+    if (hbuf) cudaFreeHost(hbuf);
+  }
+  int alloc(fame_ctx* c, long long n_, int p_) {
+    ctx = c;
+    n = n_;
+    p = p_;
+    nblk = (int)((n + kGemvThreads * kGemvRows - 1) / (kGemvThreads * kGemvRows));
+    const int M = p + 1;
+    FAME_TRY(dalloc((void**)&Q, (size_t)n * p * sizeof(double2)));
+    FAME_TRY(dalloc((void**)&Q2, (size_t)n * p * sizeof(double2)));
+    FAME_TRY(dalloc((void**)&w, n * sizeof(double2)));
+    FAME_TRY(dalloc((void**)&v, n * sizeof(double2)));
+    FAME_TRY(dalloc((void**)&coef, kMaxCols * sizeof(double2)));
+    FAME_TRY(dalloc((void**)&partial, (size_t)nblk * p * sizeof(double2)));
+    FAME_TRY(dalloc((void**)&scal, 8 * sizeof(double)));
+    FAME_TRY(dalloc((void**)&partials, 4 * kVecBlocksMax * sizeof(double)));
+    FAME_TRY(dalloc((void**)&counter, sizeof(unsigned)));
+    FAME_TRY(dalloc((void**)&H, (size_t)p * p * sizeof(double)));
+    FAME_TRY(dalloc((void**)&evals, p * sizeof(double)));
+    FAME_TRY(dalloc((void**)&U, (size_t)p * p * sizeof(double)));
+    FAME_TRY(dalloc((void**)&Ukeep, (size_t)p * p * sizeof(double)));
+    FAME_TRY(dalloc((void**)&gA, (size_t)M * M * sizeof(double)));
+    FAME_TRY(dalloc((void**)&gV, (size_t)M * M * sizeof(double)));
+    if (cudaMallocHost((void**)&hbuf, ((size_t)p * p + 4 * p + 16) * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      hbuf = nullptr;
+      return fail(FAME_ERR_OOM, "pinned host buffer for Lanczos");
+    }
+    FAME_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned), ctx->stream));
+    return FAME_OK;
+  }
+  int sync_read(const void* d, void* h, size_t bytes) {
+    FAME_CUDA_TRY(cudaMemcpyAsync(hbuf, d, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    FAME_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    std::memcpy(h, hbuf, bytes);
+    return FAME_OK;
+  }
+  // one classical Gram-Schmidt pass against Q(:,0:m); ||w||^2 -> scal[0]
+  int cgs_pass(int m, bool write_alpha) {
+    cudaStream_t s = ctx->stream;
+    k_gemv_h<<<nblk, kGemvThreads, 0, s>>>(Q, n, m, w, n, partial);
+    ::fame::count_launch();
+    k_gemv_h_reduce<<<m, 256, 0, s>>>(partial, nblk, m, coef, scal, write_alpha ? 1 : 0);
+    ::fame::count_launch();
+    k_gemv_n_sub<<<vec_blocks(n), 256, 0, s>>>(Q, n, m, coef, w, n, scal, partials, counter);
+    ::fame::count_launch();
+    FAME_CUDA_TRY(cudaGetLastError());
+    return FAME_OK;
+  }
+  int eig(int m, std::vector<double>& ev, std::vector<double>& Uh) {
+    const int M = m + (m & 1);
+    const size_t smem = 2 * (size_t)M * M * sizeof(double);
+    const bool use_smem = smem <= 200 * 1024;
+    if (use_smem && smem > 48 * 1024) {
+      FAME_CUDA_TRY(cudaFuncSetAttribute(k_jacobi_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    const int threads = std::min(1024, std::max(128, ((M / 2) * M + 31) / 32 * 32));
+    k_jacobi_eig<<<1, threads, use_smem ? smem : 0, ctx->stream>>>(H, m, evals, U, gA, gV, use_smem ? 1 : 0, 60);
+    ::fame::count_launch();
+    FAME_CUDA_TRY(cudaGetLastError());
+    ev.resize(m);
+    Uh.resize((size_t)m * m);
+    FAME_TRY(sync_read(evals, ev.data(), m * sizeof(double)));
+    FAME_TRY(sync_read(U, Uh.data(), (size_t)m * m * sizeof(double)));
+    return FAME_OK;
+  }
+  // dst(:, 0:kk) = Q(:, 0:m) * Uk (m x kk, host)
+  int combine(int m, const std::vector<double>& Uk, int kk, double2* dst, long long ldd) {
+    FAME_CUDA_TRY(cudaMemcpyAsync(Ukeep, Uk.data(), (size_t)m * kk * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    dim3 grid(std::min<long long>((n + 255) / 256, 148 * 8), (kk + kRestartCT - 1) / kRestartCT);
+    k_restart_gemm<<<grid, 256, 0, ctx->stream>>>(Q, n, m, Ukeep, kk, dst, ldd, n);
+    ::fame::count_launch();
+    FAME_CUDA_TRY(cudaGetLastError());
+    // the host vector Uk must stay alive until the copy has consumed it
+    FAME_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return FAME_OK;
+  }
+};
+
+}  // namespace fame
+
+using namespace fame;
+
+extern "C" int fame_lanczos(fame_krinv* K, int nev, double tol, int maxiter, int p, const void* v0,
+                            double* theta, void* Y, fame_lanczos_info* info) {
+  if (!K || !v0 || !theta || nev < 1 || p < nev + 1 || p > kMaxCols || maxiter < 1)
+    return fail(FAME_ERR_INVALID, "fame_lanczos arguments (need 1 <= nev < p <= 256)");
+  fame_ctx* ctx = K->ctx;
+  cudaStream_t s = ctx->stream;
+  const long long n = 2 * K->NF;
+  LanczosWs L;
+  FAME_TRY(L.alloc(ctx, n, p));
+  const double eps0 = 2.220446049250313e-16;
+  // v = v0 / sqrt(v0' v0)   (exp2/Lanczos.m:17-18)
+  k_nrm2<<<vec_blocks(n), 256, 0, s>>>((const double2*)v0, n, L.scal, L.partials, L.counter);
+  ::fame::count_launch();
+  k_scale_inv_sqrt<<<vec_blocks(n), 256, 0, s>>>((const double2*)v0, L.v, n, L.scal);
+  ::fame::count_launch();
+  FAME_CUDA_TRY(cudaGetLastError());
+
+  const int k0 = nev;
+  int k = nev;
+  std::vector<double> Alpha, Beta, d, c;
+  double beta = 0.0;
+  bool justRestarted = false;
+  int sizeV = 1, kk = 0;
+  std::vector<double> ev, Us;
+  std::vector<int> ind;
+  int mmax = 0, restarts = 0, nconv = 0;
+  double maxres = 0.0;
+  bool converged = false;
+  for (int mm = 1; mm <= maxiter; ++mm) {
+    restarts = mm;
+    for (int jj = sizeV; jj <= p; ++jj) {
+      const int j = jj - 1;
+      double2* qj = L.Q + (size_t)n * j;
+      FAME_CUDA_TRY(cudaMemcpyAsync(qj, L.v, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+      FAME_TRY(fame_krinv_apply(K, qj, L.w, 1));  // Aq = fncA(Q(:,jj))
+      // alpha = Re(Aq' Q(:,jj)) from the first pass; passes: 2, or 3 after a restart
+      FAME_TRY(L.cgs_pass(jj, true));
+      FAME_TRY(L.cgs_pass(jj, false));
+      if (justRestarted) {
+        FAME_TRY(L.cgs_pass(jj, false));
+        justRestarted = false;
+      }
+      double sc[2];
+      FAME_TRY(L.sync_read(L.scal, sc, 2 * sizeof(double)));
+      const double alpha = sc[1], beta2 = sc[0];
+      if (!(beta2 > 0.0) || std::sqrt(beta2) < 1e-14) {  // exp2/Lanczos.m:75-79
+        beta = std::sqrt(std::max(beta2, 0.0));
+        break;
+      }
+      beta = std::sqrt(beta2);
+      k_scale_inv_sqrt<<<vec_blocks(n), 256, 0, s>>>(L.w, L.v, n, L.scal);
+      ::fame::count_launch();
+      Alpha.push_back(alpha);
+      Beta.push_back(beta);
+      ++kk;
+    }
+    // H = [diag(d) c; c' T]  (exp2/Lanczos.m:92-97)
+    const int m1 = (int)Alpha.size(), kd = (int)d.size(), m = kd + m1;
+    if (m < 1) return fail(FAME_ERR_BREAKDOWN, "Lanczos breakdown before the first step");
+    std::vector<double> H((size_t)m * m, 0.0);
+    for (int i = 0; i < kd; ++i) H[i + (size_t)m * i] = d[i];
+    for (int i = 0; i < m1; ++i) {
+      H[(kd + i) + (size_t)m * (kd + i)] = Alpha[i];
+      if (i + 1 < m1) {
+        H[(kd + i) + (size_t)m * (kd + i + 1)] = Beta[i];
+        H[(kd + i + 1) + (size_t)m * (kd + i)] = Beta[i];
+      }
+    }
+    for (int i = 0; i < kd; ++i) {
+      H[i + (size_t)m * kd] = c[i];
+      H[kd + (size_t)m * i] = c[i];
+    }
+    Alpha.clear();
+    Beta.clear();
+    FAME_CUDA_TRY(cudaMemcpyAsync(L.H, H.data(), (size_t)m * m * sizeof(double), cudaMemcpyHostToDevice, s));
+    FAME_TRY(L.eig(m, ev, Us));  // synchronises: H consumed
+    mmax = m;
+    std::vector<double> res(m);
+    for (int i = 0; i < m; ++i) res[i] = std::fabs(beta * Us[(m - 1) + (size_t)m * i]);
+    ind.resize(m);
+    std::iota(ind.begin(), ind.end(), 0);
+    std::stable_sort(ind.begin(), ind.end(), [&](int a, int b) { return ev[a] > ev[b]; });
+    d.resize(m);
+    std::vector<double> rs(m);
+    for (int i = 0; i < m; ++i) {
+      d[i] = ev[ind[i]];
+      rs[i] = res[ind[i]];
+    }
+    const int nw = std::min(k0, m);
+    nconv = 0;
+    maxres = 0.0;
+    for (int i = 0; i < nw; ++i) {
+      const double thr = tol * std::max(std::pow(eps0, 2.0 / 3.0), std::fabs(d[i]));
+      if (rs[i] < thr) ++nconv;
+      maxres = std::max(maxres, rs[i]);
+    }
+    if (nconv >= k0 || mm == maxiter) {
+      converged = nconv >= k0;
+      break;
+    }
+    k = k0 + std::min(nconv, (p - k0) / 2);  // exp2/Lanczos.m:123-126
+    if (k == 1 && p > 3) k = p / 2;
+    std::vector<double> Uk((size_t)m * k);
+    c.assign(k, 0.0);
+    for (int cc = 0; cc < k; ++cc) {
+      for (int i = 0; i < m; ++i) Uk[i + (size_t)m * cc] = Us[i + (size_t)m * ind[cc]];
+      c[cc] = beta * Us[(m - 1) + (size_t)m * ind[cc]];
+    }
+    FAME_TRY(L.combine(m, Uk, k, L.Q2, n));  // Q(:,1:k) = Q*Ukeep
+    std::swap(L.Q, L.Q2);
+    d.resize(k);
+    justRestarted = true;
+    sizeV = k + 1;
+  }
+  // U = Q * Usmall(:, ind(1:k0))  (exp2/Lanczos.m:141-147)
+  const int m = mmax;
+  const int kout = std::min(k0, m);
+  for (int i = 0; i < kout; ++i) theta[i] = d[i];
+  if (Y) {
+    std::vector<double> Uk((size_t)m * kout);
+    for (int cc = 0; cc < kout; ++cc)
+      for (int i = 0; i < m; ++i) Uk[i + (size_t)m * cc] = Us[i + (size_t)m * ind[cc]];
+    FAME_TRY(L.combine(m, Uk, kout, (double2*)Y, n));
+  }
+  if (info) {
+    info->steps = kk;
+    info->restarts = restarts;
+    info->converged = converged ? 1 : 0;
+    info->nconv = nconv;
+    info->maxWantedResidual = maxres;
+  }
+  FAME_CUDA_TRY(cudaStreamSynchronize(s));
+  return FAME_OK;
+}

@@ -1,0 +1,117 @@
+// Host-side launch of one fused mass-operator chain (pass A -> B -> C) for a
+// runtime axis length n = 2N, dispatching to the compile-time kernels.
+#pragma once
+#include "fft6d.cuh"
+
+namespace fame {
+
+inline int round32(int x) { return (x + 31) / 32 * 32; }
+
+template <typename T> struct PassBTile { static constexpr int TT = 32 / (int)sizeof(C<T>) >= 1 ? 32 / (int)sizeof(C<T>) : 1; };
+
+// Set the dynamic shared-memory limit of a kernel once per process.
+template <typename K> int ensure_smem(K kernel, size_t bytes) {
+  if (bytes <= 48 * 1024) return FAME_OK;
+  FAME_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return FAME_OK;
+}
+
+template <int n, typename T, typename TE>
+int launch_passB(C<T>* work, int nfields, const TE* Es, TE escale, long long NF, cudaStream_t st, Gate gate) {
+  using Q = Cube<n>;
+  constexpr int TT = PassBTile<T>::TT;
+  static_assert(Q::n3 % TT == 0, "tile must divide n^3");
+  const size_t smem = (size_t)TT * Q::size * sizeof(C<T>);
+  static int attr = ensure_smem(k_passB<n, T, TT, TE>, smem);
+  if (attr != FAME_OK) return attr;
+  const int threads = std::min(512, std::max(64, round32(TT * Q::n2)));
+  dim3 grid(Q::n3 / TT, nfields);
+  k_passB<n, T, TT, TE><<<grid, threads, smem, st>>>(work, Es, escale, NF, gate);
+  ::fame::count_launch();
+  return FAME_OK;
+}
+
+template <int n, typename T, int F, class Pro>
+int launch_passA(const Pro& pro, C<T>* work, long long NF, cudaStream_t st, Gate gate) {
+  using Q = Cube<n>;
+  const size_t smem = (size_t)F * Q::size * sizeof(C<T>);
+  static int attr = ensure_smem(k_passA<n, T, F, Pro>, smem);
+  if (attr != FAME_OK) return attr;
+  const int threads = std::min(512, std::max(128, round32(F * Q::n2)));
+  k_passA<n, T, F, Pro><<<Q::n3, threads, smem, st>>>(pro, work, NF, gate);
+  ::fame::count_launch();
+  return FAME_OK;
+}
+
+template <int n, typename T, int F, class Epi>
+int launch_passC(const Epi& epi, const C<T>* work, long long NF, cudaStream_t st, Gate gate) {
+  using Q = Cube<n>;
+  const size_t smem = (size_t)F * Q::size * sizeof(C<T>);
+  static int attr = ensure_smem(k_passC<n, T, F, Epi>, smem);
+  if (attr != FAME_OK) return attr;
+  const int threads = std::min(512, std::max(128, round32(F * Q::n2)));
+  k_passC<n, T, F, Epi><<<Q::n3, threads, smem, st>>>(epi, work, NF, gate);
+  ::fame::count_launch();
+  return FAME_OK;
+}
+
+// Number of CTAs pass C launches (size of the reduction partials it needs).
+inline long long passC_blocks(int n) { return (long long)n * n * n; }
+
+template <int n, typename T, int F, class Pro, class Epi, typename TE>
+int chain_n(const Pro& pro, const Epi& epi, C<T>* work, const TE* Es, TE escale, long long NF,
+            cudaStream_t st, Gate gate) {
+  FAME_TRY((launch_passA<n, T, F, Pro>(pro, work, NF, st, gate)));
+  FAME_TRY((launch_passB<n, T, TE>(work, F, Es, escale, NF, st, gate)));
+  FAME_TRY((launch_passC<n, T, F, Epi>(epi, work, NF, st, gate)));
+  FAME_CUDA_TRY(cudaGetLastError());
+  return FAME_OK;
+}
+
+// y-chain for axis length n in {2,4,...,14}.  work holds F fields of NF.
+template <typename T, int F, class Pro, class Epi, typename TE>
+int run_chain(int n, const Pro& pro, const Epi& epi, C<T>* work, const TE* Es, TE escale,
+              long long NF, cudaStream_t st, Gate gate = Gate{nullptr}) {
+  switch (n) {
+    case 2: return chain_n<2, T, F>(pro, epi, work, Es, escale, NF, st, gate);
+    case 4: return chain_n<4, T, F>(pro, epi, work, Es, escale, NF, st, gate);
+    case 6: return chain_n<6, T, F>(pro, epi, work, Es, escale, NF, st, gate);
+    case 8: return chain_n<8, T, F>(pro, epi, work, Es, escale, NF, st, gate);
+    case 10: return chain_n<10, T, F>(pro, epi, work, Es, escale, NF, st, gate);
+    case 12: return chain_n<12, T, F>(pro, epi, work, Es, escale, NF, st, gate);
+    case 14: return chain_n<14, T, F>(pro, epi, work, Es, escale, NF, st, gate);
+    default: return fail(FAME_ERR_UNSUPPORTED, "mass operator supports 2N in {2,4,...,14}");
+  }
+}
+
+// ------------------------------------------------------------ functors
+// Identity prologue/epilogue (plain mass action): F independent columns.
+template <typename T, int F> struct ProCols {
+  const C<T>* x[F];
+  __device__ __forceinline__ void load(long long i, C<T>* v) const {
+#pragma unroll
+    for (int f = 0; f < F; ++f) v[f] = x[f][i];
+  }
+};
+template <typename T, int F> struct EpiCols {
+  using Acc = T;
+  static constexpr int K = 0;
+  C<T>* y[F];
+  T* partials = nullptr;
+  unsigned* counter = nullptr;
+  __device__ __forceinline__ void store(long long i, const C<T>* v, Red<T, 1>&) const {
+#pragma unroll
+    for (int f = 0; f < F; ++f) y[f][i] = v[f];
+  }
+  __device__ __forceinline__ void finalize(const Red<T, 1>&) const {}
+};
+
+// Coefficients of the orthogonalised inner operator
+// (exp1/build_experiment1_q_system_C_compact.m:21-31).
+template <typename T> struct MhatCoef {
+  const T* invC;
+  const C<T>* W1;
+  const C<T>* W2;
+};
+
+}  // namespace fame

@@ -1,0 +1,72 @@
+"""CPU tests of the C-ABI library: it loads, exports every declared symbol, and
+its host-only entry points behave (no GPU needed)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "fame.h")
+
+
+def _declared():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"^FAME_API\s+(?:int|long long|const char\*)\s+(fame_\w+)\(", txt, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    from fame_b200 import _lib
+    lib = C.CDLL(_lib.LIB_PATH)
+    names = _declared()
+    assert len(names) >= 30
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_signatures_cover_header():
+    from fame_b200 import _lib
+    names = set(_declared())
+    bound = set(_lib.SIGNATURES) | {"fame_status_string", "fame_last_error", "fame_kernel_launches"}
+    assert names <= bound, names - bound
+
+
+def test_status_strings_and_default_opts():
+    from fame_b200 import _lib
+    L = _lib.lib
+    assert L.fame_status_string(0) == b"FAME_OK"
+    assert L.fame_status_string(7) == b"FAME_ERR_SINGULAR"
+    o = _lib.fame_krinv_opts()
+    assert L.fame_krinv_default_opts(C.byref(o)) == 0
+    assert o.tolCG == 1e-10 and o.maxitCG == 1200 and o.tolM == 1e-12 and o.maxitKr == 600
+    assert o.epsC == 4.0 and o.useKrPreconditioner == 1
+    assert L.fame_version() >= 100
+
+
+def test_null_arguments_are_rejected_without_gpu():
+    from fame_b200 import _lib
+    L = _lib.lib
+    assert L.fame_krinv_default_opts(None) == 1
+    assert L.fame_mass_apply(None, 0, None, None, 1, 0) == 1
+    assert b"FAME_ERR_INVALID" in L.fame_last_error()
+    assert L.fame_krinv_apply(None, None, None, 1) == 1
+    assert L.fame_basis_get(None, 0, None) == 1
+
+
+def test_struct_layouts_match_header():
+    from fame_b200 import _lib
+    # field counts mirror include/fame.h
+    assert len(_lib.fame_krinv_opts._fields_) == 14
+    assert len(_lib.fame_krinv_stats._fields_) == 10
+    assert C.sizeof(_lib.fame_basis_info) == 8 + 4 + 4 + 8 + 8 + 48
+
+
+def test_twiddle_header_is_generated_and_exact():
+    import importlib.util
+    import math
+    pkg = os.path.join(ROOT, "null--space-free-6d-projection-method_b200", "csrc")
+    txt = open(os.path.join(pkg, "twiddles.cuh")).read()
+    vals = dict(re.findall(r"case (\d+): return ([-0-9.e]+);", txt.split("tw_sin")[0]))
+    assert float(vals[str(5 * 16 + 1)]) == math.cos(2 * math.pi / 5) or \
+        abs(float(vals[str(5 * 16 + 1)]) - math.cos(2 * math.pi / 5)) < 1e-16
+    assert float(vals[str(3 * 16 + 1)]) == -0.5

@@ -1,0 +1,106 @@
+"""GPU parity: K_r^{-1} realisations and the Lanczos eigensolver vs the oracle."""
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
+
+
+def _systems(N, Pname, q, material, cuda_device):
+    import fame_b200 as F
+    Pm = F.configs.P_GOLDEN if Pname == "golden" else F.configs.P_REFERENCE
+    if material == "exp":
+        E = O.material_smooth_exp(N)
+    else:
+        E = O.material_separable_cos(N, 12.0)
+    S = O.build_q_system(N, Pm, q, E)
+    m = F.MassBackend(torch.as_tensor(E, device=cuda_device), N)
+    return S, F.build_q_system(m, Pm, q)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_explicit_krinv_matches_oracle(cuda_device, precision):
+    import fame_b200 as F
+    S, sg = _systems(2, "reference", (0.13, 0.21, 0.17), "exp", cuda_device)
+    rng = np.random.default_rng(5)
+    b = rng.standard_normal(S.nr) + 1j * rng.standard_normal(S.nr)
+    op_ref, _ = O.make_explicit_krinv_compact(S, 1e-12, 3000)
+    y_ref = op_ref(b)
+    op, stats = F.make_explicit_krinv_compact(sg, 1e-12, 3000, precision=precision)
+    y = op(torch.as_tensor(b, device=cuda_device)).cpu().numpy()
+    assert _rel(y, y_ref) < 1e-10
+    st = stats()
+    assert st.inverseCalls == 1 and st.totalIterations > 0
+    if precision == "mixed":
+        assert st.refineSteps >= 1 and st.fp32Iterations > 0
+
+
+def test_nested_krinv_matches_explicit(cuda_device):
+    import fame_b200 as F
+    S, sg = _systems(1, "golden", (0.05, 0.04, 0.03), "cos", cuda_device)
+    rng = np.random.default_rng(6)
+    b = rng.standard_normal(S.nr) + 1j * rng.standard_normal(S.nr)
+    op_ref, _ = O.make_nested_krinv_instrumented(S, 4.0, 1e-10, 1e-12)
+    y_ref = op_ref(b)
+    for precision in ("fp64", "mixed"):
+        op, stats = F.make_nested_krinv_instrumented(sg, 4.0, 1e-10, 1e-12, precision=precision)
+        y = op(torch.as_tensor(b, device=cuda_device)).cpu().numpy()
+        assert _rel(y, y_ref) < 1e-8, precision
+        assert stats().massSolveCalls > 0
+
+
+def test_krinv_rejects_nonfinite_input(cuda_device):
+    import fame_b200 as F
+    S, sg = _systems(1, "golden", (0.05, 0.04, 0.03), "cos", cuda_device)
+    op, _ = F.make_explicit_krinv_compact(sg)
+    b = torch.ones(S.nr, dtype=torch.complex128, device=cuda_device)
+    b[3] = float("nan")
+    with pytest.raises(F.FameError) as e:
+        op(b)
+    assert e.value.status == 5  # FAME_ERR_NONFINITE
+    y = op(torch.ones(S.nr, dtype=torch.complex128, device=cuda_device))  # still usable
+    assert torch.isfinite(y).all()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_lanczos_reference_kat_n2(cuda_device, precision):
+    """Reference known answer: tracked modes 1 and 10 at N=2
+    (exp3/make_config_experiment4.m:38-45, checked at rel 5e-7)."""
+    import fame_b200 as F
+    S, sg = _systems(2, "reference", (0.13, 0.21, 0.17), "exp", cuda_device)
+    op, _ = F.make_explicit_krinv_compact(sg, 1e-10, 3000, precision=precision)
+    v0 = F.start_vector(F.configs.SEED, sg.nr)
+    Y, theta, steps, info = F.Lanczos(op, None, None, sg.nr, 10, 1e-10, 30, 40, v0)
+    lam = np.sort(1.0 / theta)
+    ref = np.array(F.configs.KAT_N2_LAMBDA)
+    assert info["converged"]
+    assert np.max(np.abs(lam[[0, 9]] - ref) / ref) < 5e-7
+    sol = O.solve_modes(S, nev=10, p=40, tol=1e-10, maxRestart=30, tolCG=1e-10)
+    assert np.max(np.abs(lam - sol["lam"]) / sol["lam"]) < 1e-10
+
+
+def test_lanczos_baseline_n3_fp64_and_mixed(cuda_device):
+    """The N=3 BASELINE workload (golden-ratio P, separable-cos material): eigenvalues of
+    the plain FP64 and mixed forms within 1e-10 of the FP64 oracle."""
+    import fame_b200 as F
+    N = 3
+    S, sg = _systems(N, "golden", F.configs.Q_BASELINE, "cos", cuda_device)
+    sol = O.solve_modes(S, nev=10, p=40, tol=1e-10, maxRestart=30, tolCG=1e-12)
+    v0 = F.start_vector(F.configs.SEED, sg.nr)
+    for precision in ("fp64", "mixed"):
+        op, _ = F.make_explicit_krinv_compact(sg, 1e-10, 3000, precision=precision)
+        Y, theta, steps, info = F.Lanczos(op, None, None, sg.nr, 10, 1e-8, 30, 40, v0)
+        lam = np.sort(1.0 / theta)
+        assert info["converged"], precision
+        assert np.max(np.abs(lam - sol["lam"]) / sol["lam"]) < 1e-10, precision
+        # Ritz vectors: residual of K_r^{-1} y = theta y
+        j = int(np.argmax(theta))
+        y = Y[:, j]
+        r = op(y) - theta[j] * y
+        assert float(torch.linalg.norm(r) / (abs(theta[j]) * torch.linalg.norm(y))) < 1e-6

@@ -1,0 +1,151 @@
+"""CPU tests: pin the oracle against the reference's known answers and constants."""
+import numpy as np
+import pytest
+
+import oracle as O
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+P_REF = np.vstack([np.eye(3), np.diag([np.sqrt(2), np.sqrt(3), np.sqrt(5)])])
+PHI = (1 + 5 ** 0.5) / 2
+P_GOLD = np.vstack([np.eye(3), np.diag([PHI, 1 / PHI, PHI ** 2])])
+
+
+def test_rank1_plan_constants_n5():
+    """exp2/run_experiment2_allgpu_static_check.m:10-11 — M = 24760990, z = 19^(0..5)."""
+    p = O.build_radix_exact_rank1_plan_scalar(5)
+    assert p["M"] == 24760990
+    assert list(p["z"]) == [1, 19, 361, 6859, 130321, 2476099]
+    assert len(np.unique(p["inputIdx"])) == p["NF"]
+    assert len(np.unique(p["targetIdx"])) == p["NF"]
+    assert p["inputIdx"].max() < p["M"]
+
+
+@pytest.mark.parametrize("N", [1, 2])
+def test_rank1_lattice_equals_6d_fft(N):
+    """exp1/smoke_test_rank1_lowmem.m:17-23: rank-1 lowmem vs tensor FFT mass < 1e-11."""
+    E = O.material_smooth_exp(N)
+    plan = O.build_radix_exact_rank1_plan_scalar(N)
+    k = O.build_exact_rank1_scalar_kernel_fft(E, plan)
+    x = O.start_vector(3, (2 * N) ** 6)
+    assert _rel(O.applyMij_rank1_exact(x, k, plan), O.applyMij_fft(x, E, N)) < 1e-11
+
+
+@pytest.mark.parametrize("N", [2, 3])
+def test_stencil_closed_form(N):
+    E = O.material_separable_cos(N, 12.0)
+    x = O.start_vector(4, (2 * N) ** 6)
+    assert _rel(O.mass_stencil_bandlimited(x, N, 12.0), O.applyMij_fft(x, E, N)) < 1e-13
+
+
+def test_mass_hermitian_positive():
+    """exp2/run_experiment3_preflight_n5.m:17-24 (Hermitian defect), at N=2."""
+    N = 2
+    E = O.material_smooth_exp(N)
+    x, y = O.start_vector(1, 4096), O.start_vector(2, 4096)
+    Mx, My = O.applyMij_fft(x, E, N), O.applyMij_fft(y, E, N)
+    assert abs(np.vdot(y, Mx) - np.conj(np.vdot(x, My))) / abs(np.vdot(y, Mx)) < 1e-10
+    assert np.real(np.vdot(x, Mx)) > 0
+
+
+def test_basis_identities():
+    """V V^* equals the curl-curl symbol K on the transverse space; W, invC definitions."""
+    N = 1
+    S = O.build_q_system(N, P_GOLD, (0.05, 0.04, 0.03), O.material_separable_cos(N))
+    n = S.NF
+    for j in range(0, n, 7):
+        e = np.zeros(3 * n, complex)
+        e[j] = 1
+        VVe = O.apply_V_blockdiag(O.apply_VH_blockdiag(e, S), S)
+        assert _rel(VVe, S.Kop(e)) < 1e-10
+    W = O.solveV1H_blockdiag(np.concatenate([np.conj(S.V31), np.conj(S.V32)]),
+                             S.V11, S.V12, S.V21, S.V22, S.detV1, n)
+    assert _rel(W[:n], S.W1) < 1e-15
+    np.testing.assert_allclose(S.invC, 1 / np.sqrt(1 + abs(S.W1) ** 2 + abs(S.W2) ** 2))
+
+
+def test_gamma_point_raises():
+    with pytest.raises(ValueError):
+        O.build_q_system(1, P_GOLD, (0.0, 0.0, 0.0), O.material_separable_cos(1))
+
+
+def test_singular_branch_orthonormal():
+    """exp1/assemble_K_and_nullspace_free_basis.m:75-91 — q parallel to (1,1,1)."""
+    P = np.vstack([np.eye(3), np.zeros((3, 3))])
+    Xi = O.build_fourier_grid_6d(1)
+    B = O.assemble_K_and_nullspace_free_basis(P, np.array([0.1, 0.1, 0.1, 0, 0, 0]), Xi)
+    assert B["nsingular"] > 0
+
+
+def test_pcg_semantics():
+    rng = np.random.default_rng(0)
+    A = rng.standard_normal((30, 30))
+    A = A @ A.T + 30 * np.eye(30)
+    b = rng.standard_normal(30)
+    x, flag, rr, it = O.pcg(lambda v: A @ v, b, 1e-12, 100)
+    assert flag == 0 and rr <= 1e-12 and np.linalg.norm(A @ x - b) / np.linalg.norm(b) <= 1e-12
+    x, flag, rr, it = O.pcg(lambda v: A @ v, b, 1e-14, 2)
+    assert flag == 1 and it == 2
+    x, flag, rr, it = O.pcg(lambda v: A @ v, np.zeros(30), 1e-10, 10)
+    assert flag == 0 and it == 0 and not x.any()
+
+
+def test_lanczos_known_diagonal():
+    """exp1/smoke_test_rank1_lowmem.m:44-54: diag(linspace(100,1,80)), top-5 rel < 1e-7."""
+    d = np.linspace(100, 1, 80)
+    v0 = O.start_vector(5, 80)
+    U, th, it, info = O.Lanczos(lambda v: d * v, 80, 5, 1e-10, 30, 20, v0)
+    assert np.max(np.abs(th - d[:5]) / d[:5]) < 1e-7
+
+
+def test_dense_eigs_n1():
+    """Lanczos on K_r^{-1} reproduces a dense eigensolve of K_r = V^* M^{-1} V at N=1."""
+    N = 1
+    S = O.build_q_system(N, P_GOLD, (0.05, 0.04, 0.03), O.material_separable_cos(N))
+    lam_dense = np.sort(np.linalg.eigvalsh(O.dense_reduced_operator(S)))[:10]
+    sol = O.solve_modes(S, nev=10, p=40, tol=1e-10, tolCG=1e-12)
+    assert np.max(np.abs(sol["lam"] - lam_dense) / lam_dense) < 1e-10
+
+
+def test_explicit_equals_nested_n1():
+    """exp1/smoke_test_rank1_lowmem.m:29-39 spirit: two K_r^{-1} realisations agree."""
+    N = 1
+    S = O.build_q_system(N, P_REF, (0.13, 0.21, 0.17), O.material_smooth_exp(N))
+    b = O.start_vector(9, S.nr)
+    yc = O.make_explicit_krinv_compact(S, 1e-12, 3000)[0](b)
+    yb = O.make_nested_krinv_instrumented(S, 4.0, 1e-12, 1e-13)[0](b)
+    assert _rel(yb, yc) < 1e-9
+
+
+@pytest.mark.slow
+def test_reference_kat_n2():
+    """exp3/make_config_experiment4.m:38-45 — tracked modes 1, 10 at N=2 (rel 5e-7)."""
+    N = 2
+    S = O.build_q_system(N, P_REF, (0.13, 0.21, 0.17), O.material_smooth_exp(N, 4.0, 1.2))
+    sol = O.solve_modes(S, nev=10, p=40, tol=1e-10, maxRestart=30, tolCG=1e-10)
+    ref = np.array([1.201276300237e-02, 4.496454358674e-02])
+    assert np.max(np.abs(sol["lam"][[0, 9]] - ref) / ref) < 5e-7
+
+
+def test_taylor_matches_direct():
+    """Taylor (p=10, 8 centers) vs the direct sum at small size (exp2/check_experiment2b_results.m:72-75 e2<=1e-4)."""
+    N = 1
+    S = O.build_q_system(N, P_GOLD, (0.05, 0.04, 0.03), O.material_separable_cos(N))
+    Q = O.build_projected_q_modes(P_GOLD, S.kLift, N)
+    c = O.start_vector(11, S.NF)
+    r1, r2, r3, sz = O.build_yee_points(6, 0.0125)
+    blocks = O.build_yee_block_partition(sz, 2)
+    ud = O.reconstruct_field_direct_blocked(c, Q, r1)
+    ut = O.reconstruct_field_taylor_multi(c, Q, r1, 10, blocks)
+    assert _rel(ut, ud) < 1e-4
+    ub = O.reconstruct_component_taylor_batch(c, Q, r1, 10, blocks)[:, 0]
+    assert _rel(ub, ut) < 5e-11  # exp3/make_config_experiment4.m:95 streaming vs batched
+
+
+def test_start_vector_deterministic():
+    a = O.start_vector(20260905, 10)
+    assert np.array_equal(a, O.start_vector(20260905, 10))
+    assert np.all(np.abs(a.real) <= 1) and np.all(np.abs(a.imag) <= 1)
