@@ -201,11 +201,16 @@ def run_fame(args):
 
     sampler = ClockSampler(dev.index)
     sampler.start()
+    time.sleep(1.0)  # let the sampler's NVML start-up finish before the timed region
+    for prec in ("mixed", "fp64"):
+        ops[prec].reset_stats()
     t_mixed, launches, res_mixed = timed_steps("mixed", args.steps)
+    st_mixed = ops["mixed"].stats()
     clocks = sampler.stop()
     step_s = max_over_ranks(sum(t_mixed) / len(t_mixed))
     t_fp64, _, res_fp64 = timed_steps("fp64", 1)
     fp64_s = max_over_ranks(t_fp64[0])
+    st_fp64 = ops["fp64"].stats()
 
     lam_m = np.sort(1.0 / res_mixed[1])
     lam_d = np.sort(1.0 / res_fp64[1])
@@ -281,6 +286,12 @@ def run_fame(args):
             "fp64_solve_s": round(fp64_s, 6), "mixed_speedup_vs_fp64": round(fp64_s / step_s, 3),
             "eig_rel_err_mixed_vs_fp64": lam_err,
             "lanczos_steps": res_mixed[3]["steps"], "converged": res_mixed[3]["converged"],
+            "step_s": [round(t, 6) for t in t_mixed],
+            "inner": {"mixed": {"krinv_calls": st_mixed.inverseCalls,
+                                "fp32_pcg_iters_per_call": round(st_mixed.fp32Iterations / max(1, st_mixed.inverseCalls), 2),
+                                "fp64_refinements_per_call": round(st_mixed.refineSteps / max(1, st_mixed.inverseCalls), 2)},
+                      "fp64": {"krinv_calls": st_fp64.inverseCalls,
+                               "pcg_iters_per_call": round(st_fp64.totalIterations / max(1, st_fp64.inverseCalls), 2)}},
             "solves_per_s_all_gpus": round(world / step_s, 4),
             "yee_pts_per_s": None,
             "roofline": {"bound": "hbm", "achieved": round(ach32, 1), "peak": peak, "unit": "GB/s",

@@ -30,6 +30,10 @@ struct BasisArgs {
   double *invC, *Qq, *q1, *q2, *q3;
   float2 *W1f, *W2f;
   float* invCf;
+  double2 *W1_l, *W2_l;
+  double* invC_l;
+  float2 *W1f_l, *W2f_l;
+  float* invCf_l;
   BasisReduce* red;
 };
 
@@ -100,6 +104,18 @@ __global__ void k_build_basis(BasisArgs a) {
     a.W1f[i] = make_float2((float)W1, 0.f);
     a.W2f[i] = make_float2((float)W2, 0.f);
     a.invCf[i] = (float)invC;
+    {  // line-order copies: within a column of n^3 modes, axis 1 slowest
+      const long long n3 = (long long)a.n * a.n * a.n;
+      const long long cb = i - i % n3;
+      const long long g = i - cb;
+      const long long il = cb + g / a.n + (long long)a.n * a.n * (g % a.n);
+      a.W1_l[il] = make_double2(W1, 0.0);
+      a.W2_l[il] = make_double2(W2, 0.0);
+      a.invC_l[il] = invC;
+      a.W1f_l[il] = make_float2((float)W1, 0.f);
+      a.W2f_l[il] = make_float2((float)W2, 0.f);
+      a.invCf_l[il] = (float)invC;
+    }
     atomic_min_pos_double(&a.red->minQq, Qq);
     atomic_min_pos_double(&a.red->minAbsDet, fabs(det));
   }
@@ -281,6 +297,12 @@ int fame_basis_create(fame_ctx* ctx, int N, const double* P, const double* q, fa
   if (s == FAME_OK) s = dalloc((void**)&b->W1f, NF * sizeof(float2));
   if (s == FAME_OK) s = dalloc((void**)&b->W2f, NF * sizeof(float2));
   if (s == FAME_OK) s = dalloc((void**)&b->invCf, NF * sizeof(float));
+  if (s == FAME_OK) s = dalloc((void**)&b->W1_l, NF * sizeof(double2));
+  if (s == FAME_OK) s = dalloc((void**)&b->W2_l, NF * sizeof(double2));
+  if (s == FAME_OK) s = dalloc((void**)&b->invC_l, NF * sizeof(double));
+  if (s == FAME_OK) s = dalloc((void**)&b->W1f_l, NF * sizeof(float2));
+  if (s == FAME_OK) s = dalloc((void**)&b->W2f_l, NF * sizeof(float2));
+  if (s == FAME_OK) s = dalloc((void**)&b->invCf_l, NF * sizeof(float));
   BasisReduce* red = nullptr;
   if (s == FAME_OK) s = dalloc((void**)&red, sizeof(BasisReduce));
   if (s != FAME_OK) {
@@ -294,6 +316,8 @@ int fame_basis_create(fame_ctx* ctx, int N, const double* P, const double* q, fa
   a.det = b->det; a.W1 = b->W1; a.W2 = b->W2;
   a.invC = b->invC; a.Qq = b->Qq; a.q1 = b->q[0]; a.q2 = b->q[1]; a.q3 = b->q[2];
   a.W1f = b->W1f; a.W2f = b->W2f; a.invCf = b->invCf;
+  a.W1_l = b->W1_l; a.W2_l = b->W2_l; a.invC_l = b->invC_l;
+  a.W1f_l = b->W1f_l; a.W2f_l = b->W2f_l; a.invCf_l = b->invCf_l;
   a.red = red;
   k_build_basis<<<ew_blocks(NF), 256, 0, ctx->stream>>>(a);
   ::fame::count_launch();
@@ -330,6 +354,8 @@ int fame_basis_destroy(fame_basis* b) {
   dfree(b->det); dfree(b->W1); dfree(b->W2); dfree(b->invC); dfree(b->Qq);
   for (int j = 0; j < 3; ++j) dfree(b->q[j]);
   dfree(b->W1f); dfree(b->W2f); dfree(b->invCf);
+  dfree(b->W1_l); dfree(b->W2_l); dfree(b->invC_l);
+  dfree(b->W1f_l); dfree(b->W2f_l); dfree(b->invCf_l);
   dfree(b->work);
   delete b;
   return FAME_OK;

@@ -11,6 +11,15 @@
 // avoid bank conflicts), one thread transforms one line in registers with a
 // fully unrolled mixed-radix (2,3,5,7) DFT whose twiddles are compile-time
 // constants.
+//
+// Two orderings of the modes of one column (cube of n^3 modes, column index
+// c456) are used:
+//   natural  (the reference's column-major order): g = i1 + n*(i2 + n*i3)
+//   line     (axis 1 slowest):                     q = (i2 + n*i3) + n^2*i1
+// Vectors that stay inside a solve (PCG iterates, W1/W2/invC) use the line
+// order, so that pass A reads and pass C writes one axis-1 line per thread
+// with consecutive threads on consecutive addresses.  Prologue and epilogue
+// functors receive both indices (ia = line order, in = natural order).
 #pragma once
 #include "fame_common.cuh"
 #include "twiddles.cuh"
@@ -159,33 +168,125 @@ struct Gate {
   __device__ __forceinline__ bool off() const { return active != nullptr && *((volatile const int*)active) == 0; }
 };
 
+// Columns (contiguous n^3 cubes) per CTA of passes A and C: enough lines
+// (G*n^2) per CTA to keep ~200-300 threads busy, bounded by shared memory.
+template <int n, typename T> struct PassACols {
+  static constexpr int n2 = n * n, n3 = n * n * n;
+  static constexpr int value = sizeof(T) == 4
+      ? (n == 2 ? 8 : n == 4 ? 16 : n == 6 ? 6 : n == 8 ? 4 : n == 10 ? 2 : n == 12 ? 2 : 1)
+      : (n == 2 ? 8 : n == 4 ? 8 : n == 6 ? 3 : n == 8 ? 2 : 1);
+  static_assert(n3 % value == 0, "columns per CTA must divide n^3");
+};
+
+// Fields of one line are kept in registers together (FP32, or a single field);
+// FP64 multi-field lines are processed one field at a time.
+template <typename T, int F> struct FieldsInRegs {
+  static constexpr bool value = sizeof(T) == 4 || F == 1;
+};
+
+// Natural <-> line order of a global mode index (see the header comment).
+template <int n> __device__ __forceinline__ long long nat_to_line(long long i) {
+  constexpr int n2 = n * n, n3 = n * n * n;
+  const long long cb = i - i % n3;
+  const int g = (int)(i - cb);
+  return cb + g / n + n2 * (g % n);
+}
+template <int n> __device__ __forceinline__ long long line_to_nat(long long i) {
+  constexpr int n2 = n * n, n3 = n * n * n;
+  const long long cb = i - i % n3;
+  const int q = (int)(i - cb);
+  return cb + q / n2 + n * (q % n2);
+}
+
 // ------------------------------------------------------------------ pass A
-// CTA = one column c456 (contiguous cube of n^3 modes) x F fields.
-// Pro::load(i, v[F]) produces the F field values at mode i.
-template <int n, typename T, int F, class Pro>
+// CTA = G consecutive columns c456 x F fields.
+//   phase 1: axis-1 lines through Pro::load(ia, in, v[F]) (thread <-> line
+//            l = i2 + n*i3, element j = i1: ia = base + l + n^2 j, coalesced
+//            across threads in line order), inverse DFT in registers, to smem;
+//   phase 2: axis-2 lines in shared memory;
+//   phase 3: axis-3 lines from shared memory, DFT, written to work in natural
+//            order (coalesced).
+template <int n, typename T, int F, int G, class Pro>
 __global__ void __launch_bounds__(512) k_passA(Pro pro, C<T>* __restrict__ work, long long NF, Gate gate) {
   if (gate.off()) return;
   using Q = Cube<n>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C<T>* s = reinterpret_cast<C<T>*>(smem_raw);
-  const long long base = (long long)blockIdx.x * Q::n3;
-  for (int g = threadIdx.x; g < Q::n3; g += blockDim.x) {
-    C<T> v[F];
-    pro.load(base + g, v);
+  const long long col0 = (long long)blockIdx.x * G;
+  constexpr int items = G * Q::n2;
+  if constexpr (FieldsInRegs<T, F>::value) {
+    for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 1 from global
+      const int cc = it / Q::n2, l = it % Q::n2;
+      const long long cb = (col0 + cc) * Q::n3;
+      C<T>* sc = s + cc * F * Q::size + Q::pitch * l;
+      T re[F][n], im[F][n];
 #pragma unroll
-    for (int f = 0; f < F; ++f) s[f * Q::size + Q::sidx(g)] = v[f];
+      for (int j = 0; j < n; ++j) {
+        C<T> v[F];
+        pro.load(cb + l + Q::n2 * j, cb + j + (long long)n * l, v);
+#pragma unroll
+        for (int f = 0; f < F; ++f) { re[f][j] = v[f].x; im[f][j] = v[f].y; }
+      }
+#pragma unroll
+      for (int f = 0; f < F; ++f) {
+        Dft<n, +1, T>::run(re[f], im[f]);
+#pragma unroll
+        for (int j = 0; j < n; ++j) sc[f * Q::size + j] = mk<T>(re[f][j], im[f][j]);
+      }
+    }
+  } else {
+    // FP64 multi-field: prologue staged through shared memory in line order, then axis 1 there
+    for (int idx = threadIdx.x; idx < G * Q::n3; idx += blockDim.x) {
+      const int cc = idx / Q::n3, q = idx % Q::n3;
+      const int i1 = q / Q::n2, l = q % Q::n2;
+      const long long cb = (col0 + cc) * Q::n3;
+      C<T> v[F];
+      pro.load(cb + q, cb + i1 + (long long)n * l, v);
+#pragma unroll
+      for (int f = 0; f < F; ++f) s[(cc * F + f) * Q::size + i1 + Q::pitch * l] = v[f];
+    }
+    __syncthreads();
+    for (int it = threadIdx.x; it < items; it += blockDim.x) {
+      const int cc = it / Q::n2, l = it % Q::n2;
+      C<T>* sc = s + cc * F * Q::size + Q::pitch * l;
+#pragma unroll
+      for (int f = 0; f < F; ++f) line_dft<n, +1, T>(sc + f * Q::size, 1);
+    }
   }
   __syncthreads();
-  cubes_dft3<n, +1, T>(s, F);
-  for (int idx = threadIdx.x; idx < F * Q::n3; idx += blockDim.x) {
-    const int f = idx / Q::n3, g = idx % Q::n3;
-    work[f * NF + base + g] = s[f * Q::size + Q::sidx(g)];
+  for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 2
+    const int cc = it / Q::n2, l = it % Q::n2;
+    C<T>* sc = s + cc * F * Q::size + (l % n) + Q::pitch * n * (l / n);
+#pragma unroll
+    for (int f = 0; f < F; ++f) line_dft<n, +1, T>(sc + f * Q::size, Q::pitch);
+  }
+  __syncthreads();
+  for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 3 -> global (natural order)
+    const int cc = it / Q::n2, m = it % Q::n2;
+    const C<T>* sc = s + cc * F * Q::size + (m % n) + Q::pitch * (m / n);
+    const long long g0 = (col0 + cc) * Q::n3 + m;
+#pragma unroll
+    for (int f = 0; f < F; ++f) {
+      T re[n], im[n];
+#pragma unroll
+      for (int j = 0; j < n; ++j) {
+        const C<T> v = sc[f * Q::size + Q::pitch * n * j];
+        re[j] = v.x;
+        im[j] = v.y;
+      }
+      Dft<n, +1, T>::run(re, im);
+#pragma unroll
+      for (int j = 0; j < n; ++j) work[f * NF + g0 + (long long)Q::n2 * j] = mk<T>(re[j], im[j]);
+    }
   }
 }
 
 // ------------------------------------------------------------------ pass B
 // CTA = TT consecutive c123 indices x all n^3 c456 indices of one field
-// (blockIdx.y).  Inverse DFT over axes 4-6, multiply by Es = E/NF, forward.
+// (blockIdx.y).  Axis 4 lines come from / go to global (TT consecutive
+// elements per row: 32-byte sectors), axes 5 and 6 run in shared memory, and
+// the axis-6 line does inverse DFT, the E/NF multiply and the forward DFT in
+// registers.
 template <int n, typename T, int TT, typename TE>
 __global__ void __launch_bounds__(512) k_passB(C<T>* __restrict__ work, const TE* __restrict__ Es, TE escale,
                                               long long NF, Gate gate) {
@@ -195,31 +296,82 @@ __global__ void __launch_bounds__(512) k_passB(C<T>* __restrict__ work, const TE
   C<T>* s = reinterpret_cast<C<T>*>(smem_raw);
   C<T>* w = work + (long long)blockIdx.y * NF;
   const long long c0 = (long long)blockIdx.x * TT;
-  for (int idx = threadIdx.x; idx < TT * Q::n3; idx += blockDim.x) {
-    const int t = idx % TT, g = idx / TT;
-    s[t * Q::size + Q::sidx(g)] = w[c0 + t + (long long)Q::n3 * g];
+  constexpr int items = TT * Q::n2;
+  constexpr long long N3 = Q::n3;
+  for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 4 (inverse) from global
+    const int t = it % TT, l = it / TT;
+    const C<T>* src = w + c0 + t + N3 * n * l;
+    T re[n], im[n];
+#pragma unroll
+    for (int j = 0; j < n; ++j) {
+      const C<T> v = src[N3 * j];
+      re[j] = v.x;
+      im[j] = v.y;
+    }
+    Dft<n, +1, T>::run(re, im);
+    C<T>* sc = s + t * Q::size + Q::pitch * l;
+#pragma unroll
+    for (int j = 0; j < n; ++j) sc[j] = mk<T>(re[j], im[j]);
   }
   __syncthreads();
-  cubes_dft3<n, +1, T>(s, TT);
-  for (int idx = threadIdx.x; idx < TT * Q::n3; idx += blockDim.x) {
-    const int t = idx % TT, g = idx / TT;
-    const T e = (T)(Es[c0 + t + (long long)Q::n3 * g] * escale);
-    C<T>& v = s[t * Q::size + Q::sidx(g)];
-    v = cscale<T>(v, e);
+  for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 5 (inverse)
+    const int t = it / Q::n2, l = it % Q::n2;
+    line_dft<n, +1, T>(s + t * Q::size + (l % n) + Q::pitch * n * (l / n), Q::pitch);
   }
   __syncthreads();
-  cubes_dft3<n, -1, T>(s, TT);
-  for (int idx = threadIdx.x; idx < TT * Q::n3; idx += blockDim.x) {
-    const int t = idx % TT, g = idx / TT;
-    w[c0 + t + (long long)Q::n3 * g] = s[t * Q::size + Q::sidx(g)];
+  for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 6: inverse, *E/NF, forward
+    const int t = it / Q::n2, m = it % Q::n2;
+    C<T>* sc = s + t * Q::size + (m % n) + Q::pitch * (m / n);
+    T re[n], im[n];
+#pragma unroll
+    for (int j = 0; j < n; ++j) {
+      const C<T> v = sc[Q::pitch * n * j];
+      re[j] = v.x;
+      im[j] = v.y;
+    }
+    Dft<n, +1, T>::run(re, im);
+    const TE* e = Es + c0 + t + N3 * m;
+#pragma unroll
+    for (int j = 0; j < n; ++j) {
+      const T ej = (T)(e[N3 * Q::n2 * j] * escale);
+      re[j] *= ej;
+      im[j] *= ej;
+    }
+    Dft<n, -1, T>::run(re, im);
+#pragma unroll
+    for (int j = 0; j < n; ++j) sc[Q::pitch * n * j] = mk<T>(re[j], im[j]);
+  }
+  __syncthreads();
+  for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 5 (forward)
+    const int t = it / Q::n2, l = it % Q::n2;
+    line_dft<n, -1, T>(s + t * Q::size + (l % n) + Q::pitch * n * (l / n), Q::pitch);
+  }
+  __syncthreads();
+  for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 4 (forward) to global
+    const int t = it % TT, l = it / TT;
+    const C<T>* sc = s + t * Q::size + Q::pitch * l;
+    T re[n], im[n];
+#pragma unroll
+    for (int j = 0; j < n; ++j) {
+      const C<T> v = sc[j];
+      re[j] = v.x;
+      im[j] = v.y;
+    }
+    Dft<n, -1, T>::run(re, im);
+    C<T>* dst = w + c0 + t + N3 * n * l;
+#pragma unroll
+    for (int j = 0; j < n; ++j) dst[N3 * j] = mk<T>(re[j], im[j]);
   }
 }
 
 // ------------------------------------------------------------------ pass C
-// CTA = one column c456 x F fields; forward DFT over axes 1-3, then
-// Epi::store(i, v[F], acc) per mode, then a grid reduction of acc with
-// Epi::finalize (when Epi::K > 0).
-template <int n, typename T, int F, class Epi>
+// CTA = G columns x F fields; forward DFT over axes 3, 2, 1: axis-3 lines
+// read from work (natural order, coalesced), axis 2 in shared memory, axis-1
+// lines in registers, then Epi::store(ia, in, v[F], acc) per mode (line
+// order coalesced across threads) and a grid reduction of acc with
+// Epi::finalize (when Epi::K > 0).  FP64 multi-field chains run axis 1 in
+// shared memory and feed the epilogue from there.
+template <int n, typename T, int F, int G, class Epi>
 __global__ void __launch_bounds__(512) k_passC(Epi epi, const C<T>* __restrict__ work, long long NF, Gate gate) {
   if (gate.off()) return;
   using Q = Cube<n>;
@@ -227,21 +379,78 @@ __global__ void __launch_bounds__(512) k_passC(Epi epi, const C<T>* __restrict__
   constexpr int K = Epi::K;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C<T>* s = reinterpret_cast<C<T>*>(smem_raw);
-  const long long base = (long long)blockIdx.x * Q::n3;
-  for (int idx = threadIdx.x; idx < F * Q::n3; idx += blockDim.x) {
-    const int f = idx / Q::n3, g = idx % Q::n3;
-    s[f * Q::size + Q::sidx(g)] = work[f * NF + base + g];
+  const long long col0 = (long long)blockIdx.x * G;
+  constexpr int items = G * Q::n2;
+  for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 3 from global
+    const int cc = it / Q::n2, m = it % Q::n2;
+    const long long g0 = (col0 + cc) * Q::n3 + m;
+    C<T>* sc = s + cc * F * Q::size + (m % n) + Q::pitch * (m / n);
+#pragma unroll
+    for (int f = 0; f < F; ++f) {
+      T re[n], im[n];
+#pragma unroll
+      for (int j = 0; j < n; ++j) {
+        const C<T> v = work[f * NF + g0 + (long long)Q::n2 * j];
+        re[j] = v.x;
+        im[j] = v.y;
+      }
+      Dft<n, -1, T>::run(re, im);
+#pragma unroll
+      for (int j = 0; j < n; ++j) sc[f * Q::size + Q::pitch * n * j] = mk<T>(re[j], im[j]);
+    }
   }
   __syncthreads();
-  cubes_dft3<n, -1, T>(s, F);
+  for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 2
+    const int cc = it / Q::n2, l = it % Q::n2;
+    C<T>* sc = s + cc * F * Q::size + (l % n) + Q::pitch * n * (l / n);
+#pragma unroll
+    for (int f = 0; f < F; ++f) line_dft<n, -1, T>(sc + f * Q::size, Q::pitch);
+  }
+  __syncthreads();
   Red<A, (K > 0 ? K : 1)> acc;
 #pragma unroll
   for (int k = 0; k < (K > 0 ? K : 1); ++k) acc.v[k] = 0;
-  for (int g = threadIdx.x; g < Q::n3; g += blockDim.x) {
-    C<T> v[F];
+  if constexpr (FieldsInRegs<T, F>::value) {
+    for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 1 + epilogue in registers
+      const int cc = it / Q::n2, l = it % Q::n2;
+      const C<T>* sc = s + cc * F * Q::size + Q::pitch * l;
+      const long long cb = (col0 + cc) * Q::n3;
+      T re[F][n], im[F][n];
 #pragma unroll
-    for (int f = 0; f < F; ++f) v[f] = s[f * Q::size + Q::sidx(g)];
-    epi.store(base + g, v, acc);
+      for (int f = 0; f < F; ++f) {
+#pragma unroll
+        for (int j = 0; j < n; ++j) {
+          const C<T> v = sc[f * Q::size + j];
+          re[f][j] = v.x;
+          im[f][j] = v.y;
+        }
+        Dft<n, -1, T>::run(re[f], im[f]);
+      }
+#pragma unroll
+      for (int j = 0; j < n; ++j) {
+        C<T> v[F];
+#pragma unroll
+        for (int f = 0; f < F; ++f) v[f] = mk<T>(re[f][j], im[f][j]);
+        epi.store(cb + l + Q::n2 * j, cb + j + (long long)n * l, v, acc);
+      }
+    }
+  } else {
+    for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 1 in shared memory
+      const int cc = it / Q::n2, l = it % Q::n2;
+      C<T>* sc = s + cc * F * Q::size + Q::pitch * l;
+#pragma unroll
+      for (int f = 0; f < F; ++f) line_dft<n, -1, T>(sc + f * Q::size, 1);
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < G * Q::n3; idx += blockDim.x) {  // epilogue, line order
+      const int cc = idx / Q::n3, q = idx % Q::n3;
+      const int i1 = q / Q::n2, l = q % Q::n2;
+      const long long cb = (col0 + cc) * Q::n3;
+      C<T> v[F];
+#pragma unroll
+      for (int f = 0; f < F; ++f) v[f] = s[(cc * F + f) * Q::size + i1 + Q::pitch * l];
+      epi.store(cb + q, cb + i1 + (long long)n * l, v, acc);
+    }
   }
   if constexpr (K > 0) {
     grid_sum_finalize<A, K>(acc, epi.partials, epi.counter, [&](const Red<A, K>& tot) { epi.finalize(tot); });

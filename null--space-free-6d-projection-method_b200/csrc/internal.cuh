@@ -29,6 +29,11 @@ struct fame_basis {
   double *invC = nullptr, *Qq = nullptr, *q[3] = {nullptr};
   float2 *W1f = nullptr, *W2f = nullptr;
   float* invCf = nullptr;
+  // line-order copies used inside solves (axis 1 slowest within each column)
+  double2 *W1_l = nullptr, *W2_l = nullptr;
+  double* invC_l = nullptr;
+  float2 *W1f_l = nullptr, *W2f_l = nullptr;
+  float* invCf_l = nullptr;
   void* work = nullptr;  // scratch of fame_apply_Mhat_C_scalar_compact (3 fields)
   size_t work_bytes = 0;
   fame_basis_info info{};

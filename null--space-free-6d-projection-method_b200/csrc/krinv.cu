@@ -15,12 +15,12 @@
 
 namespace fame {
 
-// pre chain: fields r1, r2 of r = V1^{-*} q
+// pre chain: fields r1, r2 of r = V1^{-*} q (q, V, det in natural order)
 struct ProKrPre {
   const double2* q;
   const double2 *V11, *V12, *V21, *V22, *det;
   long long NF;
-  __device__ __forceinline__ void load(long long i, double2* v) const {
+  __device__ __forceinline__ void load(long long, long long i, double2* v) const {
     const double2 q1 = q[i], q2 = q[NF + i];
     const double2 d = cconj<double>(det[i]);
     v[0] = cdiv<double>(csub<double>(cmulc<double>(V22[i], q1), cmulc<double>(V21[i], q2)), d);
@@ -28,6 +28,7 @@ struct ProKrPre {
   }
 };
 // keep mr1, mr2; form bhat (= PCG rhs b and initial residual r), x = 0, PCG state
+// (all line order)
 struct EpiKrPre {
   using Acc = double;
   static constexpr int K = 1;
@@ -38,7 +39,7 @@ struct EpiKrPre {
   int maxit;
   double* partials;
   unsigned* counter;
-  __device__ __forceinline__ void store(long long i, const double2* v, Red<double, 1>& acc) const {
+  __device__ __forceinline__ void store(long long i, long long, const double2* v, Red<double, 1>& acc) const {
     mr1[i] = v[0];
     mr2[i] = v[1];
     const double2 s = cadd<double>(cmulc<double>(c.W1[i], v[0]), cmulc<double>(c.W2[i], v[1]));
@@ -56,13 +57,14 @@ struct EpiKrPre {
 struct ProKrPost {
   MhatCoef<double> c;
   const double2* u;
-  __device__ __forceinline__ void load(long long i, double2* v) const {
+  __device__ __forceinline__ void load(long long i, long long, double2* v) const {
     const double2 z = cscale<double>(u[i], c.invC[i]);
     v[0] = cmul<double>(c.W1[i], z);
     v[1] = cmul<double>(c.W2[i], z);
   }
 };
-// y = V1^{-1}[mr1 + M W1 z; mr2 + M W2 z]; counts non-finite outputs into st->aux
+// y = V1^{-1}[mr1 + M W1 z; mr2 + M W2 z] (y, V, det natural; mr line order);
+// counts non-finite outputs into st->aux
 struct EpiKrPost {
   using Acc = double;
   static constexpr int K = 1;
@@ -72,8 +74,8 @@ struct EpiKrPost {
   PcgState* st;
   double* partials;
   unsigned* counter;
-  __device__ __forceinline__ void store(long long i, const double2* v, Red<double, 1>& acc) const {
-    const double2 t1 = cadd<double>(mr1[i], v[0]), t2 = cadd<double>(mr2[i], v[1]);
+  __device__ __forceinline__ void store(long long ia, long long i, const double2* v, Red<double, 1>& acc) const {
+    const double2 t1 = cadd<double>(mr1[ia], v[0]), t2 = cadd<double>(mr2[ia], v[1]);
     const double2 d = det[i];
     const double2 y1 = cdiv<double>(csub<double>(cmul<double>(V22[i], t1), cmul<double>(V12[i], t2)), d);
     const double2 y2 = cdiv<double>(csub<double>(cmul<double>(V11[i], t2), cmul<double>(V21[i], t1)), d);
@@ -93,6 +95,8 @@ __global__ void k_zero_c(double2* x, long long n) {
 
 template <> MhatCoef<double> coef_of<double>(fame_basis* b) { return MhatCoef<double>{b->invC, b->W1, b->W2}; }
 template <> MhatCoef<float> coef_of<float>(fame_basis* b) { return MhatCoef<float>{b->invCf, b->W1f, b->W2f}; }
+template <> MhatCoef<double> coef_line_of<double>(fame_basis* b) { return MhatCoef<double>{b->invC_l, b->W1_l, b->W2_l}; }
+template <> MhatCoef<float> coef_line_of<float>(fame_basis* b) { return MhatCoef<float>{b->invCf_l, b->W1f_l, b->W2f_l}; }
 template <> const double* es_of<double>(fame_mass* m) { return m->Es64; }
 template <> const float* es_of<float>(fame_mass* m) { return m->Es32; }
 
@@ -100,7 +104,7 @@ int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
   fame_basis* bs = K->b;
   cudaStream_t s = K->ctx->stream;
   const long long NF = K->NF;
-  const MhatCoef<double> c64 = coef_of<double>(bs);
+  const MhatCoef<double> c64 = coef_line_of<double>(bs);
   PcgBuf<double>& B = K->b64;
   PcgState* st = K->st64;
   const double tolMhat = K->o.tolCG;
@@ -117,7 +121,7 @@ int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
   double relres = 0.0;
   int iters = 0;
   if (K->o.prec_mode == FAME_PREC_FP64) {
-    FAME_TRY(pcg_iterate<double>(K, OpMhat<double>{coef_of<double>(bs), es_of<double>(K->m)}, B, st, K->lastIt64, h, K->o.verifyTrueResidual != 0, K->bhat));
+    FAME_TRY(pcg_iterate<double>(K, OpMhat<double>{coef_line_of<double>(bs), es_of<double>(K->m)}, B, st, K->lastIt64, h, K->o.verifyTrueResidual != 0, K->bhat));
     if (h.flag == -1) return fail(FAME_ERR_NONFINITE, "Mhat right-hand side contains NaN/Inf");
     iters = h.iter;
     relres = h.bnorm2 > 0 ? std::sqrt(h.rho / h.bnorm2) : 0.0;
@@ -147,7 +151,7 @@ int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
                                                               partials32, K->counter);
       ::fame::count_launch();
       PcgState h32{};
-      FAME_TRY(pcg_iterate<float>(K, OpMhat<float>{coef_of<float>(bs), es_of<float>(K->m)}, F, st32, K->lastIt32, h32, false, nullptr));
+      FAME_TRY(pcg_iterate<float>(K, OpMhat<float>{coef_line_of<float>(bs), es_of<float>(K->m)}, F, st32, K->lastIt32, h32, false, nullptr));
       if (h32.flag == -1 || h32.flag == 4)
         return fail(FAME_ERR_NOT_CONVERGED, "FP32 correction solve broke down");
       K->stats.fp32Iterations += h32.iter;
@@ -220,11 +224,11 @@ int fame_apply_Mhat_C_scalar_compact(fame_basis* b, fame_mass* m, const void* x,
   cudaStream_t s = b->ctx->stream;
   if (prec == FAME_F64) {
     const MhatCoef<double> c = coef_of<double>(b);
-    return run_chain<double, 3>(b->n, ProMhat<double>{c, (const double2*)x}, EpiMhat<double>{c, (double2*)y},
+    return run_chain<double, 3>(b->n, ProMhat<double, false>{c, (const double2*)x}, EpiMhat<double, false>{c, (double2*)y},
                                 work, m->Es64, 1.0, b->NF, s);
   }
   const MhatCoef<float> c = coef_of<float>(b);
-  return run_chain<float, 3>(b->n, ProMhat<float>{c, (const float2*)x}, EpiMhat<float>{c, (float2*)y},
+  return run_chain<float, 3>(b->n, ProMhat<float, false>{c, (const float2*)x}, EpiMhat<float, false>{c, (float2*)y},
                              (float2*)work, m->Es32, 1.0f, b->NF, s);
 }
 
@@ -299,6 +303,7 @@ int fame_krinv_destroy(fame_krinv* K) {
   dfree(K->mr1); dfree(K->mr2); dfree(K->bhat);
   dfree(K->partials); dfree(K->counter); dfree(K->st64); dfree(K->st32);
   nested_free(K);
+  lanczos_ws_free(K);
   delete K;
   return FAME_OK;
 }

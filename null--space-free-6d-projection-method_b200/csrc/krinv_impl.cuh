@@ -40,13 +40,16 @@ struct fame_krinv {
   double2 *ox = nullptr, *orr = nullptr, *oz = nullptr, *op = nullptr, *oq = nullptr;
   double* sigma = nullptr;  // |q|^2 (NF), sigma_r = [sigma; sigma]
   fame::OuterState* ost = nullptr;
+  void* lanczos_ws = nullptr;  // Lanczos basis workspace reused across solves
 };
 
 namespace fame {
 int nested_alloc(fame_krinv* K);
 void nested_free(fame_krinv* K);
 int krinv_nested_apply_one(fame_krinv* K, const double2* b, double2* x);
-template <typename T> MhatCoef<T> coef_of(fame_basis* b);
+void lanczos_ws_free(fame_krinv* K);
+template <typename T> MhatCoef<T> coef_of(fame_basis* b);       // natural order
+template <typename T> MhatCoef<T> coef_line_of(fame_basis* b);  // line order
 template <typename T> const T* es_of(fame_mass* m);
 }  // namespace fame
 

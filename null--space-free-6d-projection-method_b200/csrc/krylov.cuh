@@ -67,6 +67,8 @@ static __global__ void k_pcg_resume(PcgState* st) {
 }
 
 // ---------------------------------------------------------------- functors
+// Unless stated otherwise, functors index line-order vectors (ia) and the
+// line-order copies of W1, W2, invC.
 // Mhat x = C^{-1}(M z + W1^* M(W1 z) + W2^* M(W2 z)), z = C^{-1} x
 // (exp1/apply_Mhat_C_scalar_compact.m:8-21): three mass fields per vector.
 template <typename T>
@@ -82,20 +84,27 @@ __device__ __forceinline__ C<T> mhat_combine(const MhatCoef<T>& c, long long i, 
   return cscale<T>(s, c.invC[i]);
 }
 
-// Plain Mhat action.
-template <typename T> struct ProMhat {
+// Plain Mhat action; LINE selects line-order (ia) or natural-order (in)
+// vectors and coefficients.
+template <typename T, bool LINE> struct ProMhat {
   MhatCoef<T> c;
   const C<T>* x;
-  __device__ __forceinline__ void load(long long i, C<T>* v) const { mhat_fields<T>(c, i, x[i], v); }
+  __device__ __forceinline__ void load(long long ia, long long in, C<T>* v) const {
+    const long long i = LINE ? ia : in;
+    mhat_fields<T>(c, i, x[i], v);
+  }
 };
-template <typename T> struct EpiMhat {
+template <typename T, bool LINE> struct EpiMhat {
   using Acc = T;
   static constexpr int K = 0;
   MhatCoef<T> c;
   C<T>* y;
   T* partials = nullptr;
   unsigned* counter = nullptr;
-  __device__ __forceinline__ void store(long long i, const C<T>* v, Red<T, 1>&) const { y[i] = mhat_combine<T>(c, i, v); }
+  __device__ __forceinline__ void store(long long ia, long long in, const C<T>* v, Red<T, 1>&) const {
+    const long long i = LINE ? ia : in;
+    y[i] = mhat_combine<T>(c, i, v);
+  }
   __device__ __forceinline__ void finalize(const Red<T, 1>&) const {}
 };
 
@@ -106,7 +115,7 @@ template <typename T> struct ProPcgMhat {
   C<T>* p;
   const C<T>* r;
   const PcgState* st;
-  __device__ __forceinline__ void load(long long i, C<T>* v) const {
+  __device__ __forceinline__ void load(long long i, long long, C<T>* v) const {
     C<T> pi = r[i];
     if (st->iter > 0) pi = cadd<T>(pi, cscale<T>(p[i], (T)st->beta));
     p[i] = pi;
@@ -123,7 +132,7 @@ template <typename T> struct EpiPcgMhat {
   PcgState* st;
   T* partials;
   unsigned* counter;
-  __device__ __forceinline__ void store(long long i, const C<T>* v, Red<T, 2>& acc) const {
+  __device__ __forceinline__ void store(long long i, long long, const C<T>* v, Red<T, 2>& acc) const {
     const C<T> ap = mhat_combine<T>(c, i, v);
     Ap[i] = ap;
     const C<T> d = cmulc<T>(p[i], ap);
@@ -141,7 +150,7 @@ template <typename T, typename TD, bool ADDX> struct ProResidMhat {
   MhatCoef<T> c;
   C<T>* x;
   const C<TD>* dx;
-  __device__ __forceinline__ void load(long long i, C<T>* v) const {
+  __device__ __forceinline__ void load(long long i, long long, C<T>* v) const {
     C<T> xi = x[i];
     if (ADDX) {
       xi = cadd<T>(xi, ccast<T, TD>(dx[i]));
@@ -159,7 +168,7 @@ template <typename T> struct EpiResidMhat {
   double* out;
   T* partials;
   unsigned* counter;
-  __device__ __forceinline__ void store(long long i, const C<T>* v, Red<T, 1>& acc) const {
+  __device__ __forceinline__ void store(long long i, long long, const C<T>* v, Red<T, 1>& acc) const {
     const C<T> ri = csub<T>(b[i], mhat_combine<T>(c, i, v));
     r[i] = ri;
     acc.v[0] += cabs2<T>(ri);
@@ -175,7 +184,7 @@ template <typename T> struct ProPcgM3 {
   const C<T>* r;
   const PcgState* st;
   long long NF;
-  __device__ __forceinline__ void load(long long i, C<T>* v) const {
+  __device__ __forceinline__ void load(long long i, long long, C<T>* v) const {
     const bool upd = st->iter > 0;
     const T beta = (T)st->beta;
 #pragma unroll
@@ -196,7 +205,7 @@ template <typename T> struct EpiPcgM3 {
   long long NF;
   T* partials;
   unsigned* counter;
-  __device__ __forceinline__ void store(long long i, const C<T>* v, Red<T, 2>& acc) const {
+  __device__ __forceinline__ void store(long long i, long long, const C<T>* v, Red<T, 2>& acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       Ap[c * NF + i] = v[c];
@@ -213,7 +222,7 @@ template <typename T, typename TD, bool ADDX> struct ProResidM3 {
   C<T>* x;
   const C<TD>* dx;
   long long NF;
-  __device__ __forceinline__ void load(long long i, C<T>* v) const {
+  __device__ __forceinline__ void load(long long i, long long, C<T>* v) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       C<T> xi = x[c * NF + i];
@@ -234,7 +243,7 @@ template <typename T> struct EpiResidM3 {
   long long NF;
   T* partials;
   unsigned* counter;
-  __device__ __forceinline__ void store(long long i, const C<T>* v, Red<T, 1>& acc) const {
+  __device__ __forceinline__ void store(long long i, long long, const C<T>* v, Red<T, 1>& acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const C<T> ri = csub<T>(b[c * NF + i], v[c]);

@@ -354,6 +354,11 @@ struct LanczosWs {
   }
 };
 
+void lanczos_ws_free(fame_krinv* K) {
+  delete static_cast<LanczosWs*>(K->lanczos_ws);
+  K->lanczos_ws = nullptr;
+}
+
 }  // namespace fame
 
 using namespace fame;
@@ -365,8 +370,18 @@ extern "C" int fame_lanczos(fame_krinv* K, int nev, double tol, int maxiter, int
   fame_ctx* ctx = K->ctx;
   cudaStream_t s = ctx->stream;
   const long long n = 2 * K->NF;
-  LanczosWs L;
-  FAME_TRY(L.alloc(ctx, n, p));
+  // the basis workspace (2 x n x p complex) is kept by the operator handle and reused
+  if (!K->lanczos_ws || static_cast<LanczosWs*>(K->lanczos_ws)->p != p) {
+    lanczos_ws_free(K);
+    LanczosWs* w = new LanczosWs();
+    const int st = w->alloc(ctx, n, p);
+    if (st != FAME_OK) {
+      delete w;
+      return st;
+    }
+    K->lanczos_ws = w;
+  }
+  LanczosWs& L = *static_cast<LanczosWs*>(K->lanczos_ws);
   const double eps0 = 2.220446049250313e-16;
   // v = v0 / sqrt(v0' v0)   (exp2/Lanczos.m:17-18)
   k_nrm2<<<vec_blocks(n), 256, 0, s>>>((const double2*)v0, n, L.scal, L.partials, L.counter);

@@ -34,11 +34,12 @@ int launch_passB(C<T>* work, int nfields, const TE* Es, TE escale, long long NF,
 template <int n, typename T, int F, class Pro>
 int launch_passA(const Pro& pro, C<T>* work, long long NF, cudaStream_t st, Gate gate) {
   using Q = Cube<n>;
-  const size_t smem = (size_t)F * Q::size * sizeof(C<T>);
-  static int attr = ensure_smem(k_passA<n, T, F, Pro>, smem);
+  constexpr int G = PassACols<n, T>::value;
+  const size_t smem = (size_t)G * F * Q::size * sizeof(C<T>);
+  static int attr = ensure_smem(k_passA<n, T, F, G, Pro>, smem);
   if (attr != FAME_OK) return attr;
-  const int threads = std::min(512, std::max(128, round32(F * Q::n2)));
-  k_passA<n, T, F, Pro><<<Q::n3, threads, smem, st>>>(pro, work, NF, gate);
+  const int threads = std::min(512, std::max(32, round32(G * Q::n2)));
+  k_passA<n, T, F, G, Pro><<<Q::n3 / G, threads, smem, st>>>(pro, work, NF, gate);
   ::fame::count_launch();
   return FAME_OK;
 }
@@ -46,11 +47,12 @@ int launch_passA(const Pro& pro, C<T>* work, long long NF, cudaStream_t st, Gate
 template <int n, typename T, int F, class Epi>
 int launch_passC(const Epi& epi, const C<T>* work, long long NF, cudaStream_t st, Gate gate) {
   using Q = Cube<n>;
-  const size_t smem = (size_t)F * Q::size * sizeof(C<T>);
-  static int attr = ensure_smem(k_passC<n, T, F, Epi>, smem);
+  constexpr int G = PassACols<n, T>::value;
+  const size_t smem = (size_t)G * F * Q::size * sizeof(C<T>);
+  static int attr = ensure_smem(k_passC<n, T, F, G, Epi>, smem);
   if (attr != FAME_OK) return attr;
-  const int threads = std::min(512, std::max(128, round32(F * Q::n2)));
-  k_passC<n, T, F, Epi><<<Q::n3, threads, smem, st>>>(epi, work, NF, gate);
+  const int threads = std::min(512, std::max(32, round32(G * Q::n2)));
+  k_passC<n, T, F, G, Epi><<<Q::n3 / G, threads, smem, st>>>(epi, work, NF, gate);
   ::fame::count_launch();
   return FAME_OK;
 }
@@ -85,10 +87,10 @@ int run_chain(int n, const Pro& pro, const Epi& epi, C<T>* work, const TE* Es, T
 }
 
 // ------------------------------------------------------------ functors
-// Identity prologue/epilogue (plain mass action): F independent columns.
+// Identity prologue/epilogue (plain mass action, natural order): F columns.
 template <typename T, int F> struct ProCols {
   const C<T>* x[F];
-  __device__ __forceinline__ void load(long long i, C<T>* v) const {
+  __device__ __forceinline__ void load(long long, long long i, C<T>* v) const {
 #pragma unroll
     for (int f = 0; f < F; ++f) v[f] = x[f][i];
   }
@@ -99,7 +101,7 @@ template <typename T, int F> struct EpiCols {
   C<T>* y[F];
   T* partials = nullptr;
   unsigned* counter = nullptr;
-  __device__ __forceinline__ void store(long long i, const C<T>* v, Red<T, 1>&) const {
+  __device__ __forceinline__ void store(long long, long long i, const C<T>* v, Red<T, 1>&) const {
 #pragma unroll
     for (int f = 0; f < F; ++f) y[f][i] = v[f];
   }

@@ -64,11 +64,18 @@ __global__ void k_outer_dir(const double2* z, double2* p, long long n, const Out
     p[i] = first ? z[i] : cadd<double>(z[i], cscale<double>(p[i], beta));
 }
 
-// b3 = V p (2NF -> 3NF), r3 = b3, x3 = 0, ||b3||^2 -> inner PCG state
+// b3 = V p (2NF -> 3NF, b3 in line order), ||b3||^2 -> inner PCG state
+__device__ __forceinline__ long long line_index(long long i, int n) {
+  const long long n3 = (long long)n * n * n;
+  const long long cb = i - i % n3;
+  const long long g = i - cb;
+  return cb + g / n + (long long)n * n * (g % n);
+}
+
 template <typename T>
 __global__ void k_inner_init(const double2* p, const double2* V11, const double2* V12,
                              const double2* V21, const double2* V22, const double2* V31,
-                             const double2* V32, long long NF, double2* b3, PcgState* st,
+                             const double2* V32, long long NF, int n, double2* b3, PcgState* st,
                              double tol, int maxit, double* partials, unsigned* counter) {
   Red<double, 1> acc{};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < NF; i += (long long)gridDim.x * blockDim.x) {
@@ -76,9 +83,10 @@ __global__ void k_inner_init(const double2* p, const double2* V11, const double2
     const double2 y1 = cadd<double>(cmul<double>(V11[i], x1), cmul<double>(V12[i], x2));
     const double2 y2 = cadd<double>(cmul<double>(V21[i], x1), cmul<double>(V22[i], x2));
     const double2 y3 = cadd<double>(cmul<double>(V31[i], x1), cmul<double>(V32[i], x2));
-    b3[i] = y1;
-    b3[NF + i] = y2;
-    b3[2 * NF + i] = y3;
+    const long long il = line_index(i, n);
+    b3[il] = y1;
+    b3[NF + il] = y2;
+    b3[2 * NF + il] = y3;
     acc.v[0] += cabs2<double>(y1) + cabs2<double>(y2) + cabs2<double>(y3);
   }
   grid_sum_finalize<double, 1>(acc, partials, counter, [&](const Red<double, 1>& t) {
@@ -93,15 +101,16 @@ __global__ void k_copy_zero(const double2* b, double2* r, double2* x, long long 
   }
 }
 
-// q = V^* u (3NF -> 2NF); with DOT, pq = p^H q -> alpha = rho/pq
+// q = V^* u (3NF line order -> 2NF natural); with DOT, pq = p^H q -> alpha = rho/pq
 template <bool DOT>
 __global__ void k_outer_VH(const double2* u, const double2* V11, const double2* V12,
                            const double2* V21, const double2* V22, const double2* V31,
-                           const double2* V32, long long NF, double2* q, const double2* p,
+                           const double2* V32, long long NF, int n, double2* q, const double2* p,
                            OuterState* st, double* partials, unsigned* counter) {
   Red<double, 2> acc{};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < NF; i += (long long)gridDim.x * blockDim.x) {
-    const double2 x1 = u[i], x2 = u[NF + i], x3 = u[2 * NF + i];
+    const long long il = line_index(i, n);
+    const double2 x1 = u[il], x2 = u[NF + il], x3 = u[2 * NF + il];
     const double2 y1 = cadd<double>(cadd<double>(cmulc<double>(V11[i], x1), cmulc<double>(V21[i], x2)), cmulc<double>(V31[i], x3));
     const double2 y2 = cadd<double>(cadd<double>(cmulc<double>(V12[i], x1), cmulc<double>(V22[i], x2)), cmulc<double>(V32[i], x3));
     q[i] = y1;
@@ -220,7 +229,7 @@ static int apply_Kr(fame_krinv* K, const double2* in, double2* out) {
   PcgBuf<double>& B = K->b64;
   // b3 = V in ; inner state init (r3 = b3, x3 = 0 done below)
   k_inner_init<double><<<nb(NF), 256, 0, s>>>(in, b->V[0], b->V[3], b->V[1], b->V[4], b->V[2],
-                                              b->V[5], NF, K->bhat, K->st64, K->o.tolM,
+                                              b->V[5], NF, K->n, K->bhat, K->st64, K->o.tolM,
                                               K->o.prec_mode == FAME_PREC_MIXED ? K->o.maxRefine : K->o.maxitM,
                                               K->partials, K->counter);
   ::fame::count_launch();
@@ -229,7 +238,7 @@ static int apply_Kr(fame_krinv* K, const double2* in, double2* out) {
   FAME_CUDA_TRY(cudaGetLastError());
   FAME_TRY(inner_m3_solve(K));
   k_outer_VH<DOT><<<nb(NF), 256, 0, s>>>(B.x, b->V[0], b->V[3], b->V[1], b->V[4], b->V[2], b->V[5],
-                                         NF, out, K->op, K->ost, K->partials, K->counter);
+                                         NF, K->n, out, K->op, K->ost, K->partials, K->counter);
   ::fame::count_launch();
   FAME_CUDA_TRY(cudaGetLastError());
   return FAME_OK;

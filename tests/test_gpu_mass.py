@@ -102,22 +102,22 @@ def test_basis_and_maps(cuda_device, P, q):
     for name in ("V11", "V12", "V21", "V22", "V31", "V32", "detV1", "W1", "W2"):
         errs[name] = _rel(getattr(sysg, name).cpu().numpy(), getattr(S, name))
     assert max(errs.values()) < 1e-10, errs
-    assert _rel(sysg.invCorthDiag.cpu().numpy(), S.invC) < 1e-14
+    assert _rel(sysg.invCorthDiag.cpu().numpy(), S.invC) < 1e-12
     n = S.NF
     x2 = _rand(2 * n, 1, 2)
     x3 = _rand(3 * n, 2, 2)
     t = lambda a: torch.as_tensor(a, device=cuda_device)
     y = F.apply_V_blockdiag(t(x2), sysg.Vdata).cpu().numpy()
-    assert _rel(y, np.stack([O.apply_V_blockdiag(x2[:, j], S) for j in range(2)], 1)) < 1e-14
+    assert _rel(y, np.stack([O.apply_V_blockdiag(x2[:, j], S) for j in range(2)], 1)) < 1e-12
     y = F.apply_VH_blockdiag(t(x3), sysg.Vdata).cpu().numpy()
-    assert _rel(y, np.stack([O.apply_VH_blockdiag(x3[:, j], S) for j in range(2)], 1)) < 1e-14
+    assert _rel(y, np.stack([O.apply_VH_blockdiag(x3[:, j], S) for j in range(2)], 1)) < 1e-12
     args = [sysg.V11, sysg.V12, sysg.V21, sysg.V22, sysg.detV1, n]
     y = F.solveV1_blockdiag(t(x2), *args).cpu().numpy()
     ref = np.stack([O.solveV1_blockdiag(x2[:, j], S.V11, S.V12, S.V21, S.V22, S.detV1, n) for j in range(2)], 1)
-    assert _rel(y, ref) < 1e-13
+    assert _rel(y, ref) < 1e-11
     y = F.solveV1H_blockdiag(t(x2), *args).cpu().numpy()
     ref = np.stack([O.solveV1H_blockdiag(x2[:, j], S.V11, S.V12, S.V21, S.V22, S.detV1, n) for j in range(2)], 1)
-    assert _rel(y, ref) < 1e-13
+    assert _rel(y, ref) < 1e-11
 
 
 def test_gamma_point_is_rejected(cuda_device):

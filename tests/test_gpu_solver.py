@@ -86,21 +86,31 @@ def test_lanczos_reference_kat_n2(cuda_device, precision):
 
 
 def test_lanczos_baseline_n3_fp64_and_mixed(cuda_device):
-    """The N=3 BASELINE workload (golden-ratio P, separable-cos material): eigenvalues of
-    the plain FP64 and mixed forms within 1e-10 of the FP64 oracle."""
+    """The N=3 benchmark system (golden-ratio P, separable-cos material).
+
+    With a tight inner tolerance (1e-12) both precision forms give eigenvalues within
+    1e-10 of the FP64 oracle.  At the benchmark inner tolerance 1e-10 each K_r^{-1}
+    action carries a ~1e-10 relative error that is amplified by theta_1/theta_k (~17 for
+    the 10th eigenvalue), so two FP64 implementations agree to ~1e-9 there."""
     import fame_b200 as F
     N = 3
     S, sg = _systems(N, "golden", F.configs.Q_BASELINE, "cos", cuda_device)
     sol = O.solve_modes(S, nev=10, p=40, tol=1e-10, maxRestart=30, tolCG=1e-12)
     v0 = F.start_vector(F.configs.SEED, sg.nr)
+    lams = {}
     for precision in ("fp64", "mixed"):
-        op, _ = F.make_explicit_krinv_compact(sg, 1e-10, 3000, precision=precision)
-        Y, theta, steps, info = F.Lanczos(op, None, None, sg.nr, 10, 1e-8, 30, 40, v0)
-        lam = np.sort(1.0 / theta)
-        assert info["converged"], precision
-        assert np.max(np.abs(lam - sol["lam"]) / sol["lam"]) < 1e-10, precision
-        # Ritz vectors: residual of K_r^{-1} y = theta y
+        for tolCG in (1e-12, 1e-10):
+            op, _ = F.make_explicit_krinv_compact(sg, tolCG, 3000, precision=precision)
+            Y, theta, steps, info = F.Lanczos(op, None, None, sg.nr, 10, 1e-8, 30, 40, v0)
+            lam = np.sort(1.0 / theta)
+            assert info["converged"], precision
+            lams[precision, tolCG] = lam
+            err = np.max(np.abs(lam - sol["lam"]) / sol["lam"])
+            assert err < (1e-10 if tolCG == 1e-12 else 2e-9), (precision, tolCG, err)
+        # Ritz vector of the largest theta: residual of K_r^{-1} y = theta y
         j = int(np.argmax(theta))
         y = Y[:, j]
         r = op(y) - theta[j] * y
         assert float(torch.linalg.norm(r) / (abs(theta[j]) * torch.linalg.norm(y))) < 1e-6
+    d = np.max(np.abs(lams["mixed", 1e-10] - lams["fp64", 1e-10]) / lams["fp64", 1e-10])
+    assert d < 2e-9, d
