@@ -122,11 +122,41 @@ template <int n, int SIGN, typename T> struct Dft<n, SIGN, T, false> {
 };
 
 // ------------------------------------------------------------ cube geometry
-// One n^3 cube in shared memory: element (i1,i2,i3) at i1 + (n+1)*(i2 + n*i3).
-template <int n> struct Cube {
-  static constexpr int n2 = n * n, n3 = n * n * n, pitch = n + 1;
-  static constexpr int size = pitch * n2;  // elements incl. padding
-  static __device__ __forceinline__ int sidx(int g) { return (g % n) + pitch * (g / n); }
+// One n^3 cube in shared memory: element (i1,i2,i3) at i1 + P1*i2 + P2*i3.
+// The row pitch P1, plane pitch P2 and cube stride S were chosen per size and
+// element width by minimising shared-memory wavefronts over every access
+// pattern of the passes below (32 lanes, 128-byte wavefronts).
+template <int n, int ESZ> struct CubePitch;
+template <> struct CubePitch<2, 8> { static constexpr int P1 = 3, P2 = 6, S = 12; };
+template <> struct CubePitch<2, 16> { static constexpr int P1 = 3, P2 = 6, S = 12; };
+template <> struct CubePitch<4, 8> { static constexpr int P1 = 4, P2 = 20, S = 81; };
+template <> struct CubePitch<4, 16> { static constexpr int P1 = 5, P2 = 20, S = 84; };
+template <> struct CubePitch<6, 8> { static constexpr int P1 = 9, P2 = 54, S = 324; };
+template <> struct CubePitch<6, 16> { static constexpr int P1 = 9, P2 = 54, S = 324; };
+template <> struct CubePitch<8, 8> { static constexpr int P1 = 9, P2 = 72, S = 580; };
+template <> struct CubePitch<8, 16> { static constexpr int P1 = 9, P2 = 72, S = 580; };
+template <> struct CubePitch<10, 8> { static constexpr int P1 = 17, P2 = 170, S = 1700; };
+template <> struct CubePitch<10, 16> { static constexpr int P1 = 13, P2 = 130, S = 1300; };
+template <> struct CubePitch<12, 8> { static constexpr int P1 = 12, P2 = 156, S = 1873; };
+template <> struct CubePitch<12, 16> { static constexpr int P1 = 13, P2 = 156, S = 1876; };
+template <> struct CubePitch<14, 8> { static constexpr int P1 = 17, P2 = 238, S = 3332; };
+template <> struct CubePitch<14, 16> { static constexpr int P1 = 17, P2 = 238, S = 3332; };
+
+template <int n, typename T> struct Cube {
+  static constexpr int n2 = n * n, n3 = n * n * n;
+  static constexpr int P1 = CubePitch<n, (int)sizeof(C<T>)>::P1;
+  static constexpr int P2 = CubePitch<n, (int)sizeof(C<T>)>::P2;
+  static constexpr int size = CubePitch<n, (int)sizeof(C<T>)>::S;  // elements per cube incl. padding
+  static_assert(P1 >= n && P2 >= P1 * n && size >= P2 * n, "cube pitches");
+  static __device__ __forceinline__ int at(int i1, int i2, int i3) { return i1 + P1 * i2 + P2 * i3; }
+  // natural in-column index g = i1 + n*i2 + n^2*i3
+  static __device__ __forceinline__ int sidx(int g) { return at(g % n, (g / n) % n, g / n2); }
+  // start of the axis-1 line l = i2 + n*i3 (stride 1)
+  static __device__ __forceinline__ int line1(int l) { return P1 * (l % n) + P2 * (l / n); }
+  // start of the axis-2 line l = i1 + n*i3 (stride P1)
+  static __device__ __forceinline__ int line2(int l) { return (l % n) + P2 * (l / n); }
+  // start of the axis-3 line m = i1 + n*i2 (stride P2)
+  static __device__ __forceinline__ int line3(int m) { return (m % n) + P1 * (m / n); }
 };
 
 template <int n, int SIGN, typename T>
@@ -137,28 +167,6 @@ __device__ __forceinline__ void line_dft(C<T>* p, int stride) {
   Dft<n, SIGN, T>::run(re, im);
 #pragma unroll
   for (int j = 0; j < n; ++j) p[j * stride] = mk<T>(re[j], im[j]);
-}
-
-// 3D DFT of `ncubes` consecutive cubes in shared memory (all threads).
-template <int n, int SIGN, typename T>
-__device__ __forceinline__ void cubes_dft3(C<T>* s, int ncubes) {
-  using Q = Cube<n>;
-  const int lines = ncubes * Q::n2;
-  for (int t = threadIdx.x; t < lines; t += blockDim.x) {  // axis 1 (unit stride)
-    const int c = t / Q::n2, l = t % Q::n2;
-    line_dft<n, SIGN, T>(s + c * Q::size + Q::pitch * l, 1);
-  }
-  __syncthreads();
-  for (int t = threadIdx.x; t < lines; t += blockDim.x) {  // axis 2 (stride pitch)
-    const int c = t / Q::n2, l = t % Q::n2;
-    line_dft<n, SIGN, T>(s + c * Q::size + (l % n) + Q::pitch * n * (l / n), Q::pitch);
-  }
-  __syncthreads();
-  for (int t = threadIdx.x; t < lines; t += blockDim.x) {  // axis 3 (stride pitch*n)
-    const int c = t / Q::n2, l = t % Q::n2;
-    line_dft<n, SIGN, T>(s + c * Q::size + (l % n) + Q::pitch * (l / n), Q::pitch * n);
-  }
-  __syncthreads();
 }
 
 // Device-resident status word used to gate queued iterations: kernels return
@@ -209,7 +217,7 @@ template <int n> __device__ __forceinline__ long long line_to_nat(long long i) {
 template <int n, typename T, int F, int G, class Pro>
 __global__ void __launch_bounds__(512) k_passA(Pro pro, C<T>* __restrict__ work, long long NF, Gate gate) {
   if (gate.off()) return;
-  using Q = Cube<n>;
+  using Q = Cube<n, T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C<T>* s = reinterpret_cast<C<T>*>(smem_raw);
   const long long col0 = (long long)blockIdx.x * G;
@@ -218,7 +226,7 @@ __global__ void __launch_bounds__(512) k_passA(Pro pro, C<T>* __restrict__ work,
     for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 1 from global
       const int cc = it / Q::n2, l = it % Q::n2;
       const long long cb = (col0 + cc) * Q::n3;
-      C<T>* sc = s + cc * F * Q::size + Q::pitch * l;
+      C<T>* sc = s + cc * F * Q::size + Q::line1(l);
       T re[F][n], im[F][n];
 #pragma unroll
       for (int j = 0; j < n; ++j) {
@@ -243,12 +251,12 @@ __global__ void __launch_bounds__(512) k_passA(Pro pro, C<T>* __restrict__ work,
       C<T> v[F];
       pro.load(cb + q, cb + i1 + (long long)n * l, v);
 #pragma unroll
-      for (int f = 0; f < F; ++f) s[(cc * F + f) * Q::size + i1 + Q::pitch * l] = v[f];
+      for (int f = 0; f < F; ++f) s[(cc * F + f) * Q::size + i1 + Q::line1(l)] = v[f];
     }
     __syncthreads();
     for (int it = threadIdx.x; it < items; it += blockDim.x) {
       const int cc = it / Q::n2, l = it % Q::n2;
-      C<T>* sc = s + cc * F * Q::size + Q::pitch * l;
+      C<T>* sc = s + cc * F * Q::size + Q::line1(l);
 #pragma unroll
       for (int f = 0; f < F; ++f) line_dft<n, +1, T>(sc + f * Q::size, 1);
     }
@@ -256,21 +264,21 @@ __global__ void __launch_bounds__(512) k_passA(Pro pro, C<T>* __restrict__ work,
   __syncthreads();
   for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 2
     const int cc = it / Q::n2, l = it % Q::n2;
-    C<T>* sc = s + cc * F * Q::size + (l % n) + Q::pitch * n * (l / n);
+    C<T>* sc = s + cc * F * Q::size + Q::line2(l);
 #pragma unroll
-    for (int f = 0; f < F; ++f) line_dft<n, +1, T>(sc + f * Q::size, Q::pitch);
+    for (int f = 0; f < F; ++f) line_dft<n, +1, T>(sc + f * Q::size, Q::P1);
   }
   __syncthreads();
   for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 3 -> global (natural order)
     const int cc = it / Q::n2, m = it % Q::n2;
-    const C<T>* sc = s + cc * F * Q::size + (m % n) + Q::pitch * (m / n);
+    const C<T>* sc = s + cc * F * Q::size + Q::line3(m);
     const long long g0 = (col0 + cc) * Q::n3 + m;
 #pragma unroll
     for (int f = 0; f < F; ++f) {
       T re[n], im[n];
 #pragma unroll
       for (int j = 0; j < n; ++j) {
-        const C<T> v = sc[f * Q::size + Q::pitch * n * j];
+        const C<T> v = sc[f * Q::size + Q::P2 * j];
         re[j] = v.x;
         im[j] = v.y;
       }
@@ -291,7 +299,7 @@ template <int n, typename T, int TT, typename TE>
 __global__ void __launch_bounds__(512) k_passB(C<T>* __restrict__ work, const TE* __restrict__ Es, TE escale,
                                               long long NF, Gate gate) {
   if (gate.off()) return;
-  using Q = Cube<n>;
+  using Q = Cube<n, T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C<T>* s = reinterpret_cast<C<T>*>(smem_raw);
   C<T>* w = work + (long long)blockIdx.y * NF;
@@ -309,23 +317,23 @@ __global__ void __launch_bounds__(512) k_passB(C<T>* __restrict__ work, const TE
       im[j] = v.y;
     }
     Dft<n, +1, T>::run(re, im);
-    C<T>* sc = s + t * Q::size + Q::pitch * l;
+    C<T>* sc = s + t * Q::size + Q::line1(l);
 #pragma unroll
     for (int j = 0; j < n; ++j) sc[j] = mk<T>(re[j], im[j]);
   }
   __syncthreads();
   for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 5 (inverse)
     const int t = it / Q::n2, l = it % Q::n2;
-    line_dft<n, +1, T>(s + t * Q::size + (l % n) + Q::pitch * n * (l / n), Q::pitch);
+    line_dft<n, +1, T>(s + t * Q::size + Q::line2(l), Q::P1);
   }
   __syncthreads();
   for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 6: inverse, *E/NF, forward
     const int t = it / Q::n2, m = it % Q::n2;
-    C<T>* sc = s + t * Q::size + (m % n) + Q::pitch * (m / n);
+    C<T>* sc = s + t * Q::size + Q::line3(m);
     T re[n], im[n];
 #pragma unroll
     for (int j = 0; j < n; ++j) {
-      const C<T> v = sc[Q::pitch * n * j];
+      const C<T> v = sc[Q::P2 * j];
       re[j] = v.x;
       im[j] = v.y;
     }
@@ -339,17 +347,17 @@ __global__ void __launch_bounds__(512) k_passB(C<T>* __restrict__ work, const TE
     }
     Dft<n, -1, T>::run(re, im);
 #pragma unroll
-    for (int j = 0; j < n; ++j) sc[Q::pitch * n * j] = mk<T>(re[j], im[j]);
+    for (int j = 0; j < n; ++j) sc[Q::P2 * j] = mk<T>(re[j], im[j]);
   }
   __syncthreads();
   for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 5 (forward)
     const int t = it / Q::n2, l = it % Q::n2;
-    line_dft<n, -1, T>(s + t * Q::size + (l % n) + Q::pitch * n * (l / n), Q::pitch);
+    line_dft<n, -1, T>(s + t * Q::size + Q::line2(l), Q::P1);
   }
   __syncthreads();
   for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 4 (forward) to global
     const int t = it % TT, l = it / TT;
-    const C<T>* sc = s + t * Q::size + Q::pitch * l;
+    const C<T>* sc = s + t * Q::size + Q::line1(l);
     T re[n], im[n];
 #pragma unroll
     for (int j = 0; j < n; ++j) {
@@ -374,7 +382,7 @@ __global__ void __launch_bounds__(512) k_passB(C<T>* __restrict__ work, const TE
 template <int n, typename T, int F, int G, class Epi>
 __global__ void __launch_bounds__(512) k_passC(Epi epi, const C<T>* __restrict__ work, long long NF, Gate gate) {
   if (gate.off()) return;
-  using Q = Cube<n>;
+  using Q = Cube<n, T>;
   using A = typename Epi::Acc;
   constexpr int K = Epi::K;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -384,7 +392,7 @@ __global__ void __launch_bounds__(512) k_passC(Epi epi, const C<T>* __restrict__
   for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 3 from global
     const int cc = it / Q::n2, m = it % Q::n2;
     const long long g0 = (col0 + cc) * Q::n3 + m;
-    C<T>* sc = s + cc * F * Q::size + (m % n) + Q::pitch * (m / n);
+    C<T>* sc = s + cc * F * Q::size + Q::line3(m);
 #pragma unroll
     for (int f = 0; f < F; ++f) {
       T re[n], im[n];
@@ -396,15 +404,15 @@ __global__ void __launch_bounds__(512) k_passC(Epi epi, const C<T>* __restrict__
       }
       Dft<n, -1, T>::run(re, im);
 #pragma unroll
-      for (int j = 0; j < n; ++j) sc[f * Q::size + Q::pitch * n * j] = mk<T>(re[j], im[j]);
+      for (int j = 0; j < n; ++j) sc[f * Q::size + Q::P2 * j] = mk<T>(re[j], im[j]);
     }
   }
   __syncthreads();
   for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 2
     const int cc = it / Q::n2, l = it % Q::n2;
-    C<T>* sc = s + cc * F * Q::size + (l % n) + Q::pitch * n * (l / n);
+    C<T>* sc = s + cc * F * Q::size + Q::line2(l);
 #pragma unroll
-    for (int f = 0; f < F; ++f) line_dft<n, -1, T>(sc + f * Q::size, Q::pitch);
+    for (int f = 0; f < F; ++f) line_dft<n, -1, T>(sc + f * Q::size, Q::P1);
   }
   __syncthreads();
   Red<A, (K > 0 ? K : 1)> acc;
@@ -413,7 +421,7 @@ __global__ void __launch_bounds__(512) k_passC(Epi epi, const C<T>* __restrict__
   if constexpr (FieldsInRegs<T, F>::value) {
     for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 1 + epilogue in registers
       const int cc = it / Q::n2, l = it % Q::n2;
-      const C<T>* sc = s + cc * F * Q::size + Q::pitch * l;
+      const C<T>* sc = s + cc * F * Q::size + Q::line1(l);
       const long long cb = (col0 + cc) * Q::n3;
       T re[F][n], im[F][n];
 #pragma unroll
@@ -437,7 +445,7 @@ __global__ void __launch_bounds__(512) k_passC(Epi epi, const C<T>* __restrict__
   } else {
     for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 1 in shared memory
       const int cc = it / Q::n2, l = it % Q::n2;
-      C<T>* sc = s + cc * F * Q::size + Q::pitch * l;
+      C<T>* sc = s + cc * F * Q::size + Q::line1(l);
 #pragma unroll
       for (int f = 0; f < F; ++f) line_dft<n, -1, T>(sc + f * Q::size, 1);
     }
@@ -448,9 +456,147 @@ __global__ void __launch_bounds__(512) k_passC(Epi epi, const C<T>* __restrict__
       const long long cb = (col0 + cc) * Q::n3;
       C<T> v[F];
 #pragma unroll
-      for (int f = 0; f < F; ++f) v[f] = s[(cc * F + f) * Q::size + i1 + Q::pitch * l];
+      for (int f = 0; f < F; ++f) v[f] = s[(cc * F + f) * Q::size + i1 + Q::line1(l)];
       epi.store(cb + q, cb + i1 + (long long)n * l, v, acc);
     }
+  }
+  if constexpr (K > 0) {
+    grid_sum_finalize<A, K>(acc, epi.partials, epi.counter, [&](const Red<A, K>& tot) { epi.finalize(tot); });
+  }
+}
+
+// ------------------------------------------------- linear-field chains
+// Operators whose fields are linear in one vector, field_f(i) = a_f(i) u(i),
+// and whose result is out(i) = S(i, sum_f b_f(i) v_f(i)) -- every Mhat chain
+// (exp1/apply_Mhat_C_scalar_compact.m:8-21) is of this form.  Passes A and C
+// then run the F fields one after another through a single shared-memory cube
+// per column, holding one line of u (pass A) or of the running sum (pass C) in
+// registers: a third of the shared memory and far fewer registers than the
+// general chain.  One line per thread (blockDim >= G*n^2).
+//
+// LinPro:  C<T> load(ia, in, Ext&)   u(i) (pure loads; stores deferred to commit)
+//          void commit(ia, in, const Ext&)
+//          C<T> coef(f, ia, in)      a_f(i) (a_0 == 1 when unit0)
+// LinEpi:  C<T> coef(f, ia, in)      b_f(i) (b_0 == 1 when unit0)
+//          void store(ia, in, C<T> s, Red<Acc,K>& acc), finalize(tot)
+template <int n, typename T, int F, int G, class Pro>
+__global__ void __launch_bounds__(512) k_passA_lin(Pro pro, C<T>* __restrict__ work, long long NF, Gate gate) {
+  if (gate.off()) return;
+  using Q = Cube<n, T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C<T>* s = reinterpret_cast<C<T>*>(smem_raw);
+  const long long col0 = (long long)blockIdx.x * G;
+  constexpr int items = G * Q::n2;
+  const int it = threadIdx.x;
+  const bool act = it < items;
+  const int cc = act ? it / Q::n2 : 0, l = act ? it % Q::n2 : 0;
+  const long long cb = (col0 + cc) * Q::n3;
+  C<T> u[n];
+  if (act) {
+    typename Pro::Ext e[n];
+#pragma unroll
+    for (int j = 0; j < n; ++j) u[j] = pro.load(cb + l + Q::n2 * j, cb + j + (long long)n * l, e[j]);
+#pragma unroll
+    for (int j = 0; j < n; ++j) pro.commit(cb + l + Q::n2 * j, cb + j + (long long)n * l, e[j]);
+  }
+#pragma unroll 1
+  for (int f = 0; f < F; ++f) {
+    if (act) {  // axis 1 in registers
+      T re[n], im[n];
+#pragma unroll
+      for (int j = 0; j < n; ++j) {
+        C<T> v = u[j];
+        if (!(Pro::unit0 && f == 0)) v = cmul<T>(pro.coef(f, cb + l + Q::n2 * j, cb + j + (long long)n * l), v);
+        re[j] = v.x;
+        im[j] = v.y;
+      }
+      Dft<n, +1, T>::run(re, im);
+      C<T>* sc = s + cc * Q::size + Q::line1(l);
+#pragma unroll
+      for (int j = 0; j < n; ++j) sc[j] = mk<T>(re[j], im[j]);
+    }
+    __syncthreads();
+    if (act) line_dft<n, +1, T>(s + cc * Q::size + Q::line2(l), Q::P1);  // axis 2
+    __syncthreads();
+    if (act) {  // axis 3 -> work (natural order), thread <-> m = i1 + n*i2
+      const C<T>* sc = s + cc * Q::size + Q::line3(l);
+      T re[n], im[n];
+#pragma unroll
+      for (int j = 0; j < n; ++j) {
+        const C<T> v = sc[Q::P2 * j];
+        re[j] = v.x;
+        im[j] = v.y;
+      }
+      Dft<n, +1, T>::run(re, im);
+      C<T>* wf = work + f * NF + cb + l;
+#pragma unroll
+      for (int j = 0; j < n; ++j) wf[(long long)Q::n2 * j] = mk<T>(re[j], im[j]);
+    }
+    __syncthreads();
+  }
+}
+
+template <int n, typename T, int F, int G, class Epi>
+__global__ void __launch_bounds__(512) k_passC_lin(Epi epi, const C<T>* __restrict__ work, long long NF, Gate gate) {
+  if (gate.off()) return;
+  using Q = Cube<n, T>;
+  using A = typename Epi::Acc;
+  constexpr int K = Epi::K;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C<T>* s = reinterpret_cast<C<T>*>(smem_raw);
+  const long long col0 = (long long)blockIdx.x * G;
+  constexpr int items = G * Q::n2;
+  const int it = threadIdx.x;
+  const bool act = it < items;
+  const int cc = act ? it / Q::n2 : 0, l = act ? it % Q::n2 : 0;
+  const long long cb = (col0 + cc) * Q::n3;
+  C<T> sum[n];
+#pragma unroll
+  for (int j = 0; j < n; ++j) sum[j] = mk<T>(0, 0);
+#pragma unroll 1
+  for (int f = 0; f < F; ++f) {
+    if (act) {  // axis 3 from work (natural order), thread <-> m = i1 + n*i2
+      const C<T>* wf = work + f * NF + cb + l;
+      T re[n], im[n];
+#pragma unroll
+      for (int j = 0; j < n; ++j) {
+        const C<T> v = wf[(long long)Q::n2 * j];
+        re[j] = v.x;
+        im[j] = v.y;
+      }
+      Dft<n, -1, T>::run(re, im);
+      C<T>* sc = s + cc * Q::size + Q::line3(l);
+#pragma unroll
+      for (int j = 0; j < n; ++j) sc[Q::P2 * j] = mk<T>(re[j], im[j]);
+    }
+    __syncthreads();
+    if (act) line_dft<n, -1, T>(s + cc * Q::size + Q::line2(l), Q::P1);  // axis 2
+    __syncthreads();
+    if (act) {  // axis 1 in registers, accumulate b_f v_f
+      const C<T>* sc = s + cc * Q::size + Q::line1(l);
+      T re[n], im[n];
+#pragma unroll
+      for (int j = 0; j < n; ++j) {
+        const C<T> v = sc[j];
+        re[j] = v.x;
+        im[j] = v.y;
+      }
+      Dft<n, -1, T>::run(re, im);
+#pragma unroll
+      for (int j = 0; j < n; ++j) {
+        C<T> v = mk<T>(re[j], im[j]);
+        if (!(Epi::unit0 && f == 0)) v = cmul<T>(epi.coef(f, cb + l + Q::n2 * j, cb + j + (long long)n * l), v);
+        sum[j] = cadd<T>(sum[j], v);
+      }
+    }
+    __syncthreads();
+  }
+  Red<A, (K > 0 ? K : 1)> acc;
+#pragma unroll
+  for (int k = 0; k < (K > 0 ? K : 1); ++k) acc.v[k] = 0;
+  if (act) {
+#pragma unroll
+    for (int j = 0; j < n; ++j) epi.store(cb + l + Q::n2 * j, cb + j + (long long)n * l, sum[j], acc);
   }
   if constexpr (K > 0) {
     grid_sum_finalize<A, K>(acc, epi.partials, epi.counter, [&](const Red<A, K>& tot) { epi.finalize(tot); });

@@ -159,7 +159,7 @@ int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
       // u += dx ; r64 = bhat - Mhat u  (FP64 residual)
       ProResidMhat<double, float, true> pro{c, B.x, F.x};
       EpiResidMhat<double> epi{c, K->bhat, B.r, &st->rho, K->partials, K->counter};
-      FAME_TRY((run_chain<double, 3>(K->n, pro, epi, B.work, K->m->Es64, 1.0, NF, s)));
+      FAME_TRY((run_chain_lin<double, 3>(K->n, pro, epi, B.work, K->m->Es64, 1.0, NF, s)));
       K->stats.massApplies += 3;
       FAME_TRY(read_back(K->ctx, st, &h, sizeof(PcgState)));
       rn2 = h.rho;
@@ -224,11 +224,11 @@ int fame_apply_Mhat_C_scalar_compact(fame_basis* b, fame_mass* m, const void* x,
   cudaStream_t s = b->ctx->stream;
   if (prec == FAME_F64) {
     const MhatCoef<double> c = coef_of<double>(b);
-    return run_chain<double, 3>(b->n, ProMhat<double, false>{c, (const double2*)x}, EpiMhat<double, false>{c, (double2*)y},
+    return run_chain_lin<double, 3>(b->n, ProMhat<double, false>{c, (const double2*)x}, EpiMhat<double, false>{c, (double2*)y},
                                 work, m->Es64, 1.0, b->NF, s);
   }
   const MhatCoef<float> c = coef_of<float>(b);
-  return run_chain<float, 3>(b->n, ProMhat<float, false>{c, (const float2*)x}, EpiMhat<float, false>{c, (float2*)y},
+  return run_chain_lin<float, 3>(b->n, ProMhat<float, false>{c, (const float2*)x}, EpiMhat<float, false>{c, (float2*)y},
                              (float2*)work, m->Es32, 1.0f, b->NF, s);
 }
 

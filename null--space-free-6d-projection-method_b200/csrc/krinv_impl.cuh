@@ -66,12 +66,12 @@ template <typename T> struct OpMhat {
   int matvec(fame_krinv* K, PcgBuf<T>& B, PcgState* st, cudaStream_t s) const {
     ProPcgMhat<T> pro{c, B.p, B.r, st};
     EpiPcgMhat<T> epi{c, B.Ap, B.p, st, reinterpret_cast<T*>(K->partials), K->counter};
-    return run_chain<T, 3>(K->n, pro, epi, B.work, Es, (T)1, K->NF, s, Gate{&st->active});
+    return run_chain_lin<T, 3>(K->n, pro, epi, B.work, Es, (T)1, K->NF, s, Gate{&st->active});
   }
   int resid(fame_krinv* K, PcgBuf<T>& B, const C<T>* b, double* out, cudaStream_t s) const {
     ProResidMhat<T, T, false> pro{c, B.x, nullptr};
     EpiResidMhat<T> epi{c, b, B.r, out, reinterpret_cast<T*>(K->partials), K->counter};
-    return run_chain<T, 3>(K->n, pro, epi, B.work, Es, (T)1, K->NF, s);
+    return run_chain_lin<T, 3>(K->n, pro, epi, B.work, Es, (T)1, K->NF, s);
   }
 };
 
@@ -107,7 +107,7 @@ int pcg_iterate(fame_krinv* K, const Op& op, PcgBuf<T>& B, PcgState* st, int& la
   for (;;) {
     for (int it = 0; it < chunk; ++it) {
       FAME_TRY(op.matvec(K, B, st, s));
-      k_pcg_update<T><<<vec_blocks(nlen), 256, 0, s>>>(B.x, B.r, B.p, B.Ap, nlen, st, partials,
+      k_pcg_update<T><<<upd_blocks(nlen), 256, 0, s>>>(B.x, B.r, B.p, B.Ap, nlen, st, partials,
                                                       K->counter);
       ::fame::count_launch();
     }

@@ -7,6 +7,7 @@
 // queued iterations read PcgState::active and return at once after
 // convergence, so the host checks convergence only every few iterations.
 #pragma once
+#include <algorithm>
 #include "mass_chain.cuh"
 
 namespace fame {
@@ -70,72 +71,88 @@ static __global__ void k_pcg_resume(PcgState* st) {
 // Unless stated otherwise, functors index line-order vectors (ia) and the
 // line-order copies of W1, W2, invC.
 // Mhat x = C^{-1}(M z + W1^* M(W1 z) + W2^* M(W2 z)), z = C^{-1} x
-// (exp1/apply_Mhat_C_scalar_compact.m:8-21): three mass fields per vector.
-template <typename T>
-__device__ __forceinline__ void mhat_fields(const MhatCoef<T>& c, long long i, C<T> x, C<T>* v) {
-  const C<T> z = cscale<T>(x, c.invC[i]);
-  v[0] = z;
-  v[1] = cmul<T>(c.W1[i], z);
-  v[2] = cmul<T>(c.W2[i], z);
-}
-template <typename T>
-__device__ __forceinline__ C<T> mhat_combine(const MhatCoef<T>& c, long long i, const C<T>* v) {
-  C<T> s = cadd<T>(v[0], cadd<T>(cmulc<T>(c.W1[i], v[1]), cmulc<T>(c.W2[i], v[2])));
-  return cscale<T>(s, c.invC[i]);
-}
+// (exp1/apply_Mhat_C_scalar_compact.m:8-21) as a linear-field chain:
+// fields a_f z with a = (1, W1, W2), result C^{-1} sum_f b_f v_f with
+// b = (1, conj W1, conj W2).  Read-only arrays go through the read-only path.
+template <typename T> __device__ __forceinline__ C<T> ldc(const C<T>* p) { return __ldg(p); }
+template <typename T> __device__ __forceinline__ T ldr(const T* p) { return __ldg(p); }
+
+struct NoExt {};
+
+template <typename T> struct MhatLinCoef {
+  MhatCoef<T> c;
+  __device__ __forceinline__ C<T> a(int f, long long i) const { return ldc<T>((f == 1 ? c.W1 : c.W2) + i); }
+  __device__ __forceinline__ C<T> b(int f, long long i) const { return cconj<T>(ldc<T>((f == 1 ? c.W1 : c.W2) + i)); }
+};
 
 // Plain Mhat action; LINE selects line-order (ia) or natural-order (in)
 // vectors and coefficients.
 template <typename T, bool LINE> struct ProMhat {
+  using Ext = NoExt;
+  static constexpr bool unit0 = true;
   MhatCoef<T> c;
   const C<T>* x;
-  __device__ __forceinline__ void load(long long ia, long long in, C<T>* v) const {
+  __device__ __forceinline__ C<T> load(long long ia, long long in, Ext&) const {
     const long long i = LINE ? ia : in;
-    mhat_fields<T>(c, i, x[i], v);
+    return cscale<T>(ldc<T>(x + i), ldr<T>(c.invC + i));
+  }
+  __device__ __forceinline__ void commit(long long, long long, const Ext&) const {}
+  __device__ __forceinline__ C<T> coef(int f, long long ia, long long in) const {
+    return MhatLinCoef<T>{c}.a(f, LINE ? ia : in);
   }
 };
 template <typename T, bool LINE> struct EpiMhat {
   using Acc = T;
   static constexpr int K = 0;
+  static constexpr bool unit0 = true;
   MhatCoef<T> c;
   C<T>* y;
   T* partials = nullptr;
   unsigned* counter = nullptr;
-  __device__ __forceinline__ void store(long long ia, long long in, const C<T>* v, Red<T, 1>&) const {
+  __device__ __forceinline__ C<T> coef(int f, long long ia, long long in) const {
+    return MhatLinCoef<T>{c}.b(f, LINE ? ia : in);
+  }
+  __device__ __forceinline__ void store(long long ia, long long in, C<T> s, Red<T, 1>&) const {
     const long long i = LINE ? ia : in;
-    y[i] = mhat_combine<T>(c, i, v);
+    y[i] = cscale<T>(s, ldr<T>(c.invC + i));
   }
   __device__ __forceinline__ void finalize(const Red<T, 1>&) const {}
 };
 
 // PCG search-direction update fused into the matvec prologue:
-// p = r (first iteration) or p = r + beta p; then the Mhat fields of p.
+// p = r (first iteration) or p = r + beta p (stored after all loads), u = C^{-1} p.
 template <typename T> struct ProPcgMhat {
+  using Ext = C<T>;
+  static constexpr bool unit0 = true;
   MhatCoef<T> c;
   C<T>* p;
   const C<T>* r;
   const PcgState* st;
-  __device__ __forceinline__ void load(long long i, long long, C<T>* v) const {
-    C<T> pi = r[i];
+  __device__ __forceinline__ C<T> load(long long i, long long, Ext& e) const {
+    C<T> pi = ldc<T>(r + i);
     if (st->iter > 0) pi = cadd<T>(pi, cscale<T>(p[i], (T)st->beta));
-    p[i] = pi;
-    mhat_fields<T>(c, i, pi, v);
+    e = pi;
+    return cscale<T>(pi, ldr<T>(c.invC + i));
   }
+  __device__ __forceinline__ void commit(long long i, long long, const Ext& e) const { p[i] = e; }
+  __device__ __forceinline__ C<T> coef(int f, long long i, long long) const { return MhatLinCoef<T>{c}.a(f, i); }
 };
 // Ap = Mhat p and the reduction p^H Ap -> alpha = rho / p^H Ap.
 template <typename T> struct EpiPcgMhat {
   using Acc = T;
   static constexpr int K = 2;
+  static constexpr bool unit0 = true;
   MhatCoef<T> c;
   C<T>* Ap;
   const C<T>* p;
   PcgState* st;
   T* partials;
   unsigned* counter;
-  __device__ __forceinline__ void store(long long i, long long, const C<T>* v, Red<T, 2>& acc) const {
-    const C<T> ap = mhat_combine<T>(c, i, v);
+  __device__ __forceinline__ C<T> coef(int f, long long i, long long) const { return MhatLinCoef<T>{c}.b(f, i); }
+  __device__ __forceinline__ void store(long long i, long long, C<T> s, Red<T, 2>& acc) const {
+    const C<T> ap = cscale<T>(s, ldr<T>(c.invC + i));
     Ap[i] = ap;
-    const C<T> d = cmulc<T>(p[i], ap);
+    const C<T> d = cmulc<T>(ldc<T>(p + i), ap);
     acc.v[0] += d.x;
     acc.v[1] += d.y;
   }
@@ -147,29 +164,35 @@ template <typename T> struct EpiPcgMhat {
 // r = b - Mhat x with ||r||^2 into *out (true residual / refinement residual).
 // With ADDX, the prologue first forms x = x + dx (dx in lower precision).
 template <typename T, typename TD, bool ADDX> struct ProResidMhat {
+  using Ext = C<T>;
+  static constexpr bool unit0 = true;
   MhatCoef<T> c;
   C<T>* x;
   const C<TD>* dx;
-  __device__ __forceinline__ void load(long long i, long long, C<T>* v) const {
+  __device__ __forceinline__ C<T> load(long long i, long long, Ext& e) const {
     C<T> xi = x[i];
-    if (ADDX) {
-      xi = cadd<T>(xi, ccast<T, TD>(dx[i]));
-      x[i] = xi;
-    }
-    mhat_fields<T>(c, i, xi, v);
+    if (ADDX) xi = cadd<T>(xi, ccast<T, TD>(ldc<TD>(dx + i)));
+    e = xi;
+    return cscale<T>(xi, ldr<T>(c.invC + i));
   }
+  __device__ __forceinline__ void commit(long long i, long long, const Ext& e) const {
+    if (ADDX) x[i] = e;
+  }
+  __device__ __forceinline__ C<T> coef(int f, long long i, long long) const { return MhatLinCoef<T>{c}.a(f, i); }
 };
 template <typename T> struct EpiResidMhat {
   using Acc = T;
   static constexpr int K = 1;
+  static constexpr bool unit0 = true;
   MhatCoef<T> c;
   const C<T>* b;
   C<T>* r;
   double* out;
   T* partials;
   unsigned* counter;
-  __device__ __forceinline__ void store(long long i, long long, const C<T>* v, Red<T, 1>& acc) const {
-    const C<T> ri = csub<T>(b[i], mhat_combine<T>(c, i, v));
+  __device__ __forceinline__ C<T> coef(int f, long long i, long long) const { return MhatLinCoef<T>{c}.b(f, i); }
+  __device__ __forceinline__ void store(long long i, long long, C<T> s, Red<T, 1>& acc) const {
+    const C<T> ri = csub<T>(ldc<T>(b + i), cscale<T>(s, ldr<T>(c.invC + i)));
     r[i] = ri;
     acc.v[0] += cabs2<T>(ri);
   }
@@ -259,16 +282,41 @@ inline int vec_blocks(long long n) { return (int)std::min<long long>((n + 255) /
 constexpr int kVecBlocksMax = 148 * 8;
 
 // x += alpha p; r -= alpha Ap; rho = r^H r; convergence bookkeeping.
+// Four independent elements per thread, all loads issued before the stores.
+constexpr int kUpdUnroll = 4;
+inline int upd_blocks(long long n) {
+  return (int)std::max<long long>(1, std::min<long long>((n + 256LL * kUpdUnroll - 1) / (256LL * kUpdUnroll), 148 * 8));
+}
 template <typename T>
-__global__ void __launch_bounds__(256) k_pcg_update(C<T>* x, C<T>* r, const C<T>* p, const C<T>* Ap,
-                                                   long long n, PcgState* st, T* partials,
-                                                   unsigned* counter) {
+__global__ void __launch_bounds__(256) k_pcg_update(C<T>* x, C<T>* r, const C<T>* __restrict__ p,
+                                                   const C<T>* __restrict__ Ap, long long n, PcgState* st,
+                                                   T* partials, unsigned* counter) {
   if (*((volatile int*)&st->active) == 0) return;
   const C<T> a = mk<T>((T)st->alpha_re, (T)st->alpha_im);
   Red<T, 1> acc;
   acc.v[0] = 0;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  for (; i + (kUpdUnroll - 1) * stride < n; i += kUpdUnroll * stride) {
+    C<T> xv[kUpdUnroll], rv[kUpdUnroll], pv[kUpdUnroll], av[kUpdUnroll];
+#pragma unroll
+    for (int k = 0; k < kUpdUnroll; ++k) {
+      const long long ik = i + k * stride;
+      xv[k] = x[ik];
+      rv[k] = r[ik];
+      pv[k] = __ldg(p + ik);
+      av[k] = __ldg(Ap + ik);
+    }
+#pragma unroll
+    for (int k = 0; k < kUpdUnroll; ++k) {
+      const long long ik = i + k * stride;
+      x[ik] = cadd<T>(xv[k], cmul<T>(a, pv[k]));
+      const C<T> ri = csub<T>(rv[k], cmul<T>(a, av[k]));
+      r[ik] = ri;
+      acc.v[0] += cabs2<T>(ri);
+    }
+  }
+  for (; i < n; i += stride) {
     x[i] = cadd<T>(x[i], cmul<T>(a, p[i]));
     const C<T> ri = csub<T>(r[i], cmul<T>(a, Ap[i]));
     r[i] = ri;

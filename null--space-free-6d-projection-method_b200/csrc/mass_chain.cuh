@@ -18,7 +18,7 @@ template <typename K> int ensure_smem(K kernel, size_t bytes) {
 
 template <int n, typename T, typename TE>
 int launch_passB(C<T>* work, int nfields, const TE* Es, TE escale, long long NF, cudaStream_t st, Gate gate) {
-  using Q = Cube<n>;
+  using Q = Cube<n, T>;
   constexpr int TT = PassBTile<T>::TT;
   static_assert(Q::n3 % TT == 0, "tile must divide n^3");
   const size_t smem = (size_t)TT * Q::size * sizeof(C<T>);
@@ -33,7 +33,7 @@ int launch_passB(C<T>* work, int nfields, const TE* Es, TE escale, long long NF,
 
 template <int n, typename T, int F, class Pro>
 int launch_passA(const Pro& pro, C<T>* work, long long NF, cudaStream_t st, Gate gate) {
-  using Q = Cube<n>;
+  using Q = Cube<n, T>;
   constexpr int G = PassACols<n, T>::value;
   const size_t smem = (size_t)G * F * Q::size * sizeof(C<T>);
   static int attr = ensure_smem(k_passA<n, T, F, G, Pro>, smem);
@@ -46,7 +46,7 @@ int launch_passA(const Pro& pro, C<T>* work, long long NF, cudaStream_t st, Gate
 
 template <int n, typename T, int F, class Epi>
 int launch_passC(const Epi& epi, const C<T>* work, long long NF, cudaStream_t st, Gate gate) {
-  using Q = Cube<n>;
+  using Q = Cube<n, T>;
   constexpr int G = PassACols<n, T>::value;
   const size_t smem = (size_t)G * F * Q::size * sizeof(C<T>);
   static int attr = ensure_smem(k_passC<n, T, F, G, Epi>, smem);
@@ -82,6 +82,48 @@ int run_chain(int n, const Pro& pro, const Epi& epi, C<T>* work, const TE* Es, T
     case 10: return chain_n<10, T, F>(pro, epi, work, Es, escale, NF, st, gate);
     case 12: return chain_n<12, T, F>(pro, epi, work, Es, escale, NF, st, gate);
     case 14: return chain_n<14, T, F>(pro, epi, work, Es, escale, NF, st, gate);
+    default: return fail(FAME_ERR_UNSUPPORTED, "mass operator supports 2N in {2,4,...,14}");
+  }
+}
+
+// Columns per CTA of the linear-field passes (one line per thread).
+template <int n, typename T> struct LinCols {
+  static constexpr int value = n == 2 ? 8 : n == 4 ? 16 : n == 6 ? 12 : n == 8 ? 8 : n == 10 ? 4 : n == 12 ? 2 : 2;
+  static_assert((n * n * n) % value == 0 && value * n * n <= 512, "linear chain tiling");
+};
+
+template <int n, typename T, int F, class Pro, class Epi, typename TE>
+int chain_lin_n(const Pro& pro, const Epi& epi, C<T>* work, const TE* Es, TE escale, long long NF,
+                cudaStream_t st, Gate gate) {
+  using Q = Cube<n, T>;
+  constexpr int G = LinCols<n, T>::value;
+  const size_t smem = (size_t)G * Q::size * sizeof(C<T>);
+  const int threads = round32(G * Q::n2);
+  static int attrA = ensure_smem(k_passA_lin<n, T, F, G, Pro>, smem);
+  static int attrC = ensure_smem(k_passC_lin<n, T, F, G, Epi>, smem);
+  if (attrA != FAME_OK) return attrA;
+  if (attrC != FAME_OK) return attrC;
+  k_passA_lin<n, T, F, G, Pro><<<Q::n3 / G, threads, smem, st>>>(pro, work, NF, gate);
+  ::fame::count_launch();
+  FAME_TRY((launch_passB<n, T, TE>(work, F, Es, escale, NF, st, gate)));
+  k_passC_lin<n, T, F, G, Epi><<<Q::n3 / G, threads, smem, st>>>(epi, work, NF, gate);
+  ::fame::count_launch();
+  FAME_CUDA_TRY(cudaGetLastError());
+  return FAME_OK;
+}
+
+// Linear-field chain (see k_passA_lin) for axis length n in {2,4,...,14}.
+template <typename T, int F, class Pro, class Epi, typename TE>
+int run_chain_lin(int n, const Pro& pro, const Epi& epi, C<T>* work, const TE* Es, TE escale,
+                  long long NF, cudaStream_t st, Gate gate = Gate{nullptr}) {
+  switch (n) {
+    case 2: return chain_lin_n<2, T, F>(pro, epi, work, Es, escale, NF, st, gate);
+    case 4: return chain_lin_n<4, T, F>(pro, epi, work, Es, escale, NF, st, gate);
+    case 6: return chain_lin_n<6, T, F>(pro, epi, work, Es, escale, NF, st, gate);
+    case 8: return chain_lin_n<8, T, F>(pro, epi, work, Es, escale, NF, st, gate);
+    case 10: return chain_lin_n<10, T, F>(pro, epi, work, Es, escale, NF, st, gate);
+    case 12: return chain_lin_n<12, T, F>(pro, epi, work, Es, escale, NF, st, gate);
+    case 14: return chain_lin_n<14, T, F>(pro, epi, work, Es, escale, NF, st, gate);
     default: return fail(FAME_ERR_UNSUPPORTED, "mass operator supports 2N in {2,4,...,14}");
   }
 }

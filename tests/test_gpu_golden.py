@@ -1,0 +1,54 @@
+"""GPU vs the committed golden fixtures (the oracle's frozen outputs)."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+G = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load(name):
+    return dict(np.load(os.path.join(G, name + ".npz")))
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def test_mass_vs_fixture(cuda_device):
+    import fame_b200 as F
+    d = load("mass_n2")
+    m = F.MassBackend(torch.as_tensor(d["E"], device=cuda_device), 2)
+    y = m.MscalarOp(torch.as_tensor(d["x"], device=cuda_device)).cpu().numpy()
+    assert rel(y, d["y"]) < 1e-13
+    y32 = m.MscalarOp(torch.as_tensor(d["x"], device=cuda_device).to(torch.complex64)).cpu().numpy()
+    assert rel(y32, d["y"]) < 2e-6
+
+
+def test_basis_vs_fixture(cuda_device):
+    import fame_b200 as F
+    d = load("basis_n2_golden")
+    m = F.MassBackend(F.configs.material_separable_cos(2, device=cuda_device), 2)
+    s = F.build_q_system(m, F.configs.P_GOLDEN, F.configs.Q_BASELINE)
+    np.testing.assert_allclose(s.kLift, d["kLift"], rtol=1e-14, atol=1e-16)
+    for k in ("V11", "V12", "V21", "V22", "V31", "V32", "detV1", "W1", "W2"):
+        assert rel(getattr(s, k).cpu().numpy(), d[k]) < 1e-10, k
+    assert rel(s.invCorthDiag.cpu().numpy(), d["invC"]) < 1e-12
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_krinv_and_eigs_vs_fixture(cuda_device, precision):
+    import fame_b200 as F
+    dk, de = load("krinv_n2_tracking"), load("eigs")
+    m = F.MassBackend(torch.as_tensor(load("mass_n2")["E"], device=cuda_device), 2)
+    s = F.build_q_system(m, F.configs.P_REFERENCE, F.configs.Q_TRACKING)
+    op, _ = F.make_explicit_krinv_compact(s, 1e-12, 3000, precision=precision)
+    y = op(torch.as_tensor(dk["b"], device=cuda_device)).cpu().numpy()
+    assert rel(y, dk["y"]) < 1e-10
+    v0 = F.start_vector(F.configs.SEED, s.nr)
+    _, theta, _, info = F.Lanczos(op, None, None, s.nr, 10, 1e-10, 30, 40, v0)
+    lam = np.sort(1.0 / theta)
+    assert info["converged"]
+    assert np.max(np.abs(lam - de["n2_tracking"]) / de["n2_tracking"]) < 1e-10
