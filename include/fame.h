@@ -142,6 +142,18 @@ FAME_API int fame_basis_get(fame_basis* b, int which, void* dst);
 FAME_API int fame_apply_Mhat_C_scalar_compact(fame_basis* b, fame_mass* m, const void* x, void* y,
                                               int prec);
 
+/* Same action as fame_apply_Mhat_C_scalar_compact, with no device allocation: no
+ * counterpart in the reference.  For callers that cannot let a library allocate
+ * GPU memory (hosts that own all device memory through their own pool, loops that
+ * must not pay the device synchronisation of cudaMalloc/cudaFree).  The three-field
+ * scratch is a static 32 MiB device array held by every GPU that loads this library
+ * until exit, so 3*NF*sizeof(element) must fit: FP32 up to N=5, FP64 up to N=4;
+ * larger sizes return FAME_ERR_INVALID.  The first call on a device looks up the
+ * array's device address (make it before any stream capture).  All calls share the
+ * array: calls that overlap on the GPU (e.g. on different streams) race. */
+FAME_API int fame_apply_Mhat_C_scalar_compact_noalloc(fame_basis* b, fame_mass* m, const void* x,
+                                                      void* y, int prec);
+
 /* ---- K_r^{-1} actions ---- */
 typedef struct {
   int kind;        /* FAME_KRINV_EXPLICIT | FAME_KRINV_NESTED */

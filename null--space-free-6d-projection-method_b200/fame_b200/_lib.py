@@ -87,6 +87,7 @@ SIGNATURES = {
     "fame_lanczos": [P, I, D, I, I, P, C.POINTER(D), P, C.POINTER(fame_lanczos_info)],
     "fame_start_vector": [P, C.c_ulonglong, LL, P],
     "fame_apply_Mhat_C_scalar_compact": [P, P, P, P, I],
+    "fame_apply_Mhat_C_scalar_compact_noalloc": [P, P, P, P, I],
 }
 
 
