@@ -72,8 +72,11 @@ FAME_API long long fame_kernel_launches(void);
 /* ---- context (replaces gpu_initialize / wait_for_gpu: exp1/wait_for_gpu.m:5-11) ---- */
 FAME_API int fame_ctx_create(int device, fame_ctx** out);
 FAME_API int fame_ctx_destroy(fame_ctx* ctx);
-/* stream: a cudaStream_t (NULL = the context's own stream) */
+/* Order all work of the context on `stream` (a cudaStream_t; NULL is the legacy
+ * default stream).  A new context uses its own non-blocking stream. */
 FAME_API int fame_ctx_set_stream(fame_ctx* ctx, void* stream);
+/* Return to the context's own non-blocking stream. */
+FAME_API int fame_ctx_use_own_stream(fame_ctx* ctx);
 FAME_API int fame_ctx_sync(fame_ctx* ctx);
 
 /* ---- 6D Fourier mass operator ---- */
@@ -129,6 +132,8 @@ typedef struct {
   double minQq;        /* min |q_xi|^2 */
   double minAbsDetV1;  /* exp1/build_experiment1_q_system.m:16 */
   double kLift[6];
+  int pivot;           /* component forming the V3 row of the explicit split: 2 as in the
+                          reference, else the largest |q_c| when that V1 block is singular */
 } fame_basis_info;
 FAME_API int fame_basis_info_get(fame_basis* b, fame_basis_info* out);
 /* Export one modewise diagonal into a caller buffer (device):
@@ -170,6 +175,7 @@ typedef struct {
   int maxRefine;     /* mixed: max FP64 refinement steps per solve (20) */
   int checkEvery;    /* PCG iterations queued between host convergence checks (8) */
   int verifyTrueResidual; /* confirm convergence on the true residual, as MATLAB pcg (1) */
+  int useGraphs;     /* replay PCG iterations as captured CUDA graphs (1) */
 } fame_krinv_opts;
 FAME_API int fame_krinv_default_opts(fame_krinv_opts* o);
 FAME_API int fame_krinv_create(fame_basis* b, fame_mass* m, const fame_krinv_opts* o, fame_krinv** out);
@@ -193,6 +199,47 @@ typedef struct {
 FAME_API int fame_krinv_stats_get(fame_krinv* k, fame_krinv_stats* out);
 FAME_API int fame_krinv_stats_reset(fame_krinv* k);
 
+/* Eigenvector recovery, exp2/recover_original_eigenvectors_exp2.m:12-50:
+ * X(:,j) = M^{-1} V Y(:,j) by PCG on diag(M,M,M) (tol, maxit; FAME_PREC_MIXED uses FP64
+ * refinement around FP32 PCG), M-normalised; MX = M X.  Y: 2NF x k, X, MX: 3NF x k
+ * (device, complex128).  iterations/relres: host arrays of k (may be NULL). */
+FAME_API int fame_recover_eigvecs(fame_basis* b, fame_mass* m, const void* Y, int k, double tol,
+                                  int maxit, int prec_mode, void* X, void* MX, int* iterations,
+                                  double* relres);
+/* exp2/compute_fourier_diagnostics_exp2.m:10-19: original-GEVP residual
+ * ||Kx-lam Mx||/(||Kx||+|lam| ||Mx||), divergence ||D0 U0^H Mx||/||Mx||, Rayleigh
+ * quotient, for k columns; lambda and the outputs are host arrays of k. */
+FAME_API int fame_fourier_diagnostics(fame_basis* b, const void* X, const void* MX,
+                                      const double* lambda, int k, double* resGEVP,
+                                      double* divRelative2, double* rayleigh);
+
+/* ---- Yee-field reconstruction (complex128 coefficients, FP64) ---- */
+/* exp2/reconstruct_field_direct_blocked_exp3.m:8-15: u = exp(i R Q^T) c.
+ * coeff: NF; qModes: NF x 3 (column-major); rPoints: M x 3 (column-major); u: M. */
+FAME_API int fame_reconstruct_direct(fame_ctx* ctx, const void* coeff, const double* qModes,
+                                     long long NF, const double* rPoints, long long M, void* u);
+/* The same sum for an axis-block cut matrix P = [diag(d1); diag(d2)] (the basis' P)
+ * and points on the tensor grid xs (nx) x ys (ny) x zs (nz), u ordered x fastest
+ * (the Yee point order of exp2/build_yee_edge_points_plus.m:11-17): three complex
+ * GEMMs against per-axis phase tables.  FAME_ERR_UNSUPPORTED for a dense P. */
+FAME_API int fame_reconstruct_direct_grid(fame_basis* b, const void* coeff, const double* xs, int nx,
+                                          const double* ys, int ny, const double* zs, int nz,
+                                          void* u);
+/* exp2/taylor_on_blocks_exp3.m:8-79 (multi-center Taylor, order p <= 12).  Blocks in
+ * CSR form: point indices blockIds[blockPtr[b] .. blockPtr[b+1]) (0-based, device);
+ * fixedCenter: host 3-vector or NULL (then each block's bounding-box midpoint). */
+FAME_API int fame_taylor_on_blocks(fame_ctx* ctx, const void* coeff, const double* qModes,
+                                   long long NF, const double* rPoints, long long M, int p,
+                                   const long long* blockPtr, const long long* blockIds,
+                                   int nBlocks, const double* fixedCenter, void* u);
+
+/* ---- mass-operator adjoint (no reference function; eigenvalue gradients) ---- */
+/* out[j*nparams + t] = X(:,j)^H (dM/dtheta_t) X(:,j) for the 3-component mass
+ * diag(M,M,M) with dM/dtheta_t = fftn(dEps_t .* ifftn(.)): X 3NF x nmodes (device,
+ * complex128), dEps NF x nparams (device, real, column-major), out host. */
+FAME_API int fame_mass_adjoint(fame_mass* m, const void* X, int nmodes, const double* dEps,
+                               int nparams, double* out);
+
 /* ---- restarted Lanczos on K_r^{-1} (exp2/Lanczos.m:1-148, fncB = fncBinv = I) ---- */
 typedef struct {
   int steps;      /* total Lanczos steps (iter) */
@@ -204,6 +251,16 @@ typedef struct {
 /* n = 2NF; theta: host, k values (descending); Y: device n x k complex128 (may be NULL) */
 FAME_API int fame_lanczos(fame_krinv* k, int nev, double tol, int maxiter, int p, const void* v0,
                  double* theta, void* Y, fame_lanczos_info* info);
+/* Batched Bloch path: solve `count` independent instances (N[i], eps E[i] on the
+ * (2N_i)^6 grid (device), Bloch vector q[3i..3i+2]) for their nev largest theta of
+ * K_r^{-1}, concurrently on one device (one context, stream and host thread per
+ * instance).  theta: host count x nev; info, status: host arrays of count (may be
+ * NULL).  The reference solves Bloch points sequentially (exp4/run_exp4_medium.m:37-109).
+ * Returns the first failing instance's status. */
+FAME_API int fame_solve_batch(int device, int count, const int* N, const double* const* E,
+                              const double* q, const double* P, const fame_krinv_opts* o, int nev,
+                              double tol, int maxiter, int p, unsigned long long seed,
+                              double* theta, fame_lanczos_info* info, int* status);
 /* Start vector of the shared counter-based generator (complex128, device). */
 FAME_API int fame_start_vector(fame_ctx* ctx, unsigned long long seed, long long n, void* v);
 

@@ -118,6 +118,7 @@ int fame_ctx_destroy(fame_ctx* c) {
   cudaStreamSynchronize(c->stream);
   if (c->pinned) cudaFreeHost(c->pinned);
   if (c->ev) cudaEventDestroy(c->ev);
+  if (c->capture) cudaStreamDestroy(c->capture);
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
   return FAME_OK;
@@ -125,7 +126,13 @@ int fame_ctx_destroy(fame_ctx* c) {
 
 int fame_ctx_set_stream(fame_ctx* c, void* stream) {
   if (!c) return fail(FAME_ERR_INVALID, "ctx is NULL");
-  c->stream = stream ? (cudaStream_t)stream : c->own;
+  c->stream = (cudaStream_t)stream;  // NULL: the legacy default stream, as everywhere in CUDA
+  return FAME_OK;
+}
+
+int fame_ctx_use_own_stream(fame_ctx* c) {
+  if (!c) return fail(FAME_ERR_INVALID, "ctx is NULL");
+  c->stream = c->own;
   return FAME_OK;
 }
 

@@ -23,10 +23,12 @@ __device__ __forceinline__ void atomic_min_pos_double(unsigned long long* a, dou
 
 struct BasisArgs {
   int N, n;
+  int piv;  // physical component used as the third block row (V3); V1 = the other two
   long long NF;
   double P[18];  // column-major 6x3
   double k[6];
   double2 *V11, *V21, *V31, *V12, *V22, *V32, *det, *W1, *W2;
+  double2 *P11, *P12, *P21, *P22;  // pivoted V1 block (aliases of V when piv == 2)
   double *invC, *Qq, *q1, *q2, *q3;
   float2 *W1f, *W2f;
   float* invCf;
@@ -87,15 +89,24 @@ __global__ void k_build_basis(BasisArgs a) {
     }
     const double V11 = u11 * sq, V21 = u21 * sq, V31 = u31 * sq;
     const double V12 = u12 * sq, V22 = u22 * sq, V32 = u32 * sq;
-    const double det = V11 * V22 - V12 * V21;
-    // W = V1^{-*} [conj V31; conj V32] (all real for a real cut matrix)
-    const double W1 = (V22 * V31 - V21 * V32) / det;
-    const double W2 = (-V12 * V31 + V11 * V32) / det;
+    // pivoted split: rows ra, rb form V1, row piv forms V3
+    const double Vr[3][2] = {{V11, V12}, {V21, V22}, {V31, V32}};
+    const int ra = a.piv == 0 ? 1 : 0, rb = a.piv == 2 ? 1 : 2;
+    const double A11 = Vr[ra][0], A12 = Vr[ra][1], A21 = Vr[rb][0], A22 = Vr[rb][1];
+    const double B1 = Vr[a.piv][0], B2 = Vr[a.piv][1];
+    const double det = A11 * A22 - A12 * A21;
+    // W = V1^{-*} [conj V3_1; conj V3_2] (all real for a real cut matrix)
+    const double W1 = (A22 * B1 - A21 * B2) / det;
+    const double W2 = (-A12 * B1 + A11 * B2) / det;
     const double invC = 1.0 / sqrt(1.0 + W1 * W1 + W2 * W2);
     a.V11[i] = make_double2(V11, 0.0); a.V21[i] = make_double2(V21, 0.0);
     a.V31[i] = make_double2(V31, 0.0); a.V12[i] = make_double2(V12, 0.0);
     a.V22[i] = make_double2(V22, 0.0); a.V32[i] = make_double2(V32, 0.0);
     a.det[i] = make_double2(det, 0.0);
+    if (a.piv != 2) {
+      a.P11[i] = make_double2(A11, 0.0); a.P12[i] = make_double2(A12, 0.0);
+      a.P21[i] = make_double2(A21, 0.0); a.P22[i] = make_double2(A22, 0.0);
+    }
     a.W1[i] = make_double2(W1, 0.0);
     a.W2[i] = make_double2(W2, 0.0);
     a.invC[i] = invC;
@@ -177,6 +188,39 @@ __global__ void k_solveV1(const double2* x, const double2* V11, const double2* V
     y[2 * n * j + i] = y1;
     y[2 * n * j + n + i] = y2;
   }
+}
+
+// exp2/compute_fourier_diagnostics_exp2.m:10-19 for one column: with
+// K the modewise curl-curl symbol (exp1/assemble_K_and_nullspace_free_basis.m:110-119)
+// accumulate |Kx|^2, |Kx - lam Mx|^2, |Mx|^2, Re x^H Kx, Re x^H Mx, |D0 U0^H Mx|^2.
+__global__ void k_fourier_diag(const double2* X, const double2* MX, const double* q1, const double* q2,
+                               const double* q3, long long NF, double lam, double* partials,
+                               unsigned* counter, double* out) {
+  Red<double, 6> acc{};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < NF;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double a = q1[i], b = q2[i], c = q3[i];
+    const double2 x1 = X[i], x2 = X[NF + i], x3 = X[2 * NF + i];
+    const double2 m1 = MX[i], m2 = MX[NF + i], m3 = MX[2 * NF + i];
+    const double2 k1 = make_double2((b * b + c * c) * x1.x - a * b * x2.x - a * c * x3.x,
+                                    (b * b + c * c) * x1.y - a * b * x2.y - a * c * x3.y);
+    const double2 k2 = make_double2(-a * b * x1.x + (a * a + c * c) * x2.x - b * c * x3.x,
+                                    -a * b * x1.y + (a * a + c * c) * x2.y - b * c * x3.y);
+    const double2 k3 = make_double2(-a * c * x1.x - b * c * x2.x + (a * a + b * b) * x3.x,
+                                    -a * c * x1.y - b * c * x2.y + (a * a + b * b) * x3.y);
+    acc.v[0] += cabs2<double>(k1) + cabs2<double>(k2) + cabs2<double>(k3);
+    acc.v[1] += cabs2<double>(csub<double>(k1, cscale<double>(m1, lam))) +
+                cabs2<double>(csub<double>(k2, cscale<double>(m2, lam))) +
+                cabs2<double>(csub<double>(k3, cscale<double>(m3, lam)));
+    acc.v[2] += cabs2<double>(m1) + cabs2<double>(m2) + cabs2<double>(m3);
+    acc.v[3] += cmulc<double>(x1, k1).x + cmulc<double>(x2, k2).x + cmulc<double>(x3, k3).x;
+    acc.v[4] += cmulc<double>(x1, m1).x + cmulc<double>(x2, m2).x + cmulc<double>(x3, m3).x;
+    const double2 g = make_double2(a * m1.x + b * m2.x + c * m3.x, a * m1.y + b * m2.y + c * m3.y);
+    acc.v[5] += cabs2<double>(g);
+  }
+  grid_sum_finalize<double, 6>(acc, partials, counter, [&](const Red<double, 6>& t) {
+    for (int k = 0; k < 6; ++k) out[k] = t.v[k];
+  });
 }
 
 inline int ew_blocks(long long tot) { return (int)std::min<long long>((tot + 255) / 256, 148 * 16); }
@@ -275,6 +319,7 @@ int fame_basis_create(fame_ctx* ctx, int N, const double* P, const double* q, fa
 
   fame_basis* b = new fame_basis();
   b->ctx = ctx;
+  std::memcpy(b->P, P, sizeof(b->P));
   b->N = N;
   b->n = 2 * N;
   long long NF = 1;
@@ -309,8 +354,6 @@ int fame_basis_create(fame_ctx* ctx, int N, const double* P, const double* q, fa
     fame_basis_destroy(b);
     return s;
   }
-  BasisReduce init{0x7FF0000000000000ull, 0x7FF0000000000000ull, 0u};  // +inf
-  cudaMemcpyAsync(red, &init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream);
   a.V11 = b->V[0]; a.V21 = b->V[1]; a.V31 = b->V[2];
   a.V12 = b->V[3]; a.V22 = b->V[4]; a.V32 = b->V[5];
   a.det = b->det; a.W1 = b->W1; a.W2 = b->W2;
@@ -319,20 +362,44 @@ int fame_basis_create(fame_ctx* ctx, int N, const double* P, const double* q, fa
   a.W1_l = b->W1_l; a.W2_l = b->W2_l; a.invC_l = b->invC_l;
   a.W1f_l = b->W1f_l; a.W2f_l = b->W2f_l; a.invCf_l = b->invCf_l;
   a.red = red;
-  k_build_basis<<<ew_blocks(NF), 256, 0, ctx->stream>>>(a);
-  ::fame::count_launch();
   BasisReduce h{};
-  s = cudaGetLastError() == cudaSuccess ? read_back(ctx, red, &h, sizeof(h)) : FAME_ERR_CUDA;
+  // the reference splits components (1,2 | 3); when that V1 block is singular for some
+  // mode (q_3 = 0 makes it singular for xi = 0), pivot on the largest |q_c| instead --
+  // K_r = V^* diag(M,M,M)^{-1} V does not depend on the order of the components.
+  int pivots[2] = {2, 0};
+  {
+    double qa[3] = {std::fabs(q[0]), std::fabs(q[1]), std::fabs(q[2])};
+    pivots[1] = qa[0] >= qa[1] ? (qa[0] >= qa[2] ? 0 : 2) : (qa[1] >= qa[2] ? 1 : 2);
+  }
+  for (int attempt = 0; attempt < 2 && s == FAME_OK; ++attempt) {
+    a.piv = pivots[attempt];
+    if (attempt == 1) {
+      if (a.piv == 2) break;
+      for (int j = 0; j < 4 && s == FAME_OK; ++j) s = dalloc((void**)&b->Vp[j], NF * sizeof(double2));
+      if (s != FAME_OK) break;
+    }
+    a.P11 = b->Vp[0]; a.P12 = b->Vp[1]; a.P21 = b->Vp[2]; a.P22 = b->Vp[3];
+    BasisReduce init{0x7FF0000000000000ull, 0x7FF0000000000000ull, 0u};  // +inf
+    cudaMemcpyAsync(red, &init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream);
+    k_build_basis<<<ew_blocks(NF), 256, 0, ctx->stream>>>(a);
+    ::fame::count_launch();
+    s = cudaGetLastError() == cudaSuccess ? read_back(ctx, red, &h, sizeof(h)) : fail(FAME_ERR_CUDA, "basis kernel launch");
+    double md;
+    std::memcpy(&md, &h.minAbsDet, 8);
+    if (s != FAME_OK || md >= 1e-10) break;
+  }
+  b->pivot = a.piv;
   dfree(red);
   if (s != FAME_OK) {
     fame_basis_destroy(b);
-    return s == FAME_ERR_CUDA ? fail(s, "basis kernel launch") : s;
+    return s;
   }
   double minQq, minDet;
   std::memcpy(&minQq, &h.minQq, 8);
   std::memcpy(&minDet, &h.minAbsDet, 8);
   b->info.NF = NF;
   b->info.N = N;
+  b->info.pivot = b->pivot;
   b->info.nsingular = (int)h.nsingular;
   b->info.minQq = minQq;
   b->info.minAbsDetV1 = minDet;
@@ -357,8 +424,41 @@ int fame_basis_destroy(fame_basis* b) {
   dfree(b->W1_l); dfree(b->W2_l); dfree(b->invC_l);
   dfree(b->W1f_l); dfree(b->W2f_l); dfree(b->invCf_l);
   dfree(b->work);
+  for (int j = 0; j < 4; ++j) dfree(b->Vp[j]);
   delete b;
   return FAME_OK;
+}
+
+int fame_fourier_diagnostics(fame_basis* b, const void* X, const void* MX, const double* lambda, int k,
+                             double* resGEVP, double* divRelative2, double* rayleigh) {
+  if (!b || !X || !MX || !lambda || k < 0) return fail(FAME_ERR_INVALID, "fame_fourier_diagnostics arguments");
+  const long long NF = b->NF;
+  const int blocks = ew_blocks(NF);
+  double* buf = nullptr;
+  unsigned* counter = nullptr;
+  FAME_TRY(dalloc((void**)&buf, (6 * (size_t)blocks + 8) * sizeof(double)));
+  int s = dalloc((void**)&counter, sizeof(unsigned));
+  if (s != FAME_OK) {
+    dfree(buf);
+    return s;
+  }
+  cudaMemsetAsync(counter, 0, sizeof(unsigned), b->ctx->stream);
+  const double eps = 2.220446049250313e-16;
+  for (int j = 0; j < k && s == FAME_OK; ++j) {
+    k_fourier_diag<<<blocks, 256, 0, b->ctx->stream>>>((const double2*)X + 3 * NF * j, (const double2*)MX + 3 * NF * j,
+                                                       b->q[0], b->q[1], b->q[2], NF, lambda[j], buf + 8, counter, buf);
+    ::fame::count_launch();
+    double h[6];
+    s = cudaGetLastError() == cudaSuccess ? read_back(b->ctx, buf, h, sizeof(h)) : fail(FAME_ERR_CUDA, "diagnostics launch");
+    if (s != FAME_OK) break;
+    const double den = std::sqrt(h[0]) + std::fabs(lambda[j]) * std::sqrt(h[2]);
+    if (resGEVP) resGEVP[j] = std::sqrt(h[1]) / std::max(den, eps);
+    if (divRelative2) divRelative2[j] = std::sqrt(h[5]) / std::max(std::sqrt(h[2]), eps);
+    if (rayleigh) rayleigh[j] = h[3] / h[4];
+  }
+  dfree(buf);
+  dfree(counter);
+  return s;
 }
 
 int fame_basis_info_get(fame_basis* b, fame_basis_info* out) {

@@ -1,0 +1,97 @@
+// Batched solves of independent Bloch points of uneven size (BASELINE's
+// batched Bloch path; the reference solves them one after another,
+// exp4/run_exp4_medium.m:37-109).  Each instance gets its own context,
+// stream, mass, basis and K_r^{-1} handles and runs the restarted Lanczos in
+// its own host thread, so the GPU interleaves the kernels of small and large
+// instances; the per-iteration PCG bodies replay captured CUDA graphs.
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+#include "internal.cuh"
+
+using namespace fame;
+
+namespace {
+
+struct BatchJob {
+  int device = 0, N = 0;
+  const double* E = nullptr;
+  double q[3] = {0, 0, 0};
+  const double* P = nullptr;
+  fame_krinv_opts o{};
+  int nev = 0, maxiter = 0, p = 0;
+  double tol = 0;
+  unsigned long long seed = 0;
+  double* theta = nullptr;
+  fame_lanczos_info* info = nullptr;
+  int status = FAME_OK;
+  std::string error;
+};
+
+void run_job(BatchJob* j) {
+  fame_ctx* ctx = nullptr;
+  fame_mass* m = nullptr;
+  fame_basis* b = nullptr;
+  fame_krinv* k = nullptr;
+  void* v0 = nullptr;
+  int s = cudaSetDevice(j->device) == cudaSuccess ? FAME_OK : fail(FAME_ERR_CUDA, "cudaSetDevice");
+  if (s == FAME_OK) s = fame_ctx_create(j->device, &ctx);
+  if (s == FAME_OK) s = fame_mass_create(ctx, j->N, j->E, &m);
+  if (s == FAME_OK) s = fame_basis_create(ctx, j->N, j->P, j->q, &b);
+  if (s == FAME_OK) s = fame_krinv_create(b, m, &j->o, &k);
+  if (s == FAME_OK) s = dalloc(&v0, 2 * (size_t)b->NF * sizeof(double2));
+  if (s == FAME_OK) s = fame_start_vector(ctx, j->seed, 2 * b->NF, v0);
+  if (s == FAME_OK) s = fame_lanczos(k, j->nev, j->tol, j->maxiter, j->p, v0, j->theta, nullptr, j->info);
+  if (s != FAME_OK) j->error = fame_last_error();
+  j->status = s;
+  if (ctx) cudaStreamSynchronize(ctx->stream);
+  dfree(v0);
+  fame_krinv_destroy(k);
+  fame_basis_destroy(b);
+  fame_mass_destroy(m);
+  fame_ctx_destroy(ctx);
+}
+
+}  // namespace
+
+extern "C" int fame_solve_batch(int device, int count, const int* Ns, const double* const* E,
+                                const double* q, const double* P, const fame_krinv_opts* o, int nev,
+                                double tol, int maxiter, int p, unsigned long long seed, double* theta,
+                                fame_lanczos_info* info, int* status) {
+  if (count < 1 || !Ns || !E || !q || !P || !theta || nev < 1)
+    return fail(FAME_ERR_INVALID, "fame_solve_batch arguments");
+  std::vector<BatchJob> jobs(count);
+  for (int i = 0; i < count; ++i) {
+    BatchJob& j = jobs[i];
+    j.device = device;
+    j.N = Ns[i];
+    j.E = E[i];
+    std::memcpy(j.q, q + 3 * i, sizeof(j.q));
+    j.P = P;
+    fame_krinv_default_opts(&j.o);
+    if (o) j.o = *o;
+    j.nev = nev;
+    j.tol = tol;
+    j.maxiter = maxiter;
+    j.p = p;
+    j.seed = seed;
+    j.theta = theta + (size_t)nev * i;
+    j.info = info ? info + i : nullptr;
+  }
+  std::vector<std::thread> threads;
+  threads.reserve(count);
+  for (int i = 0; i < count; ++i) threads.emplace_back(run_job, &jobs[i]);
+  for (auto& t : threads) t.join();
+  int first = FAME_OK;
+  std::string msg;
+  for (int i = 0; i < count; ++i) {
+    if (status) status[i] = jobs[i].status;
+    if (jobs[i].status != FAME_OK && first == FAME_OK) {
+      first = jobs[i].status;
+      msg = "instance " + std::to_string(i) + ": " + jobs[i].error;
+    }
+  }
+  if (first != FAME_OK) return fail(first, msg);
+  return FAME_OK;
+}

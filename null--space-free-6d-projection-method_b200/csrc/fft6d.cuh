@@ -465,6 +465,54 @@ __global__ void __launch_bounds__(512) k_passC(Epi epi, const C<T>* __restrict__
   }
 }
 
+// Inverse-only variant of pass B (axes 4-6, no material), for the mass adjoint.
+template <int n, typename T, int TT>
+__global__ void __launch_bounds__(512) k_passB_inv(C<T>* __restrict__ work, long long NF) {
+  using Q = Cube<n, T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C<T>* s = reinterpret_cast<C<T>*>(smem_raw);
+  C<T>* w = work + (long long)blockIdx.y * NF;
+  const long long c0 = (long long)blockIdx.x * TT;
+  constexpr int items = TT * Q::n2;
+  constexpr long long N3 = Q::n3;
+  for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 4 from global
+    const int t = it % TT, l = it / TT;
+    const C<T>* src = w + c0 + t + N3 * n * l;
+    T re[n], im[n];
+#pragma unroll
+    for (int j = 0; j < n; ++j) {
+      const C<T> v = src[N3 * j];
+      re[j] = v.x;
+      im[j] = v.y;
+    }
+    Dft<n, +1, T>::run(re, im);
+    C<T>* sc = s + t * Q::size + Q::line1(l);
+#pragma unroll
+    for (int j = 0; j < n; ++j) sc[j] = mk<T>(re[j], im[j]);
+  }
+  __syncthreads();
+  for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 5
+    const int t = it / Q::n2, l = it % Q::n2;
+    line_dft<n, +1, T>(s + t * Q::size + Q::line2(l), Q::P1);
+  }
+  __syncthreads();
+  for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 6 -> global
+    const int t = it % TT, m = it / TT;
+    const C<T>* sc = s + t * Q::size + Q::line3(m);
+    T re[n], im[n];
+#pragma unroll
+    for (int j = 0; j < n; ++j) {
+      const C<T> v = sc[Q::P2 * j];
+      re[j] = v.x;
+      im[j] = v.y;
+    }
+    Dft<n, +1, T>::run(re, im);
+    C<T>* dst = w + c0 + t + N3 * m;
+#pragma unroll
+    for (int j = 0; j < n; ++j) dst[N3 * Q::n2 * j] = mk<T>(re[j], im[j]);
+  }
+}
+
 // ------------------------------------------------- linear-field chains
 // Operators whose fields are linear in one vector, field_f(i) = a_f(i) u(i),
 // and whose result is out(i) = S(i, sum_f b_f(i) v_f(i)) -- every Mhat chain

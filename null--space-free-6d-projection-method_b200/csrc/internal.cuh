@@ -7,6 +7,7 @@ struct fame_ctx {
   int device = 0;
   cudaStream_t own = nullptr;
   cudaStream_t stream = nullptr;
+  cudaStream_t capture = nullptr;  // graph-capture stream when `stream` is the context's own
   cudaEvent_t ev = nullptr;
   void* pinned = nullptr;  // small host staging area (4 KB)
   std::vector<void*> allocs;
@@ -36,7 +37,12 @@ struct fame_basis {
   float* invCf_l = nullptr;
   void* work = nullptr;  // scratch of fame_apply_Mhat_C_scalar_compact (3 fields)
   size_t work_bytes = 0;
+  double P[18] = {0};  // cut matrix, column-major 6 x 3
+  int pivot = 2;       // physical component forming the V3 row of the explicit split
+  double2* Vp[4] = {nullptr, nullptr, nullptr, nullptr};  // V1 block when pivot != 2
   fame_basis_info info{};
+  // (r, c) entry of the V1 block of the explicit split (rows = the components other than pivot)
+  const double2* V1(int r, int c) const { return pivot == 2 ? V[r + 3 * c] : Vp[2 * r + c]; }
 };
 
 namespace fame {

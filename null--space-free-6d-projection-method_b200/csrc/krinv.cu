@@ -110,7 +110,7 @@ int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
   const double tolMhat = K->o.tolCG;
   // ---- pre: r = V1^{-*} q ; mr = M r ; bhat ; PCG / refinement init
   {
-    ProKrPre pro{q, bs->V[0], bs->V[3], bs->V[1], bs->V[4], bs->det, NF};
+    ProKrPre pro{q, bs->V1(0, 0), bs->V1(0, 1), bs->V1(1, 0), bs->V1(1, 1), bs->det, NF};
     EpiKrPre epi{c64, K->mr1, K->mr2, K->bhat, B.r, B.x, st, tolMhat,
                  K->o.prec_mode == FAME_PREC_MIXED ? K->o.maxRefine : K->o.maxitCG,
                  K->partials, K->counter};
@@ -174,7 +174,7 @@ int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
   // ---- post: y = V1^{-1}[mr1 + M W1 z ; mr2 + M W2 z]
   {
     ProKrPost pro{c64, B.x};
-    EpiKrPost epi{K->mr1, K->mr2, bs->V[0], bs->V[3], bs->V[1], bs->V[4], bs->det, y, NF, st,
+    EpiKrPost epi{K->mr1, K->mr2, bs->V1(0, 0), bs->V1(0, 1), bs->V1(1, 0), bs->V1(1, 1), bs->det, y, NF, st,
                   K->partials, K->counter};
     FAME_TRY((run_chain<double, 2>(K->n, pro, epi, B.work, K->m->Es64, 1.0, NF, s)));
     K->stats.massApplies += 2;
@@ -248,6 +248,7 @@ int fame_krinv_default_opts(fame_krinv_opts* o) {
   o->maxRefine = 20;
   o->checkEvery = 4;
   o->verifyTrueResidual = 1;
+  o->useGraphs = 1;
   return FAME_OK;
 }
 
@@ -304,6 +305,8 @@ int fame_krinv_destroy(fame_krinv* K) {
   dfree(K->partials); dfree(K->counter); dfree(K->st64); dfree(K->st32);
   nested_free(K);
   lanczos_ws_free(K);
+  for (auto& g : K->graphs)
+    if (g) cudaGraphExecDestroy(g);
   delete K;
   return FAME_OK;
 }
@@ -324,6 +327,34 @@ int fame_krinv_apply(fame_krinv* K, const void* b, void* y, int ncols) {
   auto t1 = std::chrono::steady_clock::now();
   K->stats.totalInverseSeconds += std::chrono::duration<double>(t1 - t0).count();
   return FAME_OK;
+}
+
+int fame_recover_eigvecs(fame_basis* b, fame_mass* m, const void* Y, int k, double tol, int maxit,
+                         int prec_mode, void* X, void* MX, int* iterations, double* relres) {
+  if (!b || !m || !Y || !X || !MX || k < 0) return fail(FAME_ERR_INVALID, "fame_recover_eigvecs arguments");
+  fame_krinv_opts o;
+  fame_krinv_default_opts(&o);
+  o.kind = FAME_KRINV_NESTED;
+  o.prec_mode = prec_mode;
+  o.tolM = tol;
+  o.maxitM = maxit;
+  fame_krinv* K = nullptr;
+  FAME_TRY(fame_krinv_create(b, m, &o, &K));
+  const long long NF = b->NF;
+  int s = FAME_OK;
+  for (int j = 0; j < k && s == FAME_OK; ++j) {
+    int it = 0;
+    double rr = 0.0;
+    s = recover_one(K, (const double2*)Y + 2 * NF * j, (double2*)X + 3 * NF * j, (double2*)MX + 3 * NF * j,
+                    &it, &rr);
+    if (iterations) iterations[j] = it;
+    if (relres) relres[j] = rr;
+    if (s == FAME_OK && rr > 10 * tol)
+      s = fail(FAME_ERR_NOT_CONVERGED, "recover_original_eigenvectors_exp2:RecoveryCGFailure relres=" +
+                                           std::to_string(rr));
+  }
+  fame_krinv_destroy(K);
+  return s;
 }
 
 int fame_krinv_stats_get(fame_krinv* K, fame_krinv_stats* out) {

@@ -41,6 +41,8 @@ struct fame_krinv {
   double* sigma = nullptr;  // |q|^2 (NF), sigma_r = [sigma; sigma]
   fame::OuterState* ost = nullptr;
   void* lanczos_ws = nullptr;  // Lanczos basis workspace reused across solves
+  // CUDA graphs of kGraphIters PCG iterations, one per (precision, operator)
+  cudaGraphExec_t graphs[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
 namespace fame {
@@ -48,6 +50,7 @@ int nested_alloc(fame_krinv* K);
 void nested_free(fame_krinv* K);
 int krinv_nested_apply_one(fame_krinv* K, const double2* b, double2* x);
 void lanczos_ws_free(fame_krinv* K);
+int recover_one(fame_krinv* K, const double2* y, double2* X, double2* MX, int* iters, double* relres);
 template <typename T> MhatCoef<T> coef_of(fame_basis* b);       // natural order
 template <typename T> MhatCoef<T> coef_line_of(fame_basis* b);  // line order
 template <typename T> const T* es_of(fame_mass* m);
@@ -91,6 +94,66 @@ template <typename T> struct OpM3 {
   }
 };
 
+// PCG iterations per captured graph.
+constexpr int kGraphIters = 4;
+
+template <typename T, class Op> constexpr int graph_slot() {
+  return (sizeof(T) == 8 ? 0 : 1) + (Op::nvec == 3 ? 2 : 0);
+}
+
+template <typename T, class Op>
+int enqueue_iterations(fame_krinv* K, const Op& op, PcgBuf<T>& B, PcgState* st, cudaStream_t s, int count) {
+  T* partials = reinterpret_cast<T*>(K->partials);
+  const long long nlen = (long long)Op::nvec * K->NF;
+  for (int it = 0; it < count; ++it) {
+    FAME_TRY(op.matvec(K, B, st, s));
+    k_pcg_update<T><<<upd_blocks(nlen), 256, 0, s>>>(B.x, B.r, B.p, B.Ap, nlen, st, partials, K->counter);
+    ::fame::count_launch();
+  }
+  FAME_CUDA_TRY(cudaGetLastError());
+  return FAME_OK;
+}
+
+// Queue `count` gated PCG iterations: as replays of a captured graph of
+// kGraphIters iterations (count rounded up; surplus iterations are gated
+// off by the device state), or as plain launches before the graph exists.
+template <typename T, class Op>
+int queue_iterations(fame_krinv* K, const Op& op, PcgBuf<T>& B, PcgState* st, int count) {
+  cudaStream_t s = K->ctx->stream;
+  cudaGraphExec_t& ge = K->graphs[graph_slot<T, Op>()];
+  if (!K->o.useGraphs) return enqueue_iterations<T>(K, op, B, st, s, count);
+  if (!ge) {
+    // the first iterations run eagerly (kernel attributes set, modules loaded), then capture
+    FAME_TRY(enqueue_iterations<T>(K, op, B, st, s, kGraphIters));
+    count -= kGraphIters;
+    cudaStream_t cs = K->ctx->own;
+    if (cs == s) {
+      if (!K->ctx->capture) FAME_CUDA_TRY(cudaStreamCreateWithFlags(&K->ctx->capture, cudaStreamNonBlocking));
+      cs = K->ctx->capture;
+    }
+    cudaGraph_t g = nullptr;
+    FAME_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    const int st_enq = enqueue_iterations<T>(K, op, B, st, cs, kGraphIters);
+    const cudaError_t e_end = cudaStreamEndCapture(cs, &g);
+    if (st_enq != FAME_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st_enq;
+    }
+    if (e_end != cudaSuccess) return fail(FAME_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e_end));
+    const cudaError_t e_inst = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    if (e_inst != cudaSuccess) {
+      ge = nullptr;
+      return fail(FAME_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e_inst));
+    }
+  }
+  for (int done = 0; done < count; done += kGraphIters) {
+    FAME_CUDA_TRY(cudaGraphLaunch(ge, s));
+    ::fame::count_launch(4LL * kGraphIters);
+  }
+  return FAME_OK;
+}
+
 // Queue PCG iterations until the device state stops them; the host reads the
 // state once per chunk (the first chunk is sized from the previous solve's
 // iteration count).  With verify, convergence is confirmed on the true
@@ -99,23 +162,15 @@ template <typename T, class Op>
 int pcg_iterate(fame_krinv* K, const Op& op, PcgBuf<T>& B, PcgState* st, int& lastIt, PcgState& h,
                 bool verify, const C<T>* b) {
   cudaStream_t s = K->ctx->stream;
-  T* partials = reinterpret_cast<T*>(K->partials);
-  const long long nlen = (long long)Op::nvec * K->NF;
   const int every = std::max(1, K->o.checkEvery);
   int chunk = lastIt > 4 ? lastIt - 2 : every;
   int queued = 0, moresteps = 0;
   for (;;) {
-    for (int it = 0; it < chunk; ++it) {
-      FAME_TRY(op.matvec(K, B, st, s));
-      k_pcg_update<T><<<upd_blocks(nlen), 256, 0, s>>>(B.x, B.r, B.p, B.Ap, nlen, st, partials,
-                                                      K->counter);
-      ::fame::count_launch();
-    }
-    FAME_CUDA_TRY(cudaGetLastError());
+    FAME_TRY((queue_iterations<T, Op>(K, op, B, st, chunk)));
     queued += chunk;
     FAME_TRY(read_back(K->ctx, st, &h, sizeof(PcgState)));
     if (h.active) {
-      if (queued > h.maxit + 4 * every) return fail(FAME_ERR_CUDA, "PCG state did not stop at maxit");
+      if (queued > h.maxit + 4 * every + kGraphIters) return fail(FAME_ERR_CUDA, "PCG state did not stop at maxit");
       chunk = every;
       continue;
     }

@@ -54,6 +54,40 @@ int mass_scalar_cols(int n, long long NF, const C<T>* x, C<T>* y, int ncols, con
   return FAME_OK;
 }
 
+// out[t] = (1/NF) sum_y g_t(y) sum_c |w_c(y)|^2, w_c the unnormalised inverse DFT
+// of component c, i.e. NF sum_y g_t(y) sum_c |ifftn(x_c)(y)|^2 = x^H (dM/dtheta_t) x.
+constexpr int kMaxAdjParams = 8;
+__global__ void k_adjoint_reduce(const double2* w, long long NF, const double* g, int np,
+                                 double* partials, unsigned* counter, double* out) {
+  Red<double, kMaxAdjParams> acc{};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < NF; i += (long long)gridDim.x * blockDim.x) {
+    const double d = cabs2<double>(w[i]) + cabs2<double>(w[NF + i]) + cabs2<double>(w[2 * NF + i]);
+#pragma unroll
+    for (int t = 0; t < kMaxAdjParams; ++t)
+      if (t < np) acc.v[t] += g[(long long)t * NF + i] * d;
+  }
+  const double inv = 1.0 / (double)NF;
+  grid_sum_finalize<double, kMaxAdjParams>(acc, partials, counter, [&](const Red<double, kMaxAdjParams>& tot) {
+    for (int t = 0; t < kMaxAdjParams; ++t) out[t] = tot.v[t] * inv;
+  });
+}
+
+template <int n>
+int adjoint_inverse_n(const double2* x, double2* work, long long NF, cudaStream_t st) {
+  using Q = Cube<n, double>;
+  ProCols<double, 3> pro;
+  for (int c = 0; c < 3; ++c) pro.x[c] = x + c * NF;
+  FAME_TRY((launch_passA<n, double, 3>(pro, work, NF, st, Gate{nullptr})));
+  constexpr int TT = PassBTile<double>::TT;
+  const size_t smem = (size_t)TT * Q::size * sizeof(double2);
+  static int attr = ensure_smem(k_passB_inv<n, double, TT>, smem);
+  if (attr != FAME_OK) return attr;
+  k_passB_inv<n, double, TT><<<dim3(Q::n3 / TT, 3), std::min(512, std::max(64, round32(TT * Q::n2))), smem, st>>>(work, NF);
+  ::fame::count_launch();
+  FAME_CUDA_TRY(cudaGetLastError());
+  return FAME_OK;
+}
+
 int check_N(int N) {
   if (N < 1 || N > 7) return fail(FAME_ERR_UNSUPPORTED, "N must be in [1,7] (2N <= 14)");
   return FAME_OK;
@@ -156,6 +190,45 @@ int fame_mass_apply(fame_mass* m, int mode, const void* x, void* y, int nrhs, in
   if (prec == FAME_F64) return mass_apply_typed<double>(m, mode, (const double2*)x, (double2*)y, nrhs);
   if (prec == FAME_F32) return mass_apply_typed<float>(m, mode, (const float2*)x, (float2*)y, nrhs);
   return fail(FAME_ERR_INVALID, "prec must be FAME_F64 or FAME_F32");
+}
+
+int fame_mass_adjoint(fame_mass* m, const void* X, int nmodes, const double* dEps, int nparams,
+                      double* out) {
+  if (!m || !X || !dEps || !out || nmodes < 0 || nparams < 1 || nparams > kMaxAdjParams)
+    return fail(FAME_ERR_INVALID, "fame_mass_adjoint arguments (1 <= nparams <= 8)");
+  const long long NF = m->NF;
+  cudaStream_t st = m->ctx->stream;
+  double2* work = nullptr;
+  double* red = nullptr;
+  unsigned* counter = nullptr;
+  const int blocks = (int)std::min<long long>((NF + 255) / 256, 148 * 8);
+  int s = dalloc((void**)&work, 3 * NF * sizeof(double2));
+  if (s == FAME_OK) s = dalloc((void**)&red, ((size_t)blocks * kMaxAdjParams + kMaxAdjParams) * sizeof(double));
+  if (s == FAME_OK) s = dalloc((void**)&counter, sizeof(unsigned));
+  if (s == FAME_OK) cudaMemsetAsync(counter, 0, sizeof(unsigned), st);
+  for (int j = 0; j < nmodes && s == FAME_OK; ++j) {
+    const double2* xj = (const double2*)X + 3 * NF * j;
+    switch (m->n) {
+      case 2: s = adjoint_inverse_n<2>(xj, work, NF, st); break;
+      case 4: s = adjoint_inverse_n<4>(xj, work, NF, st); break;
+      case 6: s = adjoint_inverse_n<6>(xj, work, NF, st); break;
+      case 8: s = adjoint_inverse_n<8>(xj, work, NF, st); break;
+      case 10: s = adjoint_inverse_n<10>(xj, work, NF, st); break;
+      case 12: s = adjoint_inverse_n<12>(xj, work, NF, st); break;
+      case 14: s = adjoint_inverse_n<14>(xj, work, NF, st); break;
+      default: s = fail(FAME_ERR_UNSUPPORTED, "adjoint: unsupported N");
+    }
+    if (s != FAME_OK) break;
+    k_adjoint_reduce<<<blocks, 256, 0, st>>>(work, NF, dEps, nparams, red + kMaxAdjParams, counter, red);
+    ::fame::count_launch();
+    double h[kMaxAdjParams];
+    s = cudaGetLastError() == cudaSuccess ? read_back(m->ctx, red, h, sizeof(h)) : fail(FAME_ERR_CUDA, "adjoint launch");
+    for (int t = 0; t < nparams && s == FAME_OK; ++t) out[(size_t)j * nparams + t] = h[t];
+  }
+  dfree(work);
+  dfree(red);
+  dfree(counter);
+  return s;
 }
 
 int fame_applyMij_rank1_exact(fame_mass* m, const uint32_t* inputIdx, const uint32_t* targetIdx,

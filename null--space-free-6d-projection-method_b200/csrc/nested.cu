@@ -298,6 +298,83 @@ int krinv_nested_apply_one(fame_krinv* K, const double2* b, double2* x) {
   return FAME_OK;
 }
 
+// ---------------------------------------------------------------- recovery
+// x (3NF, line order) -> M3 x written in natural order, x^H M3 x -> *out
+struct ProM3x {
+  const double2* x;
+  long long NF;
+  __device__ __forceinline__ void load(long long ia, long long, double2* v) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) v[c] = x[c * NF + ia];
+  }
+};
+struct EpiM3Norm {
+  using Acc = double;
+  static constexpr int K = 1;
+  const double2* x;
+  double2* MX;
+  long long NF;
+  double* out;
+  double* partials;
+  unsigned* counter;
+  __device__ __forceinline__ void store(long long ia, long long in, const double2* v, Red<double, 1>& acc) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      MX[c * NF + in] = v[c];
+      const double2 d = cmulc<double>(x[c * NF + ia], v[c]);
+      acc.v[0] += d.x;
+    }
+  }
+  __device__ __forceinline__ void finalize(const Red<double, 1>& t) const { *out = t.v[0]; }
+};
+
+// X = x / sqrt(n2) (x line order -> X natural), MX /= sqrt(n2)
+__global__ void k_recover_scale(const double2* x, double2* X, double2* MX, long long NF, int n,
+                                const double* n2) {
+  const double s = 1.0 / sqrt(*n2);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < NF; i += (long long)gridDim.x * blockDim.x) {
+    const long long il = line_index(i, n);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      X[c * NF + i] = cscale<double>(x[c * NF + il], s);
+      MX[c * NF + i] = cscale<double>(MX[c * NF + i], s);
+    }
+  }
+}
+
+int recover_one(fame_krinv* K, const double2* y, double2* X, double2* MX, int* iters, double* relres) {
+  fame_basis* b = K->b;
+  cudaStream_t s = K->ctx->stream;
+  const long long NF = K->NF;
+  PcgBuf<double>& B = K->b64;
+  const long long it0 = K->stats.totalMassIterations;
+  // rhs = V y (line order), then x = M3^{-1} rhs
+  k_inner_init<double><<<nb(NF), 256, 0, s>>>(y, b->V[0], b->V[3], b->V[1], b->V[4], b->V[2], b->V[5],
+                                              NF, K->n, K->bhat, K->st64, K->o.tolM,
+                                              K->o.prec_mode == FAME_PREC_MIXED ? K->o.maxRefine : K->o.maxitM,
+                                              K->partials, K->counter);
+  ::fame::count_launch();
+  k_copy_zero<<<nb(3 * NF), 256, 0, s>>>(K->bhat, B.r, B.x, 3 * NF);
+  ::fame::count_launch();
+  FAME_CUDA_TRY(cudaGetLastError());
+  FAME_TRY(inner_m3_solve(K));
+  PcgState h{};
+  FAME_TRY(read_back(K->ctx, K->st64, &h, sizeof(PcgState)));
+  *iters = (int)(K->stats.totalMassIterations - it0);
+  *relres = h.bnorm2 > 0 ? std::sqrt(h.rho / h.bnorm2) : 0.0;
+  // M x and x^H M x (the mass action the normalisation needs anyway)
+  ProM3x pro{B.x, NF};
+  EpiM3Norm epi{B.x, MX, NF, &K->st64->aux, K->partials, K->counter};
+  FAME_TRY((run_chain<double, 3>(K->n, pro, epi, B.work, K->m->Es64, 1.0, NF, s)));
+  FAME_TRY(read_back(K->ctx, K->st64, &h, sizeof(PcgState)));
+  if (!(h.aux > 0.0) || !std::isfinite(h.aux))
+    return fail(FAME_ERR_NONFINITE, "recover_original_eigenvectors_exp2:BadMassNorm");
+  k_recover_scale<<<nb(NF), 256, 0, s>>>(B.x, X, MX, NF, K->n, &K->st64->aux);
+  ::fame::count_launch();
+  FAME_CUDA_TRY(cudaGetLastError());
+  return FAME_OK;
+}
+
 int nested_alloc(fame_krinv* K) {
   const long long n2 = 2 * K->NF;
   FAME_TRY(dalloc((void**)&K->orr, n2 * sizeof(double2)));

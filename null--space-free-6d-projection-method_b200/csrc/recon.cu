@@ -1,0 +1,413 @@
+// Yee-field reconstruction of a Fourier eigenvector component,
+//   u(r) = sum_j c_j exp(i q_j . r)                (exp2/reconstruct_field_direct_blocked_exp3.m:8-15)
+// and its multi-center Taylor approximation
+//   u(r) ~ sum_{|a|<=p} gamma_a(r_c) (r - r_c)^a,
+//   gamma_a(r_c) = i^|a|/a! sum_j c_j exp(i q_j . r_c) q_j^a   (exp2/taylor_on_blocks_exp3.m:1-79)
+//
+// Three device paths:
+//  * k_direct_sum: the plain sum for any cut matrix (FP64 sincos per term);
+//  * the factorised sum for an axis-block cut matrix P = [diag(d1); diag(d2)]
+//    and points on a tensor grid: q_x depends only on (xi_1, xi_4), q_y on
+//    (xi_2, xi_5), q_z on (xi_3, xi_6), so u = C x1 Ex x2 Ey x3 Ez is three
+//    complex GEMMs against per-axis phase tables (exact in exact arithmetic);
+//  * the Taylor moments (one CTA per mode chunk and center, one thread per
+//    multi-index) and the per-block polynomial evaluation.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+#include "internal.cuh"
+
+namespace fame {
+
+static inline int rblocks(long long n, int t = 256) { return (int)std::min<long long>((n + t - 1) / t, 148 * 32); }
+
+// ------------------------------------------------------------------ direct
+constexpr int kDirectPts = 128;
+constexpr int kDirectModes = 256;
+__global__ void __launch_bounds__(kDirectPts) k_direct_sum(const double2* __restrict__ c, const double* __restrict__ Q,
+                                                          long long NF, const double* __restrict__ R, long long M,
+                                                          double2* __restrict__ u) {
+  __shared__ double sq[3][kDirectModes];
+  __shared__ double2 sc[kDirectModes];
+  const long long i = (long long)blockIdx.x * kDirectPts + threadIdx.x;
+  const bool act = i < M;
+  const double rx = act ? R[i] : 0.0, ry = act ? R[M + i] : 0.0, rz = act ? R[2 * M + i] : 0.0;
+  double ar = 0.0, ai = 0.0;
+  for (long long j0 = 0; j0 < NF; j0 += kDirectModes) {
+    const int nj = (int)std::min<long long>(kDirectModes, NF - j0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < nj; t += blockDim.x) {
+      sq[0][t] = Q[j0 + t];
+      sq[1][t] = Q[NF + j0 + t];
+      sq[2][t] = Q[2 * NF + j0 + t];
+      sc[t] = c[j0 + t];
+    }
+    __syncthreads();
+    if (act) {
+      for (int t = 0; t < nj; ++t) {
+        double s, co;
+        sincos(sq[0][t] * rx + sq[1][t] * ry + sq[2][t] * rz, &s, &co);
+        ar += sc[t].x * co - sc[t].y * s;
+        ai += sc[t].x * s + sc[t].y * co;
+      }
+    }
+  }
+  if (act) u[i] = make_double2(ar, ai);
+}
+
+// -------------------------------------------------------------- factorised
+// phase table T[x + nx*a] = exp(i q(a) xs[x]),  a = j_lo + n j_hi,
+// q(a) = d1 (xi(j_lo) + k_lo) + d2 (xi(j_hi) + k_hi)
+__global__ void k_phase_table(const double* xs, int nx, int N, double d1, double k1, double d2, double k2,
+                              double2* T) {
+  const int n = 2 * N, n2 = n * n;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)nx * n2;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(t % nx), a = (int)(t / nx);
+    const int jl = a % n, jh = a / n;
+    const double xl = (jl < N ? jl : jl - n) + k1, xh = (jh < N ? jh : jh - n) + k2;
+    double s, c;
+    sincos((d1 * xl + d2 * xh) * xs[x], &s, &c);
+    T[t] = make_double2(c, s);
+  }
+}
+
+// Cp[a + n^2 (b + n^2 c)] = coeff[j1 + n j2 + n^2 j3 + n^3 j4 + n^4 j5 + n^5 j6]
+// with a = j1 + n j4, b = j2 + n j5, c = j3 + n j6
+__global__ void k_pair_permute(const double2* coeff, int n, double2* Cp) {
+  const long long n2 = (long long)n * n, NF = n2 * n2 * n2;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < NF; i += (long long)gridDim.x * blockDim.x) {
+    long long t = i;
+    int j[6];
+    for (int d = 0; d < 6; ++d) {
+      j[d] = (int)(t % n);
+      t /= n;
+    }
+    const long long a = j[0] + n * j[3], b = j[1] + n * j[4], c = j[2] + n * j[5];
+    Cp[a + n2 * (b + n2 * c)] = coeff[i];
+  }
+}
+
+// Batched complex GEMM C(m,n) = sum_k A(m,k) B(k,n) with element strides,
+// FP64, 32x32 output tile per CTA, 16-deep k tiles in shared memory.
+struct GemmArgs {
+  const double2* A;
+  const double2* B;
+  double2* C;
+  int M, N, K;
+  long long sam, sak, sbk, sbn, scm, scn;
+  long long bA, bB, bC;  // batch strides (blockIdx.z)
+};
+constexpr int kGT = 32, kGK = 16;
+__global__ void __launch_bounds__(256) k_zgemm(GemmArgs g) {
+  __shared__ double2 As[kGK][kGT + 1];
+  __shared__ double2 Bs[kGK][kGT + 1];
+  const double2* A = g.A + g.bA * blockIdx.z;
+  const double2* B = g.B + g.bB * blockIdx.z;
+  double2* Cm = g.C + g.bC * blockIdx.z;
+  const int m0 = blockIdx.x * kGT, n0 = blockIdx.y * kGT;
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;  // 16 x 16 threads, 2 x 2 outputs each
+  double2 acc[2][2];
+  for (int a = 0; a < 2; ++a)
+    for (int b = 0; b < 2; ++b) acc[a][b] = make_double2(0.0, 0.0);
+  for (int k0 = 0; k0 < g.K; k0 += kGK) {
+    for (int t = threadIdx.x; t < kGK * kGT; t += blockDim.x) {
+      const int kk = t / kGT, mm = t % kGT;
+      const int m = m0 + mm, k = k0 + kk;
+      As[kk][mm] = (m < g.M && k < g.K) ? A[m * g.sam + k * g.sak] : make_double2(0.0, 0.0);
+      const int nn = t % kGT, kb = t / kGT;
+      const int n = n0 + nn, k2 = k0 + kb;
+      Bs[kb][nn] = (n < g.N && k2 < g.K) ? B[k2 * g.sbk + n * g.sbn] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < kGK; ++kk) {
+      double2 a[2], b[2];
+      for (int q = 0; q < 2; ++q) {
+        a[q] = As[kk][tx + 16 * q];
+        b[q] = Bs[kk][ty + 16 * q];
+      }
+      for (int qa = 0; qa < 2; ++qa)
+        for (int qb = 0; qb < 2; ++qb) {
+          acc[qa][qb].x += a[qa].x * b[qb].x - a[qa].y * b[qb].y;
+          acc[qa][qb].y += a[qa].x * b[qb].y + a[qa].y * b[qb].x;
+        }
+    }
+    __syncthreads();
+  }
+  for (int qa = 0; qa < 2; ++qa)
+    for (int qb = 0; qb < 2; ++qb) {
+      const int m = m0 + tx + 16 * qa, n = n0 + ty + 16 * qb;
+      if (m < g.M && n < g.N) Cm[m * g.scm + n * g.scn] = acc[qa][qb];
+    }
+}
+
+int zgemm(const GemmArgs& g, int batch, cudaStream_t s) {
+  dim3 grid((g.M + kGT - 1) / kGT, (g.N + kGT - 1) / kGT, batch);
+  if (grid.y > 65535) return fail(FAME_ERR_UNSUPPORTED, "zgemm: N too large");
+  k_zgemm<<<grid, 256, 0, s>>>(g);
+  ::fame::count_launch();
+  FAME_CUDA_TRY(cudaGetLastError());
+  return FAME_OK;
+}
+
+// ------------------------------------------------------------------ Taylor
+// centers: per block the midpoint of the bounding box of its points
+__global__ void k_block_centers(const double* R, long long M, const long long* ptr, const long long* ids,
+                                const double* fixed, double* centers) {
+  __shared__ double mn[3][256], mx[3][256];
+  const int b = blockIdx.x;
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (long long t = ptr[b] + threadIdx.x; t < ptr[b + 1]; t += blockDim.x) {
+    const long long i = ids[t];
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = fmin(lo[d], R[d * M + i]);
+      hi[d] = fmax(hi[d], R[d * M + i]);
+    }
+  }
+  for (int d = 0; d < 3; ++d) {
+    mn[d][threadIdx.x] = lo[d];
+    mx[d][threadIdx.x] = hi[d];
+  }
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s)
+      for (int d = 0; d < 3; ++d) {
+        mn[d][threadIdx.x] = fmin(mn[d][threadIdx.x], mn[d][threadIdx.x + s]);
+        mx[d][threadIdx.x] = fmax(mx[d][threadIdx.x], mx[d][threadIdx.x + s]);
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int d = 0; d < 3; ++d) centers[3 * b + d] = fixed ? fixed[d] : 0.5 * (mn[d][0] + mx[d][0]);
+}
+
+constexpr int kTaySub = 64;     // modes staged per sub-chunk
+constexpr int kTayChunk = 4096; // modes per CTA
+constexpr int kMaxP = 12;
+// partial[(chunk * nB + b) * L + alpha] = sum_{j in chunk} c_j e^{i q_j.r_c} q_j^alpha
+__global__ void __launch_bounds__(512) k_taylor_moments(const double2* __restrict__ c, const double* __restrict__ Q,
+                                                       long long NF, const double* __restrict__ centers,
+                                                       const int* __restrict__ alist, int L, int p, int nB,
+                                                       double2* __restrict__ partial) {
+  __shared__ double2 w[kTaySub];
+  __shared__ double pw[3][kTaySub][kMaxP + 1];
+  const int chunk = blockIdx.x, b = blockIdx.y;
+  const double cx = centers[3 * b], cy = centers[3 * b + 1], cz = centers[3 * b + 2];
+  const int al = threadIdx.x;
+  const bool act = al < L;
+  const int a1 = act ? alist[3 * al] : 0, a2 = act ? alist[3 * al + 1] : 0, a3 = act ? alist[3 * al + 2] : 0;
+  double ar = 0.0, ai = 0.0;
+  const long long j0c = (long long)chunk * kTayChunk;
+  const long long j1c = std::min<long long>(NF, j0c + kTayChunk);
+  for (long long j0 = j0c; j0 < j1c; j0 += kTaySub) {
+    const int nj = (int)std::min<long long>(kTaySub, j1c - j0);
+    __syncthreads();
+    if ((int)threadIdx.x < nj) {
+      const long long j = j0 + threadIdx.x;
+      const double qx = Q[j], qy = Q[NF + j], qz = Q[2 * NF + j];
+      double s, co;
+      sincos(qx * cx + qy * cy + qz * cz, &s, &co);
+      const double2 cj = c[j];
+      w[threadIdx.x] = make_double2(cj.x * co - cj.y * s, cj.x * s + cj.y * co);
+      double px = 1.0, py = 1.0, pz = 1.0;
+      for (int k = 0; k <= p; ++k) {
+        pw[0][threadIdx.x][k] = px;
+        pw[1][threadIdx.x][k] = py;
+        pw[2][threadIdx.x][k] = pz;
+        px *= qx;
+        py *= qy;
+        pz *= qz;
+      }
+    }
+    __syncthreads();
+    if (act) {
+      for (int t = 0; t < nj; ++t) {
+        const double mono = pw[0][t][a1] * pw[1][t][a2] * pw[2][t][a3];
+        ar += w[t].x * mono;
+        ai += w[t].y * mono;
+      }
+    }
+  }
+  if (act) partial[((long long)chunk * nB + b) * L + al] = make_double2(ar, ai);
+}
+
+// gamma[b*L + a] = coef[a] * sum_chunks partial (fixed order)
+__global__ void k_taylor_reduce(const double2* partial, int nChunks, int nB, int L, const double2* coef,
+                                double2* gamma) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)nB * L) return;
+  double ar = 0.0, ai = 0.0;
+  for (int ch = 0; ch < nChunks; ++ch) {
+    const double2 v = partial[(long long)ch * nB * L + t];
+    ar += v.x;
+    ai += v.y;
+  }
+  const double2 cf = coef[t % L];
+  gamma[t] = make_double2(cf.x * ar - cf.y * ai, cf.x * ai + cf.y * ar);
+}
+
+// u(ids[t]) = sum_a gamma[b, a] (r - r_c)^a for the block's points
+__global__ void __launch_bounds__(256) k_taylor_eval(const double* __restrict__ R, long long M,
+                                                    const long long* __restrict__ ptr, const long long* __restrict__ ids,
+                                                    const double* __restrict__ centers, const double2* __restrict__ gamma,
+                                                    const int* __restrict__ alist, int L, int p, double2* __restrict__ u) {
+  extern __shared__ double2 sg[];
+  int* sa = reinterpret_cast<int*>(sg + L);
+  const int b = blockIdx.y;
+  for (int t = threadIdx.x; t < L; t += blockDim.x) {
+    sg[t] = gamma[(long long)b * L + t];
+    sa[3 * t] = alist[3 * t];
+    sa[3 * t + 1] = alist[3 * t + 1];
+    sa[3 * t + 2] = alist[3 * t + 2];
+  }
+  __syncthreads();
+  const long long t = ptr[b] + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ptr[b + 1]) return;
+  const long long i = ids[t];
+  const double dx = R[i] - centers[3 * b], dy = R[M + i] - centers[3 * b + 1], dz = R[2 * M + i] - centers[3 * b + 2];
+  double px[kMaxP + 1], py[kMaxP + 1], pz[kMaxP + 1];
+  px[0] = py[0] = pz[0] = 1.0;
+  for (int k = 1; k <= p; ++k) {
+    px[k] = px[k - 1] * dx;
+    py[k] = py[k - 1] * dy;
+    pz[k] = pz[k - 1] * dz;
+  }
+  double ar = 0.0, ai = 0.0;
+  for (int a = 0; a < L; ++a) {
+    const double mono = px[sa[3 * a]] * py[sa[3 * a + 1]] * pz[sa[3 * a + 2]];
+    ar += sg[a].x * mono;
+    ai += sg[a].y * mono;
+  }
+  u[i] = make_double2(ar, ai);
+}
+
+}  // namespace fame
+
+using namespace fame;
+
+extern "C" {
+
+int fame_reconstruct_direct(fame_ctx* ctx, const void* coeff, const double* qModes, long long NF,
+                            const double* rPoints, long long M, void* u) {
+  if (!ctx || !coeff || !qModes || !rPoints || !u || NF <= 0 || M < 0)
+    return fail(FAME_ERR_INVALID, "reconstruct_direct arguments");
+  if (M == 0) return FAME_OK;
+  k_direct_sum<<<(int)((M + kDirectPts - 1) / kDirectPts), kDirectPts, 0, ctx->stream>>>(
+      (const double2*)coeff, qModes, NF, rPoints, M, (double2*)u);
+  ::fame::count_launch();
+  FAME_CUDA_TRY(cudaGetLastError());
+  return FAME_OK;
+}
+
+int fame_reconstruct_direct_grid(fame_basis* bs, const void* coeff, const double* xs, int nx,
+                                 const double* ys, int ny, const double* zs, int nz, void* u) {
+  if (!bs || !coeff || !xs || !ys || !zs || !u || nx <= 0 || ny <= 0 || nz <= 0)
+    return fail(FAME_ERR_INVALID, "reconstruct_direct_grid arguments");
+  const double* P = bs->P;  // column-major 6 x 3
+  for (int l = 0; l < 6; ++l)
+    for (int c = 0; c < 3; ++c)
+      if (l % 3 != c && P[c * 6 + l] != 0.0)
+        return fail(FAME_ERR_UNSUPPORTED, "factorised reconstruction needs an axis-block cut matrix [diag; diag]");
+  const int N = bs->N, n = 2 * N;
+  const long long n2 = (long long)n * n, NF = bs->NF;
+  cudaStream_t s = bs->ctx->stream;
+  double2 *Tx = nullptr, *Ty = nullptr, *Tz = nullptr, *Cp = nullptr, *T1 = nullptr, *T2 = nullptr;
+  int st = dalloc((void**)&Tx, (size_t)nx * n2 * sizeof(double2));
+  if (st == FAME_OK) st = dalloc((void**)&Ty, (size_t)ny * n2 * sizeof(double2));
+  if (st == FAME_OK) st = dalloc((void**)&Tz, (size_t)nz * n2 * sizeof(double2));
+  if (st == FAME_OK) st = dalloc((void**)&Cp, (size_t)NF * sizeof(double2));
+  if (st == FAME_OK) st = dalloc((void**)&T1, (size_t)nx * n2 * n2 * sizeof(double2));
+  if (st == FAME_OK) st = dalloc((void**)&T2, (size_t)nx * ny * n2 * sizeof(double2));
+  const double* k = bs->info.kLift;
+  if (st == FAME_OK) {
+    k_phase_table<<<rblocks((long long)nx * n2), 256, 0, s>>>(xs, nx, N, P[0], k[0], P[3], k[3], Tx);
+    ::fame::count_launch();
+    k_phase_table<<<rblocks((long long)ny * n2), 256, 0, s>>>(ys, ny, N, P[6 + 1], k[1], P[6 + 4], k[4], Ty);
+    ::fame::count_launch();
+    k_phase_table<<<rblocks((long long)nz * n2), 256, 0, s>>>(zs, nz, N, P[12 + 2], k[2], P[12 + 5], k[5], Tz);
+    ::fame::count_launch();
+    k_pair_permute<<<rblocks(NF), 256, 0, s>>>((const double2*)coeff, n, Cp);
+    ::fame::count_launch();
+    // T1[x, (b,c)] = sum_a Tx[x, a] Cp[a, (b,c)]
+    GemmArgs g1{Tx, Cp, T1, nx, (int)(n2 * n2), (int)n2, 1, nx, 1, n2, 1, nx, 0, 0, 0};
+    st = zgemm(g1, 1, s);
+    // T2[x, y, c] = sum_b T1[x, b, c] Ty[y, b]   (batched over c)
+    GemmArgs g2{T1, Ty, T2, nx, ny, (int)n2, 1, nx, ny, 1, 1, nx, (long long)nx * n2, 0, (long long)nx * ny};
+    if (st == FAME_OK) st = zgemm(g2, (int)n2, s);
+    // u[(x,y), z] = sum_c T2[(x,y), c] Tz[z, c]
+    GemmArgs g3{T2, Tz, (double2*)u, nx * ny, nz, (int)n2, 1, (long long)nx * ny, nz, 1, 1, (long long)nx * ny, 0, 0, 0};
+    if (st == FAME_OK) st = zgemm(g3, 1, s);
+    if (st == FAME_OK) st = cudaStreamSynchronize(s) == cudaSuccess ? FAME_OK : fail(FAME_ERR_CUDA, "sync");
+  }
+  dfree(Tx); dfree(Ty); dfree(Tz); dfree(Cp); dfree(T1); dfree(T2);
+  return st;
+}
+
+int fame_taylor_on_blocks(fame_ctx* ctx, const void* coeff, const double* qModes, long long NF,
+                          const double* rPoints, long long M, int p, const long long* blockPtr,
+                          const long long* blockIds, int nBlocks, const double* fixedCenter, void* u) {
+  if (!ctx || !coeff || !qModes || !rPoints || !u || !blockPtr || !blockIds || NF <= 0 || M < 0 ||
+      nBlocks < 1)
+    return fail(FAME_ERR_INVALID, "taylor_on_blocks arguments");
+  if (p < 0 || p > kMaxP) return fail(FAME_ERR_UNSUPPORTED, "Taylor order must be in [0,12]");
+  // multi-indices |a| <= p, a1 outer, a3 inner (exp2/build_multi_index_list_3d_exp3.m:3-14)
+  std::vector<int> al;
+  std::vector<double2> cf;
+  for (int a1 = 0; a1 <= p; ++a1)
+    for (int a2 = 0; a2 <= p - a1; ++a2)
+      for (int a3 = 0; a3 <= p - a1 - a2; ++a3) {
+        al.push_back(a1);
+        al.push_back(a2);
+        al.push_back(a3);
+        const int s = a1 + a2 + a3;
+        const double mag = std::exp(-(std::lgamma(a1 + 1.0) + std::lgamma(a2 + 1.0) + std::lgamma(a3 + 1.0)));
+        const double re[4] = {1, 0, -1, 0}, im[4] = {0, 1, 0, -1};  // i^s
+        cf.push_back(make_double2(mag * re[s % 4], mag * im[s % 4]));
+      }
+  const int L = (int)cf.size();
+  if (L > 512) return fail(FAME_ERR_UNSUPPORTED, "too many Taylor terms");
+  const int nChunks = (int)((NF + kTayChunk - 1) / kTayChunk);
+  cudaStream_t s = ctx->stream;
+  int* dal = nullptr;
+  double2 *dcf = nullptr, *partial = nullptr, *gamma = nullptr;
+  double *centers = nullptr, *dfix = nullptr;
+  int st = dalloc((void**)&dal, al.size() * sizeof(int));
+  if (st == FAME_OK) st = dalloc((void**)&dcf, cf.size() * sizeof(double2));
+  if (st == FAME_OK) st = dalloc((void**)&partial, (size_t)nChunks * nBlocks * L * sizeof(double2));
+  if (st == FAME_OK) st = dalloc((void**)&gamma, (size_t)nBlocks * L * sizeof(double2));
+  if (st == FAME_OK) st = dalloc((void**)&centers, (size_t)nBlocks * 3 * sizeof(double));
+  if (st == FAME_OK && fixedCenter) st = dalloc((void**)&dfix, 3 * sizeof(double));
+  if (st == FAME_OK) {
+    cudaMemcpyAsync(dal, al.data(), al.size() * sizeof(int), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dcf, cf.data(), cf.size() * sizeof(double2), cudaMemcpyHostToDevice, s);
+    if (fixedCenter) cudaMemcpyAsync(dfix, fixedCenter, 3 * sizeof(double), cudaMemcpyHostToDevice, s);
+    k_block_centers<<<nBlocks, 256, 0, s>>>(rPoints, M, blockPtr, blockIds, dfix, centers);
+    ::fame::count_launch();
+    dim3 gm(nChunks, nBlocks);
+    k_taylor_moments<<<gm, std::max(32, (L + 31) / 32 * 32), 0, s>>>((const double2*)coeff, qModes, NF, centers,
+                                                                     dal, L, p, nBlocks, partial);
+    ::fame::count_launch();
+    k_taylor_reduce<<<(nBlocks * L + 255) / 256, 256, 0, s>>>(partial, nChunks, nBlocks, L, dcf, gamma);
+    ::fame::count_launch();
+    // one grid column per block; x-extent covers the largest block
+    std::vector<long long> hp(nBlocks + 1);
+    cudaMemcpyAsync(hp.data(), blockPtr, (nBlocks + 1) * sizeof(long long), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) st = fail(FAME_ERR_CUDA, "taylor sync");
+    long long maxPts = 0;
+    for (int b = 0; b < nBlocks && st == FAME_OK; ++b) maxPts = std::max(maxPts, hp[b + 1] - hp[b]);
+    if (st == FAME_OK && maxPts > 0) {
+      dim3 ge((unsigned)((maxPts + 255) / 256), nBlocks);
+      const size_t smem = L * sizeof(double2) + 3 * L * sizeof(int);
+      k_taylor_eval<<<ge, 256, smem, s>>>(rPoints, M, blockPtr, blockIds, centers, gamma, dal, L, p,
+                                          (double2*)u);
+      ::fame::count_launch();
+    }
+    if (st == FAME_OK && cudaGetLastError() != cudaSuccess) st = fail(FAME_ERR_CUDA, "taylor launch");
+    if (st == FAME_OK && cudaStreamSynchronize(s) != cudaSuccess) st = fail(FAME_ERR_CUDA, "taylor sync");
+  }
+  dfree(dal); dfree(dcf); dfree(partial); dfree(gamma); dfree(centers); dfree(dfix);
+  return st;
+}
+
+}  // extern "C"

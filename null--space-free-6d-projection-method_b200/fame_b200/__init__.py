@@ -10,3 +10,5 @@ fails if the library has not been built.
 from ._lib import FameError, LIB_PATH  # noqa: F401  (loads the library or raises)
 from .core import *  # noqa: F401,F403
 from . import configs  # noqa: F401
+from .recon import *  # noqa: F401,F403
+from . import grad  # noqa: F401

@@ -29,7 +29,8 @@ FAME_PREC_FP64, FAME_PREC_MIXED = 0, 1
 
 class fame_basis_info(C.Structure):
     _fields_ = [("NF", C.c_longlong), ("N", C.c_int), ("nsingular", C.c_int),
-                ("minQq", C.c_double), ("minAbsDetV1", C.c_double), ("kLift", C.c_double * 6)]
+                ("minQq", C.c_double), ("minAbsDetV1", C.c_double), ("kLift", C.c_double * 6),
+                ("pivot", C.c_int)]
 
 
 class fame_krinv_opts(C.Structure):
@@ -37,7 +38,8 @@ class fame_krinv_opts(C.Structure):
                 ("maxitCG", C.c_int), ("tolKr", C.c_double), ("tolM", C.c_double),
                 ("maxitKr", C.c_int), ("maxitM", C.c_int), ("epsC", C.c_double),
                 ("useKrPreconditioner", C.c_int), ("tolInner32", C.c_double),
-                ("maxRefine", C.c_int), ("checkEvery", C.c_int), ("verifyTrueResidual", C.c_int)]
+                ("maxRefine", C.c_int), ("checkEvery", C.c_int), ("verifyTrueResidual", C.c_int),
+                ("useGraphs", C.c_int)]
 
 
 class fame_krinv_stats(C.Structure):
@@ -64,6 +66,7 @@ SIGNATURES = {
     "fame_ctx_create": [I, C.POINTER(P)],
     "fame_ctx_destroy": [P],
     "fame_ctx_set_stream": [P, P],
+    "fame_ctx_use_own_stream": [P],
     "fame_ctx_sync": [P],
     "fame_applyMij_fft": [P, I, P, P, P, I, I],
     "fame_mass_create": [P, I, P, C.POINTER(P)],
@@ -88,6 +91,15 @@ SIGNATURES = {
     "fame_start_vector": [P, C.c_ulonglong, LL, P],
     "fame_apply_Mhat_C_scalar_compact": [P, P, P, P, I],
     "fame_apply_Mhat_C_scalar_compact_noalloc": [P, P, P, P, I],
+    "fame_recover_eigvecs": [P, P, P, I, D, I, I, P, P, C.POINTER(I), C.POINTER(D)],
+    "fame_fourier_diagnostics": [P, P, P, C.POINTER(D), I, C.POINTER(D), C.POINTER(D), C.POINTER(D)],
+    "fame_reconstruct_direct": [P, P, P, LL, P, LL, P],
+    "fame_reconstruct_direct_grid": [P, P, P, I, P, I, P, I, P],
+    "fame_taylor_on_blocks": [P, P, P, LL, P, LL, I, P, P, I, C.POINTER(D), P],
+    "fame_mass_adjoint": [P, P, I, P, I, C.POINTER(D)],
+    "fame_solve_batch": [I, I, C.POINTER(I), C.POINTER(P), C.POINTER(D), C.POINTER(D),
+                         C.POINTER(fame_krinv_opts), I, D, I, I, C.c_ulonglong, C.POINTER(D),
+                         C.POINTER(fame_lanczos_info), C.POINTER(I)],
 }
 
 

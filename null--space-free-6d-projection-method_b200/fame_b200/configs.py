@@ -22,6 +22,11 @@ SEED = 20260905                          # exp1/make_config_BC_fig1a.m:42
 # Reference KAT: N=2, modes 1 and 10 of the tracking system (exp3/make_config_experiment4.m:38-40)
 KAT_N2_LAMBDA = (1.201276300237e-02, 4.496454358674e-02)
 
+# At Gamma (q = 0) the xi = 0 mode has q_xi = 0 and the null-space-free reduction is
+# singular (exp1/assemble_K_and_nullspace_free_basis.m:36-42); the Bloch-path
+# workload solves that point at this small shift along the first path segment.
+GAMMA_SHIFT = np.array([1e-3, 0.0, 0.0])
+
 # Solver settings of the 10-eigenpair workloads (shift 0, Krylov block 40, outer tol 1e-8,
 # inner Mhat PCG tol 1e-10).
 SOLVE = dict(nev=10, p=40, tol=1e-8, maxRestart=30, tolCG=1e-10, maxitCG=3000)

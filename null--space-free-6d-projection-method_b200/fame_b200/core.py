@@ -21,7 +21,7 @@ __all__ = [
     "Context", "applyMij_fft", "MassBackend", "apply_V_blockdiag", "apply_VH_blockdiag",
     "solveV1_blockdiag", "solveV1H_blockdiag", "QSystem", "build_q_system",
     "make_explicit_krinv_compact", "make_nested_krinv_instrumented", "KrInv", "Lanczos",
-    "start_vector", "FameError", "apply_Mhat_C_scalar_compact", "kernel_launches",
+    "start_vector", "FameError", "apply_Mhat_C_scalar_compact", "kernel_launches", "solve_batch",
 ]
 
 
@@ -255,6 +255,7 @@ class QSystem:
         self.minAbsDetV1 = info.minAbsDetV1
         self.minQq = info.minQq
         self.nsingular = info.nsingular
+        self.pivot = info.pivot
         self._cache = {}
 
     def __getattr__(self, name):
@@ -452,3 +453,31 @@ def Lanczos(fncA, fncB, fncBinv, n, k, tol, maxiter, p, v0, flag_gpu=True, verbo
     return Y.t(), ew, info.steps, dict(steps=info.steps, restarts=info.restarts,
                                        converged=bool(info.converged), nconv=info.nconv,
                                        maxWantedResidual=info.maxWantedResidual)
+
+
+def solve_batch(Ns, materials, qs, P, nev=10, tol=1e-8, maxiter=30, p=40, tolCG=1e-10,
+                precision="mixed", seed=None, device=None):
+    """Solve independent Bloch points of uneven size concurrently (one call).
+
+    ``materials[i]`` is the float64 device eps grid of instance i.  Returns
+    ``(lam, infos)`` with lam (count x nev) ascending eigenvalues lambda = 1/theta.
+    """
+    from . import configs
+    count = len(Ns)
+    dev = torch.cuda.current_device() if device is None else device
+    Es = [e.contiguous() for e in materials]
+    Earr = (C.c_void_p * count)(*[e.data_ptr() for e in Es])
+    Narr = (C.c_int * count)(*[int(n) for n in Ns])
+    qarr = (C.c_double * (3 * count))(*np.asarray(qs, dtype=np.float64).reshape(-1))
+    Parr = (C.c_double * 18)(*np.asarray(P, dtype=np.float64).reshape(6, 3).reshape(-1, order="F"))
+    o = _opts(kind=L.FAME_KRINV_EXPLICIT, tolCG=tolCG, maxitCG=3000,
+              prec_mode=L.FAME_PREC_MIXED if precision == "mixed" else L.FAME_PREC_FP64)
+    theta = (C.c_double * (count * nev))()
+    infos = (L.fame_lanczos_info * count)()
+    status = (C.c_int * count)()
+    torch.cuda.synchronize(dev)
+    call("fame_solve_batch", dev, count, Narr, Earr, qarr, Parr, C.byref(o), nev, float(tol), int(maxiter),
+         int(p), C.c_ulonglong(configs.SEED if seed is None else seed), theta, infos, status)
+    th = np.array(theta[:]).reshape(count, nev)
+    return np.sort(1.0 / th, axis=1), [dict(steps=i.steps, converged=bool(i.converged), nconv=i.nconv)
+                                       for i in infos]

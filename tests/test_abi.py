@@ -56,9 +56,9 @@ def test_null_arguments_are_rejected_without_gpu():
 def test_struct_layouts_match_header():
     from fame_b200 import _lib
     # field counts mirror include/fame.h
-    assert len(_lib.fame_krinv_opts._fields_) == 14
+    assert len(_lib.fame_krinv_opts._fields_) == 15
     assert len(_lib.fame_krinv_stats._fields_) == 10
-    assert C.sizeof(_lib.fame_basis_info) == 8 + 4 + 4 + 8 + 8 + 48
+    assert C.sizeof(_lib.fame_basis_info) == 8 + 4 + 4 + 8 + 8 + 48 + 8
 
 
 def test_twiddle_header_is_generated_and_exact():

@@ -114,3 +114,25 @@ def test_lanczos_baseline_n3_fp64_and_mixed(cuda_device):
         assert float(torch.linalg.norm(r) / (abs(theta[j]) * torch.linalg.norm(y))) < 1e-6
     d = np.max(np.abs(lams["mixed", 1e-10] - lams["fp64", 1e-10]) / lams["fp64", 1e-10])
     assert d < 2e-9, d
+
+
+def test_pivoted_split_when_v1_is_singular(cuda_device):
+    """q_3 = 0 makes the reference's V1 block singular for xi = 0; the basis pivots and
+    the explicit K_r^{-1} then agrees with the nested one (which never inverts V1)."""
+    import fame_b200 as F
+    N = 1
+    q = (0.1, 0.05, 0.0)
+    E = O.material_separable_cos(N, 12.0)
+    m = F.MassBackend(torch.as_tensor(E, device=cuda_device), N)
+    sg = F.build_q_system(m, F.configs.P_GOLDEN, q)
+    assert sg.pivot == 0 and sg.minAbsDetV1 > 1e-10
+    rng = np.random.default_rng(8)
+    b = rng.standard_normal(sg.nr) + 1j * rng.standard_normal(sg.nr)
+    bt = torch.as_tensor(b, device=cuda_device)
+    yc = F.make_explicit_krinv_compact(sg, 1e-12, 3000)[0](bt).cpu().numpy()
+    yb = F.make_nested_krinv_instrumented(sg, 4.0, 1e-12, 1e-13)[0](bt).cpu().numpy()
+    assert _rel(yc, yb) < 1e-9
+    with np.errstate(all="ignore"):  # the oracle's W is singular here; the nested form never uses it
+        S = O.build_q_system(N, F.configs.P_GOLDEN, q, E)
+    yo = O.make_nested_krinv_instrumented(S, 4.0, 1e-12, 1e-13)[0](b)
+    assert _rel(yb, yo) < 1e-9
