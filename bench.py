@@ -42,6 +42,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["fame", "reference"], default="fame")
     ap.add_argument("--N", type=int, default=N_BENCH)
+    ap.add_argument("--case", choices=["chain", "pcg", "solve"], default=None,
+                    help="run one piece of the step alone (for profiling), print its device time")
+    ap.add_argument("--precision", choices=["fp32", "fp64", "mixed"], default="mixed")
+    ap.add_argument("--reps", type=int, default=3)
     return ap.parse_args()
 
 
@@ -409,6 +413,53 @@ def cpu_baseline(N, steps_in_solve=40, kind="port"):
                       % (N, cores, stats()["totalMhatIterations"], dt, steps_in_solve)}
 
 
+def run_case(args):
+    """One piece of the benchmark step, repeated ``--reps`` times on cuda:0:
+
+    * ``chain``: the Mhat action (passes A/B/C over 3 fields), FP32 (``--precision
+      fp32``/``mixed``) or FP64 — the kernel chain the roofline line reports;
+    * ``pcg``: one explicit K_r^{-1} action (``--precision mixed|fp64``);
+    * ``solve``: one full 10-eigenpair Lanczos solve (the timed step).
+    """
+    import torch
+    import fame_b200 as F
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    N = args.N
+    NF = (2 * N) ** 6
+    cfg = F.configs
+    S = cfg.SOLVE
+    E = cfg.material_separable_cos(N, 12.0, device=dev)
+    mass = F.MassBackend(E, N)
+    sysq = F.build_q_system(mass, cfg.P_GOLDEN, cfg.Q_BASELINE)
+    v0 = F.start_vector(cfg.SEED, sysq.nr)
+    prec = "fp64" if args.precision == "fp64" else "mixed"
+    if args.case == "chain":
+        x = torch.randn(NF, dtype=torch.complex128 if prec == "fp64" else torch.complex64, device=dev)
+        body = lambda: F.apply_Mhat_C_scalar_compact(x, sysq)  # noqa: E731
+    else:
+        op = F.make_explicit_krinv_compact(sysq, S["tolCG"], S["maxitCG"], precision=prec)[0]
+        if args.case == "pcg":
+            q = (v0 / torch.linalg.norm(v0)).reshape(-1, 1)
+            body = lambda: op(q)  # noqa: E731
+        else:
+            body = lambda: F.Lanczos(op, None, None, sysq.nr, S["nev"], S["tol"],  # noqa: E731
+                                     S["maxRestart"], S["p"], v0)
+    body()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    l0 = F.kernel_launches()
+    e0.record()
+    for _ in range(args.reps):
+        body()
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"case": args.case, "N": N, "precision": prec, "reps": args.reps,
+                      "s_per_rep": e0.elapsed_time(e1) / 1e3 / args.reps,
+                      "launches_per_rep": (F.kernel_launches() - l0) / args.reps}), flush=True)
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -439,6 +490,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.case:
+        run_case(args)
     else:
         run_fame(args)
 

@@ -2,6 +2,7 @@
 // generator.
 #include <atomic>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include "internal.cuh"
 
@@ -36,6 +37,59 @@ int dalloc(void** p, size_t bytes) {
 
 void dfree(void* p) {
   if (p) cudaFree(p);
+}
+
+// Per-device state shared by all handles: the device fault word that bounded
+// in-kernel waits set when they give up, and the SM count.
+constexpr int kMaxDevices = 64;
+static std::atomic<unsigned*> g_fault[kMaxDevices];
+static std::atomic<int> g_sms[kMaxDevices];
+static std::mutex g_dev_mu;
+
+static int current_device() {
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= kMaxDevices) return -1;
+  return d;
+}
+
+int ensure_device_state(int device) {
+  if (device < 0 || device >= kMaxDevices) return fail(FAME_ERR_INVALID, "device index out of range");
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  if (g_fault[device].load() == nullptr) {
+    unsigned* p = nullptr;
+    FAME_CUDA_TRY(cudaMalloc(&p, sizeof(unsigned)));
+    FAME_CUDA_TRY(cudaMemset(p, 0, sizeof(unsigned)));
+    g_fault[device].store(p);
+  }
+  if (g_sms[device].load() == 0) {
+    int v = 0;
+    FAME_CUDA_TRY(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device));
+    g_sms[device].store(v);
+  }
+  return FAME_OK;
+}
+
+unsigned* fault_word() {
+  const int d = current_device();
+  return d < 0 ? nullptr : g_fault[d].load();
+}
+
+int num_sms() {
+  const int d = current_device();
+  const int v = d < 0 ? 0 : g_sms[d].load();
+  return v > 0 ? v : 148;
+}
+
+int check_fault(fame_ctx* ctx) {
+  unsigned* p = g_fault[ctx->device].load();
+  if (!p) return FAME_OK;
+  FAME_CUDA_TRY(cudaMemcpyAsync(ctx->pinned, p, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+  FAME_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  unsigned v = 0;
+  std::memcpy(&v, ctx->pinned, sizeof(unsigned));
+  if (v == 0) return FAME_OK;
+  FAME_CUDA_TRY(cudaMemsetAsync(p, 0, sizeof(unsigned), ctx->stream));
+  return fail(FAME_ERR_CUDA, "a bounded device-side wait gave up (bulk copy never completed); results are invalid");
 }
 
 int read_back(fame_ctx* ctx, const void* dsrc, void* hdst, size_t bytes) {
@@ -99,6 +153,7 @@ int fame_ctx_create(int device, fame_ctx** out) {
   FAME_CUDA_TRY(cudaGetDeviceCount(&count));
   if (device < 0 || device >= count) return fail(FAME_ERR_INVALID, "bad device index");
   FAME_CUDA_TRY(cudaSetDevice(device));
+  FAME_TRY(ensure_device_state(device));
   fame_ctx* c = new fame_ctx();
   c->device = device;
   if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess ||
@@ -139,7 +194,7 @@ int fame_ctx_use_own_stream(fame_ctx* c) {
 int fame_ctx_sync(fame_ctx* c) {
   if (!c) return fail(FAME_ERR_INVALID, "ctx is NULL");
   FAME_CUDA_TRY(cudaStreamSynchronize(c->stream));
-  return FAME_OK;
+  return check_fault(c);
 }
 
 int fame_start_vector(fame_ctx* c, unsigned long long seed, long long n, void* v) {

@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <algorithm>
 #include <string>
 #include "../../include/fame.h"
 
@@ -62,6 +63,10 @@ void set_last_error(int code, const std::string& msg);
 int fail(int code, const std::string& msg);
 // Number of kernels this library has launched (all devices, all handles).
 void count_launch(long long n = 1);
+// Per-device fault word (set by bounded in-kernel waits that gave up; nullptr
+// before a context exists on the current device) and SM count of the current device.
+unsigned* fault_word();
+int num_sms();
 
 // --------------------------------------------------------------- reductions
 // Sum of K accumulators.  Each block reduces its threads' values, writes

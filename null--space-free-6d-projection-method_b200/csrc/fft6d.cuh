@@ -4,8 +4,9 @@
 //
 // The 6D transform is split into three passes over HBM/L2:
 //   pass A  inverse DFT along axes 1-3 (contiguous n^3 cubes), fused prologue;
-//   pass B  inverse DFT along axes 4-6 (cubes strided by n^3), multiply by
-//           E/NF, forward DFT along axes 4-6;
+//   pass B  inverse DFT along axes 4-6 (one tile of TT c123 indices x n^3
+//           c456 indices at a time, see WorkTile), multiply by E/NF, forward
+//           DFT along axes 4-6 (passb.cuh);
 //   pass C  forward DFT along axes 1-3, fused epilogue (+ grid reduction).
 // Each CTA stages whole n^3 cubes in shared memory (rows padded to n+1 to
 // avoid bank conflicts), one thread transforms one line in registers with a
@@ -94,9 +95,56 @@ template <int n, int SIGN, typename T> struct Dft<n, SIGN, T, true> {
   }
 };
 
-// Composite length n = R*M (R smallest prime factor): decimation in time.
+// Coprime split n = n1*n2 (n1 the full power of the smallest prime factor),
+// n2 == 1 when n is a prime power.
+template <int n> struct PfaSplit {
+  static constexpr int p = SmallestFactor<n>::value;
+  static constexpr int pow_of(int m) { return m % p == 0 ? p * pow_of(m / p) : 1; }
+  static constexpr int n1 = pow_of(n), n2 = n / n1;
+  static constexpr int inv(int a, int m) {  // a^{-1} mod m (m > 1, gcd(a, m) = 1)
+    int r = 1;
+    while ((a * r) % m != 1) ++r;
+    return r;
+  }
+};
+
+// Composite length n = R*M (R smallest prime factor): decimation in time for
+// prime powers; for n = n1*n2 with coprime n1, n2 > 1 the prime-factor
+// (Good-Thomas) algorithm, which needs no twiddle factors: input
+// x[(n2*i1 + n1*i2) mod n] -> length-n2 DFTs over i2, length-n1 DFTs over i1
+// -> output X[(k1*n2*(n2^-1 mod n1) + k2*n1*(n1^-1 mod n2)) mod n].
 template <int n, int SIGN, typename T> struct Dft<n, SIGN, T, false> {
   static __device__ __forceinline__ void run(T* re, T* im) {
+    if constexpr (PfaSplit<n>::n2 > 1) {
+      constexpr int n1 = PfaSplit<n>::n1, n2 = PfaSplit<n>::n2;
+      constexpr int u2 = PfaSplit<n>::inv(n2 % n1, n1), u1 = PfaSplit<n>::inv(n1 % n2, n2);
+      T ar[n1][n2], ai[n1][n2];
+#pragma unroll
+      for (int i1 = 0; i1 < n1; ++i1)
+#pragma unroll
+        for (int i2 = 0; i2 < n2; ++i2) {
+          ar[i1][i2] = re[(n2 * i1 + n1 * i2) % n];
+          ai[i1][i2] = im[(n2 * i1 + n1 * i2) % n];
+        }
+#pragma unroll
+      for (int i1 = 0; i1 < n1; ++i1) Dft<n2, SIGN, T>::run(ar[i1], ai[i1]);
+#pragma unroll
+      for (int k2 = 0; k2 < n2; ++k2) {
+        T br[n1], bi[n1];
+#pragma unroll
+        for (int i1 = 0; i1 < n1; ++i1) { br[i1] = ar[i1][k2]; bi[i1] = ai[i1][k2]; }
+        Dft<n1, SIGN, T>::run(br, bi);
+#pragma unroll
+        for (int k1 = 0; k1 < n1; ++k1) {
+          re[(k1 * n2 * u2 + k2 * n1 * u1) % n] = br[k1];
+          im[(k1 * n2 * u2 + k2 * n1 * u1) % n] = bi[k1];
+        }
+      }
+    } else {
+      run_dit(re, im);
+    }
+  }
+  static __device__ __forceinline__ void run_dit(T* re, T* im) {
     constexpr int R = SmallestFactor<n>::value, M = n / R;
     T ar[R][M], ai[R][M];
 #pragma unroll
@@ -206,6 +254,24 @@ template <int n> __device__ __forceinline__ long long line_to_nat(long long i) {
   return cb + q / n2 + n * (q % n2);
 }
 
+// Layout of the F work fields between the passes ("tile-major"): the n^3
+// values of c123 = i1 + n*i2 + n^2*i3 are cut into tiles of TT consecutive
+// indices, and tile k of a field is one contiguous block of TT*n^3 elements,
+// rows of TT elements ordered by c456 = i4 + n*i5 + n^2*i6:
+//   element (c123, c456) at TT*((c123/TT)*n^3 + c456) + c123%TT.
+// Pass A writes and pass C reads rows of TT*sizeof(C<T>) >= 16 bytes; pass B
+// pulls a tile (or one i6-plane of it) with a single bulk copy.
+template <int n, typename T> struct WorkTile {
+  static constexpr int TT = sizeof(T) == 4 ? (n <= 6 ? 8 : n <= 10 ? 4 : 2)
+                                           : (n <= 6 ? 4 : n <= 12 ? 2 : 1);
+  static_assert((n * n * n) % TT == 0, "tile width must divide n^3");
+};
+template <int n, typename T> __host__ __device__ __forceinline__ long long work_at(long long c123, long long c456) {
+  constexpr int TT = WorkTile<n, T>::TT;
+  constexpr long long n3 = (long long)n * n * n;
+  return TT * ((c123 / TT) * n3 + c456) + c123 % TT;
+}
+
 // ------------------------------------------------------------------ pass A
 // CTA = G consecutive columns c456 x F fields.
 //   phase 1: axis-1 lines through Pro::load(ia, in, v[F]) (thread <-> line
@@ -272,7 +338,7 @@ __global__ void __launch_bounds__(512) k_passA(Pro pro, C<T>* __restrict__ work,
   for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 3 -> global (natural order)
     const int cc = it / Q::n2, m = it % Q::n2;
     const C<T>* sc = s + cc * F * Q::size + Q::line3(m);
-    const long long g0 = (col0 + cc) * Q::n3 + m;
+    const long long c456 = col0 + cc;
 #pragma unroll
     for (int f = 0; f < F; ++f) {
       T re[n], im[n];
@@ -284,91 +350,8 @@ __global__ void __launch_bounds__(512) k_passA(Pro pro, C<T>* __restrict__ work,
       }
       Dft<n, +1, T>::run(re, im);
 #pragma unroll
-      for (int j = 0; j < n; ++j) work[f * NF + g0 + (long long)Q::n2 * j] = mk<T>(re[j], im[j]);
+      for (int j = 0; j < n; ++j) work[f * NF + work_at<n, T>(m + Q::n2 * j, c456)] = mk<T>(re[j], im[j]);
     }
-  }
-}
-
-// ------------------------------------------------------------------ pass B
-// CTA = TT consecutive c123 indices x all n^3 c456 indices of one field
-// (blockIdx.y).  Axis 4 lines come from / go to global (TT consecutive
-// elements per row: 32-byte sectors), axes 5 and 6 run in shared memory, and
-// the axis-6 line does inverse DFT, the E/NF multiply and the forward DFT in
-// registers.
-template <int n, typename T, int TT, typename TE>
-__global__ void __launch_bounds__(512) k_passB(C<T>* __restrict__ work, const TE* __restrict__ Es, TE escale,
-                                              long long NF, Gate gate) {
-  if (gate.off()) return;
-  using Q = Cube<n, T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C<T>* s = reinterpret_cast<C<T>*>(smem_raw);
-  C<T>* w = work + (long long)blockIdx.y * NF;
-  const long long c0 = (long long)blockIdx.x * TT;
-  constexpr int items = TT * Q::n2;
-  constexpr long long N3 = Q::n3;
-  for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 4 (inverse) from global
-    const int t = it % TT, l = it / TT;
-    const C<T>* src = w + c0 + t + N3 * n * l;
-    T re[n], im[n];
-#pragma unroll
-    for (int j = 0; j < n; ++j) {
-      const C<T> v = src[N3 * j];
-      re[j] = v.x;
-      im[j] = v.y;
-    }
-    Dft<n, +1, T>::run(re, im);
-    C<T>* sc = s + t * Q::size + Q::line1(l);
-#pragma unroll
-    for (int j = 0; j < n; ++j) sc[j] = mk<T>(re[j], im[j]);
-  }
-  __syncthreads();
-  for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 5 (inverse)
-    const int t = it / Q::n2, l = it % Q::n2;
-    line_dft<n, +1, T>(s + t * Q::size + Q::line2(l), Q::P1);
-  }
-  __syncthreads();
-  for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 6: inverse, *E/NF, forward
-    const int t = it / Q::n2, m = it % Q::n2;
-    C<T>* sc = s + t * Q::size + Q::line3(m);
-    T re[n], im[n];
-#pragma unroll
-    for (int j = 0; j < n; ++j) {
-      const C<T> v = sc[Q::P2 * j];
-      re[j] = v.x;
-      im[j] = v.y;
-    }
-    Dft<n, +1, T>::run(re, im);
-    const TE* e = Es + c0 + t + N3 * m;
-#pragma unroll
-    for (int j = 0; j < n; ++j) {
-      const T ej = (T)(e[N3 * Q::n2 * j] * escale);
-      re[j] *= ej;
-      im[j] *= ej;
-    }
-    Dft<n, -1, T>::run(re, im);
-#pragma unroll
-    for (int j = 0; j < n; ++j) sc[Q::P2 * j] = mk<T>(re[j], im[j]);
-  }
-  __syncthreads();
-  for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 5 (forward)
-    const int t = it / Q::n2, l = it % Q::n2;
-    line_dft<n, -1, T>(s + t * Q::size + Q::line2(l), Q::P1);
-  }
-  __syncthreads();
-  for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 4 (forward) to global
-    const int t = it % TT, l = it / TT;
-    const C<T>* sc = s + t * Q::size + Q::line1(l);
-    T re[n], im[n];
-#pragma unroll
-    for (int j = 0; j < n; ++j) {
-      const C<T> v = sc[j];
-      re[j] = v.x;
-      im[j] = v.y;
-    }
-    Dft<n, -1, T>::run(re, im);
-    C<T>* dst = w + c0 + t + N3 * n * l;
-#pragma unroll
-    for (int j = 0; j < n; ++j) dst[N3 * j] = mk<T>(re[j], im[j]);
   }
 }
 
@@ -391,14 +374,14 @@ __global__ void __launch_bounds__(512) k_passC(Epi epi, const C<T>* __restrict__
   constexpr int items = G * Q::n2;
   for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 3 from global
     const int cc = it / Q::n2, m = it % Q::n2;
-    const long long g0 = (col0 + cc) * Q::n3 + m;
+    const long long c456 = col0 + cc;
     C<T>* sc = s + cc * F * Q::size + Q::line3(m);
 #pragma unroll
     for (int f = 0; f < F; ++f) {
       T re[n], im[n];
 #pragma unroll
       for (int j = 0; j < n; ++j) {
-        const C<T> v = work[f * NF + g0 + (long long)Q::n2 * j];
+        const C<T> v = work[f * NF + work_at<n, T>(m + Q::n2 * j, c456)];
         re[j] = v.x;
         im[j] = v.y;
       }
@@ -465,40 +448,70 @@ __global__ void __launch_bounds__(512) k_passC(Epi epi, const C<T>* __restrict__
   }
 }
 
-// Inverse-only variant of pass B (axes 4-6, no material), for the mass adjoint.
-template <int n, typename T, int TT>
-__global__ void __launch_bounds__(512) k_passB_inv(C<T>* __restrict__ work, long long NF) {
+// ------------------------------------------------- linear-field chains
+// Operators whose fields are linear in one vector, field_f(i) = a_f(i) u(i),
+// and whose result is out(i) = S(i, sum_f b_f(i) v_f(i)) -- every Mhat chain
+// (exp1/apply_Mhat_C_scalar_compact.m:8-21) is of this form.  Passes A and C
+// transform the F fields of G columns concurrently: one thread per (field,
+// column, line), F*G cubes in shared memory, two barriers per pass.
+//
+// LinPro:  C<T> load(ia, in, Ext&)   u(i) (pure loads; stores deferred to commit)
+//          void commit(ia, in, const Ext&)   (field-0 threads, after all loads)
+//          C<T> coef(f, ia, in)      a_f(i) (a_0 == 1 when unit0)
+// LinEpi:  C<T> coef(f, ia, in)      b_f(i) (b_0 == 1 when unit0)
+//          void store(ia, in, C<T> s, Red<Acc,K>& acc), finalize(tot)
+// Epilogues whose vectors are in natural order declare `static constexpr bool natural = true`.
+template <class E, class = void> struct EpiNatural { static constexpr bool value = false; };
+template <class E> struct EpiNatural<E, decltype(void(E::natural))> { static constexpr bool value = E::natural; };
+
+template <int n, int F, int G> struct LinThreads {
+  static constexpr int value = (F * G * n * n + 31) / 32 * 32;
+};
+
+template <int n, typename T, int F, int G, class Pro>
+__global__ void __launch_bounds__(LinThreads<n, F, G>::value) k_passA_lin(Pro pro, C<T>* __restrict__ work, long long NF, Gate gate) {
+  if (gate.off()) return;
   using Q = Cube<n, T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C<T>* s = reinterpret_cast<C<T>*>(smem_raw);
-  C<T>* w = work + (long long)blockIdx.y * NF;
-  const long long c0 = (long long)blockIdx.x * TT;
-  constexpr int items = TT * Q::n2;
-  constexpr long long N3 = Q::n3;
-  for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 4 from global
-    const int t = it % TT, l = it / TT;
-    const C<T>* src = w + c0 + t + N3 * n * l;
+  const long long col0 = (long long)blockIdx.x * G;
+  constexpr int per_f = G * Q::n2;
+  const int it = threadIdx.x;
+  const bool act = it < F * per_f;
+  const int f = act ? it / per_f : 0, rem = act ? it % per_f : 0;
+  const int cc = rem / Q::n2, l = rem % Q::n2;
+  const long long cb = (col0 + cc) * Q::n3;
+  C<T>* cube = s + (f * G + cc) * Q::size;
+  typename Pro::Ext e[n];
+  if (act) {  // prologue and axis 1 in registers
+    C<T> u[n];
+#pragma unroll
+    for (int j = 0; j < n; ++j) u[j] = pro.load(cb + l + Q::n2 * j, cb + j + (long long)n * l, e[j]);
+    const bool unit = Pro::unit0 && f == 0;
     T re[n], im[n];
 #pragma unroll
     for (int j = 0; j < n; ++j) {
-      const C<T> v = src[N3 * j];
+      C<T> v = u[j];
+      if (!unit) v = cmul<T>(pro.coef(f, cb + l + Q::n2 * j, cb + j + (long long)n * l), v);
       re[j] = v.x;
       im[j] = v.y;
     }
     Dft<n, +1, T>::run(re, im);
-    C<T>* sc = s + t * Q::size + Q::line1(l);
+    C<T>* sc = cube + Q::line1(l);
 #pragma unroll
     for (int j = 0; j < n; ++j) sc[j] = mk<T>(re[j], im[j]);
   }
-  __syncthreads();
-  for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 5
-    const int t = it / Q::n2, l = it % Q::n2;
-    line_dft<n, +1, T>(s + t * Q::size + Q::line2(l), Q::P1);
+  __syncthreads();  // every field's loads are done: field 0 may store the prologue state
+  if (act) {
+    if (f == 0) {
+#pragma unroll
+      for (int j = 0; j < n; ++j) pro.commit(cb + l + Q::n2 * j, cb + j + (long long)n * l, e[j]);
+    }
+    line_dft<n, +1, T>(cube + Q::line2(l), Q::P1);  // axis 2
   }
   __syncthreads();
-  for (int it = threadIdx.x; it < items; it += blockDim.x) {  // axis 6 -> global
-    const int t = it % TT, m = it / TT;
-    const C<T>* sc = s + t * Q::size + Q::line3(m);
+  if (act) {  // axis 3 -> work (tile-major), thread <-> m = i1 + n*i2
+    const C<T>* sc = cube + Q::line3(l);
     T re[n], im[n];
 #pragma unroll
     for (int j = 0; j < n; ++j) {
@@ -507,85 +520,14 @@ __global__ void __launch_bounds__(512) k_passB_inv(C<T>* __restrict__ work, long
       im[j] = v.y;
     }
     Dft<n, +1, T>::run(re, im);
-    C<T>* dst = w + c0 + t + N3 * m;
+    C<T>* wf = work + f * NF;
 #pragma unroll
-    for (int j = 0; j < n; ++j) dst[N3 * Q::n2 * j] = mk<T>(re[j], im[j]);
-  }
-}
-
-// ------------------------------------------------- linear-field chains
-// Operators whose fields are linear in one vector, field_f(i) = a_f(i) u(i),
-// and whose result is out(i) = S(i, sum_f b_f(i) v_f(i)) -- every Mhat chain
-// (exp1/apply_Mhat_C_scalar_compact.m:8-21) is of this form.  Passes A and C
-// then run the F fields one after another through a single shared-memory cube
-// per column, holding one line of u (pass A) or of the running sum (pass C) in
-// registers: a third of the shared memory and far fewer registers than the
-// general chain.  One line per thread (blockDim >= G*n^2).
-//
-// LinPro:  C<T> load(ia, in, Ext&)   u(i) (pure loads; stores deferred to commit)
-//          void commit(ia, in, const Ext&)
-//          C<T> coef(f, ia, in)      a_f(i) (a_0 == 1 when unit0)
-// LinEpi:  C<T> coef(f, ia, in)      b_f(i) (b_0 == 1 when unit0)
-//          void store(ia, in, C<T> s, Red<Acc,K>& acc), finalize(tot)
-template <int n, typename T, int F, int G, class Pro>
-__global__ void __launch_bounds__(512) k_passA_lin(Pro pro, C<T>* __restrict__ work, long long NF, Gate gate) {
-  if (gate.off()) return;
-  using Q = Cube<n, T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C<T>* s = reinterpret_cast<C<T>*>(smem_raw);
-  const long long col0 = (long long)blockIdx.x * G;
-  constexpr int items = G * Q::n2;
-  const int it = threadIdx.x;
-  const bool act = it < items;
-  const int cc = act ? it / Q::n2 : 0, l = act ? it % Q::n2 : 0;
-  const long long cb = (col0 + cc) * Q::n3;
-  C<T> u[n];
-  if (act) {
-    typename Pro::Ext e[n];
-#pragma unroll
-    for (int j = 0; j < n; ++j) u[j] = pro.load(cb + l + Q::n2 * j, cb + j + (long long)n * l, e[j]);
-#pragma unroll
-    for (int j = 0; j < n; ++j) pro.commit(cb + l + Q::n2 * j, cb + j + (long long)n * l, e[j]);
-  }
-#pragma unroll 1
-  for (int f = 0; f < F; ++f) {
-    if (act) {  // axis 1 in registers
-      T re[n], im[n];
-#pragma unroll
-      for (int j = 0; j < n; ++j) {
-        C<T> v = u[j];
-        if (!(Pro::unit0 && f == 0)) v = cmul<T>(pro.coef(f, cb + l + Q::n2 * j, cb + j + (long long)n * l), v);
-        re[j] = v.x;
-        im[j] = v.y;
-      }
-      Dft<n, +1, T>::run(re, im);
-      C<T>* sc = s + cc * Q::size + Q::line1(l);
-#pragma unroll
-      for (int j = 0; j < n; ++j) sc[j] = mk<T>(re[j], im[j]);
-    }
-    __syncthreads();
-    if (act) line_dft<n, +1, T>(s + cc * Q::size + Q::line2(l), Q::P1);  // axis 2
-    __syncthreads();
-    if (act) {  // axis 3 -> work (natural order), thread <-> m = i1 + n*i2
-      const C<T>* sc = s + cc * Q::size + Q::line3(l);
-      T re[n], im[n];
-#pragma unroll
-      for (int j = 0; j < n; ++j) {
-        const C<T> v = sc[Q::P2 * j];
-        re[j] = v.x;
-        im[j] = v.y;
-      }
-      Dft<n, +1, T>::run(re, im);
-      C<T>* wf = work + f * NF + cb + l;
-#pragma unroll
-      for (int j = 0; j < n; ++j) wf[(long long)Q::n2 * j] = mk<T>(re[j], im[j]);
-    }
-    __syncthreads();
+    for (int j = 0; j < n; ++j) wf[work_at<n, T>(l + Q::n2 * j, col0 + cc)] = mk<T>(re[j], im[j]);
   }
 }
 
 template <int n, typename T, int F, int G, class Epi>
-__global__ void __launch_bounds__(512) k_passC_lin(Epi epi, const C<T>* __restrict__ work, long long NF, Gate gate) {
+__global__ void __launch_bounds__(LinThreads<n, F, G>::value) k_passC_lin(Epi epi, const C<T>* __restrict__ work, long long NF, Gate gate) {
   if (gate.off()) return;
   using Q = Cube<n, T>;
   using A = typename Epi::Acc;
@@ -593,58 +535,59 @@ __global__ void __launch_bounds__(512) k_passC_lin(Epi epi, const C<T>* __restri
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C<T>* s = reinterpret_cast<C<T>*>(smem_raw);
   const long long col0 = (long long)blockIdx.x * G;
-  constexpr int items = G * Q::n2;
+  constexpr int per_f = G * Q::n2;
   const int it = threadIdx.x;
-  const bool act = it < items;
-  const int cc = act ? it / Q::n2 : 0, l = act ? it % Q::n2 : 0;
-  const long long cb = (col0 + cc) * Q::n3;
-  C<T> sum[n];
+  const bool act = it < F * per_f;
+  const int f = act ? it / per_f : 0, rem = act ? it % per_f : 0;
+  const int cc = rem / Q::n2, l = rem % Q::n2;
+  C<T>* cube = s + (f * G + cc) * Q::size;
+  if (act) {  // axis 3 from work (tile-major), thread <-> m = i1 + n*i2
+    const C<T>* wf = work + f * NF;
+    T re[n], im[n];
 #pragma unroll
-  for (int j = 0; j < n; ++j) sum[j] = mk<T>(0, 0);
-#pragma unroll 1
-  for (int f = 0; f < F; ++f) {
-    if (act) {  // axis 3 from work (natural order), thread <-> m = i1 + n*i2
-      const C<T>* wf = work + f * NF + cb + l;
-      T re[n], im[n];
-#pragma unroll
-      for (int j = 0; j < n; ++j) {
-        const C<T> v = wf[(long long)Q::n2 * j];
-        re[j] = v.x;
-        im[j] = v.y;
-      }
-      Dft<n, -1, T>::run(re, im);
-      C<T>* sc = s + cc * Q::size + Q::line3(l);
-#pragma unroll
-      for (int j = 0; j < n; ++j) sc[Q::P2 * j] = mk<T>(re[j], im[j]);
+    for (int j = 0; j < n; ++j) {
+      const C<T> v = wf[work_at<n, T>(l + Q::n2 * j, col0 + cc)];
+      re[j] = v.x;
+      im[j] = v.y;
     }
-    __syncthreads();
-    if (act) line_dft<n, -1, T>(s + cc * Q::size + Q::line2(l), Q::P1);  // axis 2
-    __syncthreads();
-    if (act) {  // axis 1 in registers, accumulate b_f v_f
-      const C<T>* sc = s + cc * Q::size + Q::line1(l);
-      T re[n], im[n];
+    Dft<n, -1, T>::run(re, im);
+    C<T>* sc = cube + Q::line3(l);
 #pragma unroll
-      for (int j = 0; j < n; ++j) {
-        const C<T> v = sc[j];
-        re[j] = v.x;
-        im[j] = v.y;
-      }
-      Dft<n, -1, T>::run(re, im);
-#pragma unroll
-      for (int j = 0; j < n; ++j) {
-        C<T> v = mk<T>(re[j], im[j]);
-        if (!(Epi::unit0 && f == 0)) v = cmul<T>(epi.coef(f, cb + l + Q::n2 * j, cb + j + (long long)n * l), v);
-        sum[j] = cadd<T>(sum[j], v);
-      }
-    }
-    __syncthreads();
+    for (int j = 0; j < n; ++j) sc[Q::P2 * j] = mk<T>(re[j], im[j]);
   }
+  __syncthreads();
+  if (act) line_dft<n, -1, T>(cube + Q::line2(l), Q::P1);  // axis 2
+  __syncthreads();
+  if (act) line_dft<n, -1, T>(cube + Q::line1(l), 1);  // axis 1
+  __syncthreads();
+  // combine the fields mode by mode; modes are enumerated in the order of the
+  // epilogue's vectors (line order q = l + n^2 j, or natural order j + n l) so
+  // that consecutive threads touch consecutive addresses; all of a thread's
+  // modes are unrolled so that their loads are in flight together.
   Red<A, (K > 0 ? K : 1)> acc;
 #pragma unroll
   for (int k = 0; k < (K > 0 ? K : 1); ++k) acc.v[k] = 0;
-  if (act) {
+  constexpr int modes = G * Q::n3, nthr = LinThreads<n, F, G>::value;
+  constexpr int per_thread = (modes + nthr - 1) / nthr;
+  constexpr bool nat = EpiNatural<Epi>::value;
 #pragma unroll
-    for (int j = 0; j < n; ++j) epi.store(cb + l + Q::n2 * j, cb + j + (long long)n * l, sum[j], acc);
+  for (int r = 0; r < per_thread; ++r) {
+    const int idx = it + r * nthr;
+    if (idx < modes) {
+      const int c2 = idx / Q::n3, q = idx % Q::n3;
+      const int j = nat ? q % n : q / Q::n2, l2 = nat ? q / n : q % Q::n2;
+      const long long cb = (col0 + c2) * Q::n3;
+      const long long ia = cb + l2 + (long long)Q::n2 * j, in = cb + j + (long long)n * l2;
+      const int pos = Q::line1(l2) + j;
+      C<T> sum = mk<T>(0, 0);
+#pragma unroll
+      for (int g = 0; g < F; ++g) {
+        C<T> v = s[(g * G + c2) * Q::size + pos];
+        if (!(Epi::unit0 && g == 0)) v = cmul<T>(epi.coef(g, ia, in), v);
+        sum = cadd<T>(sum, v);
+      }
+      epi.store(ia, in, sum, acc);
+    }
   }
   if constexpr (K > 0) {
     grid_sum_finalize<A, K>(acc, epi.partials, epi.counter, [&](const Red<A, K>& tot) { epi.finalize(tot); });

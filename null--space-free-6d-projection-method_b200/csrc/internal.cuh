@@ -17,8 +17,9 @@ struct fame_mass {
   fame_ctx* ctx = nullptr;
   int N = 0, n = 0;
   long long NF = 0;
-  double* Es64 = nullptr;  // E / NF, FP64
-  float* Es32 = nullptr;   // E / NF, FP32
+  double* Et64 = nullptr;  // E / NF, FP64, pass-B tile order of the FP64 chains (k_tile_E)
+  float* Et32 = nullptr;   // E / NF, FP32, pass-B tile order of the FP32 chains
+  void* work = nullptr;    // one NF-field of complex128 scratch for the mass modes
 };
 
 struct fame_basis {
@@ -51,4 +52,6 @@ int dalloc(void** p, size_t bytes);
 void dfree(void* p);
 // copy a small device struct to host (synchronises the stream)
 int read_back(fame_ctx* ctx, const void* dsrc, void* hdst, size_t bytes);
+// FAME_ERR_CUDA (and clears the word) if a bounded device-side wait gave up on ctx's device
+int check_fault(fame_ctx* ctx);
 }  // namespace fame

@@ -97,8 +97,8 @@ template <> MhatCoef<double> coef_of<double>(fame_basis* b) { return MhatCoef<do
 template <> MhatCoef<float> coef_of<float>(fame_basis* b) { return MhatCoef<float>{b->invCf, b->W1f, b->W2f}; }
 template <> MhatCoef<double> coef_line_of<double>(fame_basis* b) { return MhatCoef<double>{b->invC_l, b->W1_l, b->W2_l}; }
 template <> MhatCoef<float> coef_line_of<float>(fame_basis* b) { return MhatCoef<float>{b->invCf_l, b->W1f_l, b->W2f_l}; }
-template <> const double* es_of<double>(fame_mass* m) { return m->Es64; }
-template <> const float* es_of<float>(fame_mass* m) { return m->Es32; }
+template <> const double* es_of<double>(fame_mass* m) { return m->Et64; }
+template <> const float* es_of<float>(fame_mass* m) { return m->Et32; }
 
 int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
   fame_basis* bs = K->b;
@@ -114,7 +114,7 @@ int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
     EpiKrPre epi{c64, K->mr1, K->mr2, K->bhat, B.r, B.x, st, tolMhat,
                  K->o.prec_mode == FAME_PREC_MIXED ? K->o.maxRefine : K->o.maxitCG,
                  K->partials, K->counter};
-    FAME_TRY((run_chain<double, 2>(K->n, pro, epi, B.work, K->m->Es64, 1.0, NF, s)));
+    FAME_TRY((run_chain<double, 2>(K->n, pro, epi, B.work, K->m->Et64, NF, s)));
     K->stats.massApplies += 2;
   }
   PcgState h{};
@@ -159,7 +159,7 @@ int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
       // u += dx ; r64 = bhat - Mhat u  (FP64 residual)
       ProResidMhat<double, float, true> pro{c, B.x, F.x};
       EpiResidMhat<double> epi{c, K->bhat, B.r, &st->rho, K->partials, K->counter};
-      FAME_TRY((run_chain_lin<double, 3>(K->n, pro, epi, B.work, K->m->Es64, 1.0, NF, s)));
+      FAME_TRY((run_chain_lin<double, 3>(K->n, pro, epi, B.work, K->m->Et64, NF, s)));
       K->stats.massApplies += 3;
       FAME_TRY(read_back(K->ctx, st, &h, sizeof(PcgState)));
       rn2 = h.rho;
@@ -176,7 +176,7 @@ int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
     ProKrPost pro{c64, B.x};
     EpiKrPost epi{K->mr1, K->mr2, bs->V1(0, 0), bs->V1(0, 1), bs->V1(1, 0), bs->V1(1, 1), bs->det, y, NF, st,
                   K->partials, K->counter};
-    FAME_TRY((run_chain<double, 2>(K->n, pro, epi, B.work, K->m->Es64, 1.0, NF, s)));
+    FAME_TRY((run_chain<double, 2>(K->n, pro, epi, B.work, K->m->Et64, NF, s)));
     K->stats.massApplies += 2;
   }
   FAME_TRY(read_back(K->ctx, st, &h, sizeof(PcgState)));
@@ -225,11 +225,11 @@ int fame_apply_Mhat_C_scalar_compact(fame_basis* b, fame_mass* m, const void* x,
   if (prec == FAME_F64) {
     const MhatCoef<double> c = coef_of<double>(b);
     return run_chain_lin<double, 3>(b->n, ProMhat<double, false>{c, (const double2*)x}, EpiMhat<double, false>{c, (double2*)y},
-                                work, m->Es64, 1.0, b->NF, s);
+                                work, m->Et64, b->NF, s);
   }
   const MhatCoef<float> c = coef_of<float>(b);
   return run_chain_lin<float, 3>(b->n, ProMhat<float, false>{c, (const float2*)x}, EpiMhat<float, false>{c, (float2*)y},
-                             (float2*)work, m->Es32, 1.0f, b->NF, s);
+                             (float2*)work, m->Et32, b->NF, s);
 }
 
 int fame_krinv_default_opts(fame_krinv_opts* o) {

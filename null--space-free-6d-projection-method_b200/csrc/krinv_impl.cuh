@@ -69,12 +69,12 @@ template <typename T> struct OpMhat {
   int matvec(fame_krinv* K, PcgBuf<T>& B, PcgState* st, cudaStream_t s) const {
     ProPcgMhat<T> pro{c, B.p, B.r, st};
     EpiPcgMhat<T> epi{c, B.Ap, B.p, st, reinterpret_cast<T*>(K->partials), K->counter};
-    return run_chain_lin<T, 3>(K->n, pro, epi, B.work, Es, (T)1, K->NF, s, Gate{&st->active});
+    return run_chain_lin<T, 3>(K->n, pro, epi, B.work, Es, K->NF, s, Gate{&st->active});
   }
   int resid(fame_krinv* K, PcgBuf<T>& B, const C<T>* b, double* out, cudaStream_t s) const {
     ProResidMhat<T, T, false> pro{c, B.x, nullptr};
     EpiResidMhat<T> epi{c, b, B.r, out, reinterpret_cast<T*>(K->partials), K->counter};
-    return run_chain_lin<T, 3>(K->n, pro, epi, B.work, Es, (T)1, K->NF, s);
+    return run_chain_lin<T, 3>(K->n, pro, epi, B.work, Es, K->NF, s);
   }
 };
 
@@ -85,12 +85,12 @@ template <typename T> struct OpM3 {
   int matvec(fame_krinv* K, PcgBuf<T>& B, PcgState* st, cudaStream_t s) const {
     ProPcgM3<T> pro{B.p, B.r, st, K->NF};
     EpiPcgM3<T> epi{B.Ap, B.p, st, K->NF, reinterpret_cast<T*>(K->partials), K->counter};
-    return run_chain<T, 3>(K->n, pro, epi, B.work, Es, (T)1, K->NF, s, Gate{&st->active});
+    return run_chain<T, 3>(K->n, pro, epi, B.work, Es, K->NF, s, Gate{&st->active});
   }
   int resid(fame_krinv* K, PcgBuf<T>& B, const C<T>* b, double* out, cudaStream_t s) const {
     ProResidM3<T, T, false> pro{B.x, nullptr, K->NF};
     EpiResidM3<T> epi{b, B.r, out, K->NF, reinterpret_cast<T*>(K->partials), K->counter};
-    return run_chain<T, 3>(K->n, pro, epi, B.work, Es, (T)1, K->NF, s);
+    return run_chain<T, 3>(K->n, pro, epi, B.work, Es, K->NF, s);
   }
 };
 

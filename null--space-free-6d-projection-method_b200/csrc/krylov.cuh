@@ -105,6 +105,7 @@ template <typename T, bool LINE> struct EpiMhat {
   using Acc = T;
   static constexpr int K = 0;
   static constexpr bool unit0 = true;
+  static constexpr bool natural = !LINE;
   MhatCoef<T> c;
   C<T>* y;
   T* partials = nullptr;

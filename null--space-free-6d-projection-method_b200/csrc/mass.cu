@@ -7,13 +7,26 @@
 
 namespace fame {
 
-__global__ void k_scale_E(const double* E, long long NF, double s, double* o64, float* o32) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < NF;
-       i += (long long)gridDim.x * blockDim.x) {
-    const double v = E[i] * s;
-    o64[i] = v;
-    o32[i] = (float)v;
+// Pass-B tile width of the chains in precision T for a runtime axis length n.
+template <typename T> int work_tt(int n) {
+  switch (n) {
+    case 2: return WorkTile<2, T>::TT;
+    case 4: return WorkTile<4, T>::TT;
+    case 6: return WorkTile<6, T>::TT;
+    case 8: return WorkTile<8, T>::TT;
+    case 10: return WorkTile<10, T>::TT;
+    case 12: return WorkTile<12, T>::TT;
+    default: return WorkTile<14, T>::TT;
   }
+}
+
+// E*scale in the pass-B tile order of the chains in precision T.
+template <typename T> int tile_E(const double* E, int n, long long NF, double scale, T* out, cudaStream_t st) {
+  const int blocks = (int)std::min<long long>((NF + 255) / 256, 148 * 16);
+  k_tile_E<T><<<blocks, 256, 0, st>>>(E, n, work_tt<T>(n), NF, scale, out);
+  ::fame::count_launch();
+  FAME_CUDA_TRY(cudaGetLastError());
+  return FAME_OK;
 }
 
 // Verify that (inputIdx, targetIdx, M) is the radix rank-1 plan of
@@ -33,23 +46,17 @@ __global__ void k_check_rank1(const uint32_t* in, const uint32_t* tg, long long 
   }
 }
 
+// Scalar mass action on ncols columns.  work: one NF-field of scratch that
+// must not alias x or y (pass C reads it tile-major while writing y by columns).
 template <typename T>
-int mass_scalar_cols(int n, long long NF, const C<T>* x, C<T>* y, int ncols, const double* Es64,
-                     const float* Es32, double escale, cudaStream_t st) {
+int mass_scalar_cols(int n, long long NF, const C<T>* x, C<T>* y, int ncols, const T* Et, C<T>* work,
+                     cudaStream_t st) {
   for (int j = 0; j < ncols; ++j) {
     ProCols<T, 1> pro;
     pro.x[0] = x + (long long)j * NF;
     EpiCols<T, 1> epi;
     epi.y[0] = y + (long long)j * NF;
-    if constexpr (sizeof(T) == 8) {
-      FAME_TRY((run_chain<T, 1>(n, pro, epi, y + (long long)j * NF, Es64, escale, NF, st)));
-    } else {
-      if (Es32) {
-        FAME_TRY((run_chain<T, 1>(n, pro, epi, y + (long long)j * NF, Es32, (float)escale, NF, st)));
-      } else {
-        FAME_TRY((run_chain<T, 1>(n, pro, epi, y + (long long)j * NF, Es64, escale, NF, st)));
-      }
-    }
+    FAME_TRY((run_chain<T, 1>(n, pro, epi, work, Et, NF, st)));
   }
   return FAME_OK;
 }
@@ -57,14 +64,18 @@ int mass_scalar_cols(int n, long long NF, const C<T>* x, C<T>* y, int ncols, con
 // out[t] = (1/NF) sum_y g_t(y) sum_c |w_c(y)|^2, w_c the unnormalised inverse DFT
 // of component c, i.e. NF sum_y g_t(y) sum_c |ifftn(x_c)(y)|^2 = x^H (dM/dtheta_t) x.
 constexpr int kMaxAdjParams = 8;
-__global__ void k_adjoint_reduce(const double2* w, long long NF, const double* g, int np,
+__global__ void k_adjoint_reduce(const double2* w, long long NF, int n, int TT, const double* g, int np,
                                  double* partials, unsigned* counter, double* out) {
+  const long long n3 = (long long)n * n * n;
   Red<double, kMaxAdjParams> acc{};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < NF; i += (long long)gridDim.x * blockDim.x) {
+    // w is tile-major (WorkTile): element i holds grid point c123 + n^3*c456
+    const long long rr = i / TT, c456 = rr % n3, c123 = (rr / n3) * TT + i % TT;
+    const long long y = c123 + n3 * c456;
     const double d = cabs2<double>(w[i]) + cabs2<double>(w[NF + i]) + cabs2<double>(w[2 * NF + i]);
 #pragma unroll
     for (int t = 0; t < kMaxAdjParams; ++t)
-      if (t < np) acc.v[t] += g[(long long)t * NF + i] * d;
+      if (t < np) acc.v[t] += g[(long long)t * NF + y] * d;
   }
   const double inv = 1.0 / (double)NF;
   grid_sum_finalize<double, kMaxAdjParams>(acc, partials, counter, [&](const Red<double, kMaxAdjParams>& tot) {
@@ -74,15 +85,14 @@ __global__ void k_adjoint_reduce(const double2* w, long long NF, const double* g
 
 template <int n>
 int adjoint_inverse_n(const double2* x, double2* work, long long NF, cudaStream_t st) {
-  using Q = Cube<n, double>;
+  using G = PassBGeom<n, double>;
   ProCols<double, 3> pro;
   for (int c = 0; c < 3; ++c) pro.x[c] = x + c * NF;
   FAME_TRY((launch_passA<n, double, 3>(pro, work, NF, st, Gate{nullptr})));
-  constexpr int TT = PassBTile<double>::TT;
-  const size_t smem = (size_t)TT * Q::size * sizeof(double2);
-  static int attr = ensure_smem(k_passB_inv<n, double, TT>, smem);
+  const size_t smem = (size_t)G::stage * sizeof(double2);
+  static int attr = ensure_smem(k_passB_inv<n, double>, smem);
   if (attr != FAME_OK) return attr;
-  k_passB_inv<n, double, TT><<<dim3(Q::n3 / TT, 3), std::min(512, std::max(64, round32(TT * Q::n2))), smem, st>>>(work, NF);
+  k_passB_inv<n, double><<<dim3(G::n3 / G::TT, 3), G::threads, smem, st>>>(work, NF);
   ::fame::count_launch();
   FAME_CUDA_TRY(cudaGetLastError());
   return FAME_OK;
@@ -100,35 +110,55 @@ long long grid_NF(int N) {
 }
 
 // mode dispatch on a typed pointer pair
+template <typename T> const T* et_of(fame_mass* m);
+template <> const double* et_of<double>(fame_mass* m) { return m->Et64; }
+template <> const float* et_of<float>(fame_mass* m) { return m->Et32; }
+
+// mode dispatch on a typed pointer pair
 template <typename T>
 int mass_apply_typed(fame_mass* m, int mode, const C<T>* x, C<T>* y, int nrhs) {
   const long long NF = m->NF;
   cudaStream_t st = m->ctx->stream;
-  const double* E64 = m->Es64;
-  const float* E32 = m->Es32;
+  const T* Et = et_of<T>(m);
+  C<T>* work = reinterpret_cast<C<T>*>(m->work);
   switch (mode) {
     case FAME_MASS_SCALAR:
-      return mass_scalar_cols<T>(m->n, NF, x, y, nrhs, E64, E32, 1.0, st);
+      return mass_scalar_cols<T>(m->n, NF, x, y, nrhs, Et, work, st);
     case FAME_MASS_FULL3:
       // 3NF x nrhs, column-major: each column holds three components
-      return mass_scalar_cols<T>(m->n, NF, x, y, 3 * nrhs, E64, E32, 1.0, st);
+      return mass_scalar_cols<T>(m->n, NF, x, y, 3 * nrhs, Et, work, st);
     case FAME_MASS_COL3:
       for (int j = 0; j < nrhs; ++j) {
         C<T>* yj = y + 3LL * NF * j;
         FAME_CUDA_TRY(cudaMemsetAsync(yj, 0, 2 * NF * sizeof(C<T>), st));
-        FAME_TRY(mass_scalar_cols<T>(m->n, NF, x + NF * j, yj + 2 * NF, 1, E64, E32, 1.0, st));
+        FAME_TRY(mass_scalar_cols<T>(m->n, NF, x + NF * j, yj + 2 * NF, 1, Et, work, st));
       }
       return FAME_OK;
     case FAME_MASS_COLS12:
       for (int j = 0; j < nrhs; ++j) {
         C<T>* yj = y + 3LL * NF * j;
-        FAME_TRY(mass_scalar_cols<T>(m->n, NF, x + 2 * NF * j, yj, 2, E64, E32, 1.0, st));
+        FAME_TRY(mass_scalar_cols<T>(m->n, NF, x + 2 * NF * j, yj, 2, Et, work, st));
         FAME_CUDA_TRY(cudaMemsetAsync(yj + 2 * NF, 0, NF * sizeof(C<T>), st));
       }
       return FAME_OK;
     default:
       return fail(FAME_ERR_INVALID, "unknown mass mode");
   }
+}
+
+// One-shot applyMij_fft with a caller's natural-order E: a temporary tiled E/NF.
+template <typename T>
+int apply_fft_raw(fame_ctx* ctx, int n, long long NF, const double* E, const C<T>* x, C<T>* y, int nrhs) {
+  T* Et = nullptr;
+  C<T>* work = nullptr;
+  FAME_TRY(dalloc((void**)&Et, NF * sizeof(T)));
+  int s = dalloc((void**)&work, NF * sizeof(C<T>));
+  if (s == FAME_OK) s = tile_E<T>(E, n, NF, 1.0 / (double)NF, Et, ctx->stream);
+  if (s == FAME_OK) s = mass_scalar_cols<T>(n, NF, x, y, nrhs, Et, work, ctx->stream);
+  if (s == FAME_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) s = fail(FAME_ERR_CUDA, "applyMij_fft");
+  dfree(Et);
+  dfree(work);
+  return s;
 }
 
 }  // namespace fame
@@ -142,13 +172,8 @@ int fame_applyMij_fft(fame_ctx* ctx, int N, const double* E, const void* x, void
   if (!ctx || !E || !x || !y || nrhs < 0) return fail(FAME_ERR_INVALID, "applyMij_fft arguments");
   FAME_TRY(check_N(N));
   const long long NF = grid_NF(N);
-  const double escale = 1.0 / (double)NF;
-  if (prec == FAME_F64)
-    return mass_scalar_cols<double>(2 * N, NF, (const double2*)x, (double2*)y, nrhs, E, nullptr,
-                                    escale, ctx->stream);
-  if (prec == FAME_F32)
-    return mass_scalar_cols<float>(2 * N, NF, (const float2*)x, (float2*)y, nrhs, E, nullptr,
-                                   escale, ctx->stream);
+  if (prec == FAME_F64) return apply_fft_raw<double>(ctx, 2 * N, NF, E, (const double2*)x, (double2*)y, nrhs);
+  if (prec == FAME_F32) return apply_fft_raw<float>(ctx, 2 * N, NF, E, (const float2*)x, (float2*)y, nrhs);
   return fail(FAME_ERR_INVALID, "prec must be FAME_F64 or FAME_F32");
 }
 
@@ -161,17 +186,19 @@ int fame_mass_create(fame_ctx* ctx, int N, const double* E, fame_mass** out) {
   m->N = N;
   m->n = 2 * N;
   m->NF = grid_NF(N);
-  int s = dalloc((void**)&m->Es64, m->NF * sizeof(double));
-  if (s == FAME_OK) s = dalloc((void**)&m->Es32, m->NF * sizeof(float));
+  int s = dalloc((void**)&m->Et64, m->NF * sizeof(double));
+  if (s == FAME_OK) s = dalloc((void**)&m->Et32, m->NF * sizeof(float));
+  if (s == FAME_OK) s = dalloc(&m->work, m->NF * sizeof(double2));
+  const double scale = 1.0 / (double)m->NF;
+  if (s == FAME_OK) s = tile_E<double>(E, m->n, m->NF, scale, m->Et64, ctx->stream);
+  if (s == FAME_OK) s = tile_E<float>(E, m->n, m->NF, scale, m->Et32, ctx->stream);
   if (s != FAME_OK) {
-    dfree(m->Es64);
+    dfree(m->Et64);
+    dfree(m->Et32);
+    dfree(m->work);
     delete m;
     return s;
   }
-  const int blocks = (int)std::min<long long>((m->NF + 255) / 256, 148 * 16);
-  k_scale_E<<<blocks, 256, 0, ctx->stream>>>(E, m->NF, 1.0 / (double)m->NF, m->Es64, m->Es32);
-  ::fame::count_launch();
-  FAME_CUDA_TRY(cudaGetLastError());
   *out = m;
   return FAME_OK;
 }
@@ -179,8 +206,9 @@ int fame_mass_create(fame_ctx* ctx, int N, const double* E, fame_mass** out) {
 int fame_mass_destroy(fame_mass* m) {
   if (!m) return FAME_OK;
   cudaStreamSynchronize(m->ctx->stream);
-  dfree(m->Es64);
-  dfree(m->Es32);
+  dfree(m->Et64);
+  dfree(m->Et32);
+  dfree(m->work);
   delete m;
   return FAME_OK;
 }
@@ -219,7 +247,8 @@ int fame_mass_adjoint(fame_mass* m, const void* X, int nmodes, const double* dEp
       default: s = fail(FAME_ERR_UNSUPPORTED, "adjoint: unsupported N");
     }
     if (s != FAME_OK) break;
-    k_adjoint_reduce<<<blocks, 256, 0, st>>>(work, NF, dEps, nparams, red + kMaxAdjParams, counter, red);
+    k_adjoint_reduce<<<blocks, 256, 0, st>>>(work, NF, m->n, work_tt<double>(m->n), dEps, nparams,
+                                             red + kMaxAdjParams, counter, red);
     ::fame::count_launch();
     double h[kMaxAdjParams];
     s = cudaGetLastError() == cudaSuccess ? read_back(m->ctx, red, h, sizeof(h)) : fail(FAME_ERR_CUDA, "adjoint launch");

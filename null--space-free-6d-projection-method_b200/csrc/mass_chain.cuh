@@ -1,13 +1,11 @@
 // Host-side launch of one fused mass-operator chain (pass A -> B -> C) for a
 // runtime axis length n = 2N, dispatching to the compile-time kernels.
 #pragma once
-#include "fft6d.cuh"
+#include "passb.cuh"
 
 namespace fame {
 
 inline int round32(int x) { return (x + 31) / 32 * 32; }
-
-template <typename T> struct PassBTile { static constexpr int TT = 32 / (int)sizeof(C<T>) >= 1 ? 32 / (int)sizeof(C<T>) : 1; };
 
 // Set the dynamic shared-memory limit of a kernel once per process.
 template <typename K> int ensure_smem(K kernel, size_t bytes) {
@@ -16,17 +14,23 @@ template <typename K> int ensure_smem(K kernel, size_t bytes) {
   return FAME_OK;
 }
 
+// Pass B over nfields tile-major fields with the tiled material Et (E/NF in the
+// layout of k_tile_E for this n and T): a persistent grid of (resident CTAs per
+// SM) x SMs, each CTA owning a contiguous range of (tile, field) units.
 template <int n, typename T, typename TE>
-int launch_passB(C<T>* work, int nfields, const TE* Es, TE escale, long long NF, cudaStream_t st, Gate gate) {
-  using Q = Cube<n, T>;
-  constexpr int TT = PassBTile<T>::TT;
-  static_assert(Q::n3 % TT == 0, "tile must divide n^3");
-  const size_t smem = (size_t)TT * Q::size * sizeof(C<T>);
-  static int attr = ensure_smem(k_passB<n, T, TT, TE>, smem);
+int launch_passB(C<T>* work, int nfields, const TE* Et, long long NF, cudaStream_t st, Gate gate) {
+  using G = PassBGeom<n, T>;
+  constexpr size_t smem = G::template smem_bytes<TE>();
+  static int attr = ensure_smem(k_passB<n, T, TE>, smem);
   if (attr != FAME_OK) return attr;
-  const int threads = std::min(512, std::max(64, round32(TT * Q::n2)));
-  dim3 grid(Q::n3 / TT, nfields);
-  k_passB<n, T, TT, TE><<<grid, threads, smem, st>>>(work, Es, escale, NF, gate);
+  static int per_sm = [] {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_passB<n, T, TE>, G::threads, smem) != cudaSuccess) b = 1;
+    return b < 1 ? 1 : b;
+  }();
+  const int units = (G::n3 / G::TT) * nfields;
+  const int grid = std::min(units, per_sm * num_sms());
+  k_passB<n, T, TE><<<grid, G::threads, smem, st>>>(work, Et, nfields, NF, gate, fault_word());
   ::fame::count_launch();
   return FAME_OK;
 }
@@ -61,10 +65,10 @@ int launch_passC(const Epi& epi, const C<T>* work, long long NF, cudaStream_t st
 inline long long passC_blocks(int n) { return (long long)n * n * n; }
 
 template <int n, typename T, int F, class Pro, class Epi, typename TE>
-int chain_n(const Pro& pro, const Epi& epi, C<T>* work, const TE* Es, TE escale, long long NF,
+int chain_n(const Pro& pro, const Epi& epi, C<T>* work, const TE* Et, long long NF,
             cudaStream_t st, Gate gate) {
   FAME_TRY((launch_passA<n, T, F, Pro>(pro, work, NF, st, gate)));
-  FAME_TRY((launch_passB<n, T, TE>(work, F, Es, escale, NF, st, gate)));
+  FAME_TRY((launch_passB<n, T, TE>(work, F, Et, NF, st, gate)));
   FAME_TRY((launch_passC<n, T, F, Epi>(epi, work, NF, st, gate)));
   FAME_CUDA_TRY(cudaGetLastError());
   return FAME_OK;
@@ -72,40 +76,39 @@ int chain_n(const Pro& pro, const Epi& epi, C<T>* work, const TE* Es, TE escale,
 
 // y-chain for axis length n in {2,4,...,14}.  work holds F fields of NF.
 template <typename T, int F, class Pro, class Epi, typename TE>
-int run_chain(int n, const Pro& pro, const Epi& epi, C<T>* work, const TE* Es, TE escale,
-              long long NF, cudaStream_t st, Gate gate = Gate{nullptr}) {
+int run_chain(int n, const Pro& pro, const Epi& epi, C<T>* work, const TE* Et, long long NF, cudaStream_t st, Gate gate = Gate{nullptr}) {
   switch (n) {
-    case 2: return chain_n<2, T, F>(pro, epi, work, Es, escale, NF, st, gate);
-    case 4: return chain_n<4, T, F>(pro, epi, work, Es, escale, NF, st, gate);
-    case 6: return chain_n<6, T, F>(pro, epi, work, Es, escale, NF, st, gate);
-    case 8: return chain_n<8, T, F>(pro, epi, work, Es, escale, NF, st, gate);
-    case 10: return chain_n<10, T, F>(pro, epi, work, Es, escale, NF, st, gate);
-    case 12: return chain_n<12, T, F>(pro, epi, work, Es, escale, NF, st, gate);
-    case 14: return chain_n<14, T, F>(pro, epi, work, Es, escale, NF, st, gate);
+    case 2: return chain_n<2, T, F>(pro, epi, work, Et, NF, st, gate);
+    case 4: return chain_n<4, T, F>(pro, epi, work, Et, NF, st, gate);
+    case 6: return chain_n<6, T, F>(pro, epi, work, Et, NF, st, gate);
+    case 8: return chain_n<8, T, F>(pro, epi, work, Et, NF, st, gate);
+    case 10: return chain_n<10, T, F>(pro, epi, work, Et, NF, st, gate);
+    case 12: return chain_n<12, T, F>(pro, epi, work, Et, NF, st, gate);
+    case 14: return chain_n<14, T, F>(pro, epi, work, Et, NF, st, gate);
     default: return fail(FAME_ERR_UNSUPPORTED, "mass operator supports 2N in {2,4,...,14}");
   }
 }
 
-// Columns per CTA of the linear-field passes (one line per thread).
-template <int n, typename T> struct LinCols {
-  static constexpr int value = n == 2 ? 8 : n == 4 ? 16 : n == 6 ? 12 : n == 8 ? 8 : n == 10 ? 4 : n == 12 ? 2 : 2;
-  static_assert((n * n * n) % value == 0 && value * n * n <= 512, "linear chain tiling");
+// Columns per CTA of the linear-field passes (F*G*n^2 threads, F*G cubes).
+template <int n, typename T, int F> struct LinCols {
+  static constexpr int value = n == 2 ? 8 : n == 4 ? 8 : n == 6 ? 4 : n == 8 ? 2 : 1;
+  static_assert((n * n * n) % value == 0 && F * value * n * n <= 1024, "linear chain tiling");
 };
 
 template <int n, typename T, int F, class Pro, class Epi, typename TE>
-int chain_lin_n(const Pro& pro, const Epi& epi, C<T>* work, const TE* Es, TE escale, long long NF,
+int chain_lin_n(const Pro& pro, const Epi& epi, C<T>* work, const TE* Et, long long NF,
                 cudaStream_t st, Gate gate) {
   using Q = Cube<n, T>;
-  constexpr int G = LinCols<n, T>::value;
-  const size_t smem = (size_t)G * Q::size * sizeof(C<T>);
-  const int threads = round32(G * Q::n2);
+  constexpr int G = LinCols<n, T, F>::value;
+  const size_t smem = (size_t)F * G * Q::size * sizeof(C<T>);
+  const int threads = LinThreads<n, F, G>::value;
   static int attrA = ensure_smem(k_passA_lin<n, T, F, G, Pro>, smem);
   static int attrC = ensure_smem(k_passC_lin<n, T, F, G, Epi>, smem);
   if (attrA != FAME_OK) return attrA;
   if (attrC != FAME_OK) return attrC;
   k_passA_lin<n, T, F, G, Pro><<<Q::n3 / G, threads, smem, st>>>(pro, work, NF, gate);
   ::fame::count_launch();
-  FAME_TRY((launch_passB<n, T, TE>(work, F, Es, escale, NF, st, gate)));
+  FAME_TRY((launch_passB<n, T, TE>(work, F, Et, NF, st, gate)));
   k_passC_lin<n, T, F, G, Epi><<<Q::n3 / G, threads, smem, st>>>(epi, work, NF, gate);
   ::fame::count_launch();
   FAME_CUDA_TRY(cudaGetLastError());
@@ -114,16 +117,15 @@ int chain_lin_n(const Pro& pro, const Epi& epi, C<T>* work, const TE* Es, TE esc
 
 // Linear-field chain (see k_passA_lin) for axis length n in {2,4,...,14}.
 template <typename T, int F, class Pro, class Epi, typename TE>
-int run_chain_lin(int n, const Pro& pro, const Epi& epi, C<T>* work, const TE* Es, TE escale,
-                  long long NF, cudaStream_t st, Gate gate = Gate{nullptr}) {
+int run_chain_lin(int n, const Pro& pro, const Epi& epi, C<T>* work, const TE* Et, long long NF, cudaStream_t st, Gate gate = Gate{nullptr}) {
   switch (n) {
-    case 2: return chain_lin_n<2, T, F>(pro, epi, work, Es, escale, NF, st, gate);
-    case 4: return chain_lin_n<4, T, F>(pro, epi, work, Es, escale, NF, st, gate);
-    case 6: return chain_lin_n<6, T, F>(pro, epi, work, Es, escale, NF, st, gate);
-    case 8: return chain_lin_n<8, T, F>(pro, epi, work, Es, escale, NF, st, gate);
-    case 10: return chain_lin_n<10, T, F>(pro, epi, work, Es, escale, NF, st, gate);
-    case 12: return chain_lin_n<12, T, F>(pro, epi, work, Es, escale, NF, st, gate);
-    case 14: return chain_lin_n<14, T, F>(pro, epi, work, Es, escale, NF, st, gate);
+    case 2: return chain_lin_n<2, T, F>(pro, epi, work, Et, NF, st, gate);
+    case 4: return chain_lin_n<4, T, F>(pro, epi, work, Et, NF, st, gate);
+    case 6: return chain_lin_n<6, T, F>(pro, epi, work, Et, NF, st, gate);
+    case 8: return chain_lin_n<8, T, F>(pro, epi, work, Et, NF, st, gate);
+    case 10: return chain_lin_n<10, T, F>(pro, epi, work, Et, NF, st, gate);
+    case 12: return chain_lin_n<12, T, F>(pro, epi, work, Et, NF, st, gate);
+    case 14: return chain_lin_n<14, T, F>(pro, epi, work, Et, NF, st, gate);
     default: return fail(FAME_ERR_UNSUPPORTED, "mass operator supports 2N in {2,4,...,14}");
   }
 }

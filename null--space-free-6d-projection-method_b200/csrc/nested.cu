@@ -174,7 +174,7 @@ static int inner_m3_solve(fame_krinv* K) {
   PcgState h{};
   const double tolM = K->o.tolM;
   if (K->o.prec_mode == FAME_PREC_FP64) {
-    FAME_TRY(pcg_iterate<double>(K, OpM3<double>{K->m->Es64}, B, K->st64, K->lastIt64, h,
+    FAME_TRY(pcg_iterate<double>(K, OpM3<double>{K->m->Et64}, B, K->st64, K->lastIt64, h,
                                  K->o.verifyTrueResidual != 0, K->bhat));
     if (h.flag == -1) return fail(FAME_ERR_NONFINITE, "nested inner right-hand side is NaN/Inf");
     const double rr = h.bnorm2 > 0 ? std::sqrt(h.rho / h.bnorm2) : 0.0;
@@ -199,13 +199,13 @@ static int inner_m3_solve(fame_krinv* K) {
                                                     K->o.maxitM, partials32, K->counter);
     ::fame::count_launch();
     PcgState h32{};
-    FAME_TRY(pcg_iterate<float>(K, OpM3<float>{K->m->Es32}, F, K->st32, K->lastIt32, h32, false, nullptr));
+    FAME_TRY(pcg_iterate<float>(K, OpM3<float>{K->m->Et32}, F, K->st32, K->lastIt32, h32, false, nullptr));
     if (h32.flag == -1 || h32.flag == 4) return fail(FAME_ERR_NOT_CONVERGED, "FP32 correction solve broke down");
     its += h32.iter;
     K->stats.fp32Iterations += h32.iter;
     ProResidM3<double, float, true> pro{B.x, F.x, NF};
     EpiResidM3<double> epi{K->bhat, B.r, &K->st64->rho, NF, K->partials, K->counter};
-    FAME_TRY((run_chain<double, 3>(K->n, pro, epi, B.work, K->m->Es64, 1.0, NF, s)));
+    FAME_TRY((run_chain<double, 3>(K->n, pro, epi, B.work, K->m->Et64, NF, s)));
     K->stats.massApplies += 3;
     FAME_TRY(read_back(K->ctx, K->st64, &h, sizeof(PcgState)));
     rn2 = h.rho;
@@ -365,7 +365,7 @@ int recover_one(fame_krinv* K, const double2* y, double2* X, double2* MX, int* i
   // M x and x^H M x (the mass action the normalisation needs anyway)
   ProM3x pro{B.x, NF};
   EpiM3Norm epi{B.x, MX, NF, &K->st64->aux, K->partials, K->counter};
-  FAME_TRY((run_chain<double, 3>(K->n, pro, epi, B.work, K->m->Es64, 1.0, NF, s)));
+  FAME_TRY((run_chain<double, 3>(K->n, pro, epi, B.work, K->m->Et64, NF, s)));
   FAME_TRY(read_back(K->ctx, K->st64, &h, sizeof(PcgState)));
   if (!(h.aux > 0.0) || !std::isfinite(h.aux))
     return fail(FAME_ERR_NONFINITE, "recover_original_eigenvectors_exp2:BadMassNorm");

@@ -63,12 +63,12 @@ extern "C" int fame_apply_Mhat_C_scalar_compact_noalloc(fame_basis* b, fame_mass
     if (prec == FAME_F64) {
       const MhatCoef<double> c = coef_of<double>(b);
       s = run_chain_lin<double, 3>(b->n, ProMhat<double, false>{c, (const double2*)x},
-                                   EpiMhat<double, false>{c, (double2*)y}, (double2*)work, m->Es64,
-                                   1.0, b->NF, st);
+                                   EpiMhat<double, false>{c, (double2*)y}, (double2*)work, m->Et64,
+                                   b->NF, st);
     } else {
       const MhatCoef<float> c = coef_of<float>(b);
       s = run_chain_lin<float, 3>(b->n, ProMhat<float, false>{c, (const float2*)x},
-                                  EpiMhat<float, false>{c, (float2*)y}, (float2*)work, m->Es32, 1.0f,
+                                  EpiMhat<float, false>{c, (float2*)y}, (float2*)work, m->Et32,
                                   b->NF, st);
     }
   }
