@@ -92,6 +92,19 @@ int check_fault(fame_ctx* ctx) {
   return fail(FAME_ERR_CUDA, "a bounded device-side wait gave up (bulk copy never completed); results are invalid");
 }
 
+int ctx_workspace(fame_ctx* ctx, size_t bytes, void** out) {
+  if (bytes > ctx->ws_bytes) {
+    FAME_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    dfree(ctx->ws);
+    ctx->ws = nullptr;
+    ctx->ws_bytes = 0;
+    FAME_TRY(dalloc(&ctx->ws, bytes));
+    ctx->ws_bytes = bytes;
+  }
+  *out = ctx->ws;
+  return FAME_OK;
+}
+
 int read_back(fame_ctx* ctx, const void* dsrc, void* hdst, size_t bytes) {
   if (bytes > 4096) return fail(FAME_ERR_INVALID, "read_back larger than staging area");
   FAME_CUDA_TRY(cudaMemcpyAsync(ctx->pinned, dsrc, bytes, cudaMemcpyDeviceToHost, ctx->stream));
@@ -172,6 +185,7 @@ int fame_ctx_destroy(fame_ctx* c) {
   if (!c) return FAME_OK;
   cudaStreamSynchronize(c->stream);
   if (c->pinned) cudaFreeHost(c->pinned);
+  dfree(c->ws);
   if (c->ev) cudaEventDestroy(c->ev);
   if (c->capture) cudaStreamDestroy(c->capture);
   if (c->own) cudaStreamDestroy(c->own);

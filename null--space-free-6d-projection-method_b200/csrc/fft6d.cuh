@@ -452,82 +452,76 @@ __global__ void __launch_bounds__(512) k_passC(Epi epi, const C<T>* __restrict__
 // Operators whose fields are linear in one vector, field_f(i) = a_f(i) u(i),
 // and whose result is out(i) = S(i, sum_f b_f(i) v_f(i)) -- every Mhat chain
 // (exp1/apply_Mhat_C_scalar_compact.m:8-21) is of this form.  Passes A and C
-// transform the F fields of G columns concurrently: one thread per (field,
-// column, line), F*G cubes in shared memory, two barriers per pass.
+// then run the F fields one after another through a single shared-memory cube
+// per column, holding one line of u (pass A) or of the running sum (pass C) in
+// registers: a third of the shared memory and far fewer registers than the
+// general chain.  One line per thread (blockDim >= G*n^2).
 //
 // LinPro:  C<T> load(ia, in, Ext&)   u(i) (pure loads; stores deferred to commit)
-//          void commit(ia, in, const Ext&)   (field-0 threads, after all loads)
+//          void commit(ia, in, const Ext&)
 //          C<T> coef(f, ia, in)      a_f(i) (a_0 == 1 when unit0)
 // LinEpi:  C<T> coef(f, ia, in)      b_f(i) (b_0 == 1 when unit0)
 //          void store(ia, in, C<T> s, Red<Acc,K>& acc), finalize(tot)
-// Epilogues whose vectors are in natural order declare `static constexpr bool natural = true`.
-template <class E, class = void> struct EpiNatural { static constexpr bool value = false; };
-template <class E> struct EpiNatural<E, decltype(void(E::natural))> { static constexpr bool value = E::natural; };
-
-template <int n, int F, int G> struct LinThreads {
-  static constexpr int value = (F * G * n * n + 31) / 32 * 32;
-};
-
 template <int n, typename T, int F, int G, class Pro>
-__global__ void __launch_bounds__(LinThreads<n, F, G>::value) k_passA_lin(Pro pro, C<T>* __restrict__ work, long long NF, Gate gate) {
+__global__ void __launch_bounds__(512) k_passA_lin(Pro pro, C<T>* __restrict__ work, long long NF, Gate gate) {
   if (gate.off()) return;
   using Q = Cube<n, T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C<T>* s = reinterpret_cast<C<T>*>(smem_raw);
   const long long col0 = (long long)blockIdx.x * G;
-  constexpr int per_f = G * Q::n2;
+  constexpr int items = G * Q::n2;
   const int it = threadIdx.x;
-  const bool act = it < F * per_f;
-  const int f = act ? it / per_f : 0, rem = act ? it % per_f : 0;
-  const int cc = rem / Q::n2, l = rem % Q::n2;
+  const bool act = it < items;
+  const int cc = act ? it / Q::n2 : 0, l = act ? it % Q::n2 : 0;
   const long long cb = (col0 + cc) * Q::n3;
-  C<T>* cube = s + (f * G + cc) * Q::size;
-  typename Pro::Ext e[n];
-  if (act) {  // prologue and axis 1 in registers
-    C<T> u[n];
-#pragma unroll
-    for (int j = 0; j < n; ++j) u[j] = pro.load(cb + l + Q::n2 * j, cb + j + (long long)n * l, e[j]);
-    const bool unit = Pro::unit0 && f == 0;
-    T re[n], im[n];
+  C<T> u[n];
+  if (act) {  // each thread owns the modes of its line: stores may follow each load
 #pragma unroll
     for (int j = 0; j < n; ++j) {
-      C<T> v = u[j];
-      if (!unit) v = cmul<T>(pro.coef(f, cb + l + Q::n2 * j, cb + j + (long long)n * l), v);
-      re[j] = v.x;
-      im[j] = v.y;
+      typename Pro::Ext e;
+      u[j] = pro.load(cb + l + Q::n2 * j, cb + j + (long long)n * l, e);
+      pro.commit(cb + l + Q::n2 * j, cb + j + (long long)n * l, e);
     }
-    Dft<n, +1, T>::run(re, im);
-    C<T>* sc = cube + Q::line1(l);
-#pragma unroll
-    for (int j = 0; j < n; ++j) sc[j] = mk<T>(re[j], im[j]);
   }
-  __syncthreads();  // every field's loads are done: field 0 may store the prologue state
-  if (act) {
-    if (f == 0) {
+#pragma unroll 1
+  for (int f = 0; f < F; ++f) {
+    if (act) {  // axis 1 in registers
+      T re[n], im[n];
 #pragma unroll
-      for (int j = 0; j < n; ++j) pro.commit(cb + l + Q::n2 * j, cb + j + (long long)n * l, e[j]);
+      for (int j = 0; j < n; ++j) {
+        C<T> v = u[j];
+        if (!(Pro::unit0 && f == 0)) v = cmul<T>(pro.coef(f, cb + l + Q::n2 * j, cb + j + (long long)n * l), v);
+        re[j] = v.x;
+        im[j] = v.y;
+      }
+      Dft<n, +1, T>::run(re, im);
+      C<T>* sc = s + cc * Q::size + Q::line1(l);
+#pragma unroll
+      for (int j = 0; j < n; ++j) sc[j] = mk<T>(re[j], im[j]);
     }
-    line_dft<n, +1, T>(cube + Q::line2(l), Q::P1);  // axis 2
-  }
-  __syncthreads();
-  if (act) {  // axis 3 -> work (tile-major), thread <-> m = i1 + n*i2
-    const C<T>* sc = cube + Q::line3(l);
-    T re[n], im[n];
+    __syncthreads();
+    if (act) line_dft<n, +1, T>(s + cc * Q::size + Q::line2(l), Q::P1);  // axis 2
+    __syncthreads();
+    if (act) {  // axis 3 -> work (tile-major), thread <-> m = i1 + n*i2
+      const C<T>* sc = s + cc * Q::size + Q::line3(l);
+      T re[n], im[n];
 #pragma unroll
-    for (int j = 0; j < n; ++j) {
-      const C<T> v = sc[Q::P2 * j];
-      re[j] = v.x;
-      im[j] = v.y;
+      for (int j = 0; j < n; ++j) {
+        const C<T> v = sc[Q::P2 * j];
+        re[j] = v.x;
+        im[j] = v.y;
+      }
+      Dft<n, +1, T>::run(re, im);
+      C<T>* wf = work + f * NF;
+#pragma unroll
+      for (int j = 0; j < n; ++j) wf[work_at<n, T>(l + Q::n2 * j, col0 + cc)] = mk<T>(re[j], im[j]);
     }
-    Dft<n, +1, T>::run(re, im);
-    C<T>* wf = work + f * NF;
-#pragma unroll
-    for (int j = 0; j < n; ++j) wf[work_at<n, T>(l + Q::n2 * j, col0 + cc)] = mk<T>(re[j], im[j]);
+    __syncthreads();
   }
 }
 
 template <int n, typename T, int F, int G, class Epi>
-__global__ void __launch_bounds__(LinThreads<n, F, G>::value) k_passC_lin(Epi epi, const C<T>* __restrict__ work, long long NF, Gate gate) {
+__global__ void __launch_bounds__(512) k_passC_lin(Epi epi, const C<T>* __restrict__ work, long long NF, Gate gate) {
   if (gate.off()) return;
   using Q = Cube<n, T>;
   using A = typename Epi::Acc;
@@ -535,59 +529,58 @@ __global__ void __launch_bounds__(LinThreads<n, F, G>::value) k_passC_lin(Epi ep
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C<T>* s = reinterpret_cast<C<T>*>(smem_raw);
   const long long col0 = (long long)blockIdx.x * G;
-  constexpr int per_f = G * Q::n2;
+  constexpr int items = G * Q::n2;
   const int it = threadIdx.x;
-  const bool act = it < F * per_f;
-  const int f = act ? it / per_f : 0, rem = act ? it % per_f : 0;
-  const int cc = rem / Q::n2, l = rem % Q::n2;
-  C<T>* cube = s + (f * G + cc) * Q::size;
-  if (act) {  // axis 3 from work (tile-major), thread <-> m = i1 + n*i2
-    const C<T>* wf = work + f * NF;
-    T re[n], im[n];
+  const bool act = it < items;
+  const int cc = act ? it / Q::n2 : 0, l = act ? it % Q::n2 : 0;
+  const long long cb = (col0 + cc) * Q::n3;
+  C<T> sum[n];
 #pragma unroll
-    for (int j = 0; j < n; ++j) {
-      const C<T> v = wf[work_at<n, T>(l + Q::n2 * j, col0 + cc)];
-      re[j] = v.x;
-      im[j] = v.y;
+  for (int j = 0; j < n; ++j) sum[j] = mk<T>(0, 0);
+#pragma unroll 1
+  for (int f = 0; f < F; ++f) {
+    if (act) {  // axis 3 from work (tile-major), thread <-> m = i1 + n*i2
+      const C<T>* wf = work + f * NF;
+      T re[n], im[n];
+#pragma unroll
+      for (int j = 0; j < n; ++j) {
+        const C<T> v = wf[work_at<n, T>(l + Q::n2 * j, col0 + cc)];
+        re[j] = v.x;
+        im[j] = v.y;
+      }
+      Dft<n, -1, T>::run(re, im);
+      C<T>* sc = s + cc * Q::size + Q::line3(l);
+#pragma unroll
+      for (int j = 0; j < n; ++j) sc[Q::P2 * j] = mk<T>(re[j], im[j]);
     }
-    Dft<n, -1, T>::run(re, im);
-    C<T>* sc = cube + Q::line3(l);
+    __syncthreads();
+    if (act) line_dft<n, -1, T>(s + cc * Q::size + Q::line2(l), Q::P1);  // axis 2
+    __syncthreads();
+    if (act) {  // axis 1 in registers, accumulate b_f v_f
+      const C<T>* sc = s + cc * Q::size + Q::line1(l);
+      T re[n], im[n];
 #pragma unroll
-    for (int j = 0; j < n; ++j) sc[Q::P2 * j] = mk<T>(re[j], im[j]);
+      for (int j = 0; j < n; ++j) {
+        const C<T> v = sc[j];
+        re[j] = v.x;
+        im[j] = v.y;
+      }
+      Dft<n, -1, T>::run(re, im);
+#pragma unroll
+      for (int j = 0; j < n; ++j) {
+        C<T> v = mk<T>(re[j], im[j]);
+        if (!(Epi::unit0 && f == 0)) v = cmul<T>(epi.coef(f, cb + l + Q::n2 * j, cb + j + (long long)n * l), v);
+        sum[j] = cadd<T>(sum[j], v);
+      }
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  if (act) line_dft<n, -1, T>(cube + Q::line2(l), Q::P1);  // axis 2
-  __syncthreads();
-  if (act) line_dft<n, -1, T>(cube + Q::line1(l), 1);  // axis 1
-  __syncthreads();
-  // combine the fields mode by mode; modes are enumerated in the order of the
-  // epilogue's vectors (line order q = l + n^2 j, or natural order j + n l) so
-  // that consecutive threads touch consecutive addresses; all of a thread's
-  // modes are unrolled so that their loads are in flight together.
   Red<A, (K > 0 ? K : 1)> acc;
 #pragma unroll
   for (int k = 0; k < (K > 0 ? K : 1); ++k) acc.v[k] = 0;
-  constexpr int modes = G * Q::n3, nthr = LinThreads<n, F, G>::value;
-  constexpr int per_thread = (modes + nthr - 1) / nthr;
-  constexpr bool nat = EpiNatural<Epi>::value;
+  if (act) {
 #pragma unroll
-  for (int r = 0; r < per_thread; ++r) {
-    const int idx = it + r * nthr;
-    if (idx < modes) {
-      const int c2 = idx / Q::n3, q = idx % Q::n3;
-      const int j = nat ? q % n : q / Q::n2, l2 = nat ? q / n : q % Q::n2;
-      const long long cb = (col0 + c2) * Q::n3;
-      const long long ia = cb + l2 + (long long)Q::n2 * j, in = cb + j + (long long)n * l2;
-      const int pos = Q::line1(l2) + j;
-      C<T> sum = mk<T>(0, 0);
-#pragma unroll
-      for (int g = 0; g < F; ++g) {
-        C<T> v = s[(g * G + c2) * Q::size + pos];
-        if (!(Epi::unit0 && g == 0)) v = cmul<T>(epi.coef(g, ia, in), v);
-        sum = cadd<T>(sum, v);
-      }
-      epi.store(ia, in, sum, acc);
-    }
+    for (int j = 0; j < n; ++j) epi.store(cb + l + Q::n2 * j, cb + j + (long long)n * l, sum[j], acc);
   }
   if constexpr (K > 0) {
     grid_sum_finalize<A, K>(acc, epi.partials, epi.counter, [&](const Red<A, K>& tot) { epi.finalize(tot); });

@@ -10,6 +10,8 @@ struct fame_ctx {
   cudaStream_t capture = nullptr;  // graph-capture stream when `stream` is the context's own
   cudaEvent_t ev = nullptr;
   void* pinned = nullptr;  // small host staging area (4 KB)
+  void* ws = nullptr;      // grow-only device workspace (ctx_workspace)
+  size_t ws_bytes = 0;
   std::vector<void*> allocs;
 };
 
@@ -54,4 +56,17 @@ void dfree(void* p);
 int read_back(fame_ctx* ctx, const void* dsrc, void* hdst, size_t bytes);
 // FAME_ERR_CUDA (and clears the word) if a bounded device-side wait gave up on ctx's device
 int check_fault(fame_ctx* ctx);
+// At least `bytes` of device workspace owned by ctx, reused across calls (grown
+// after a stream synchronisation); valid until the next call on the context.
+int ctx_workspace(fame_ctx* ctx, size_t bytes, void** out);
+// Consecutive 256-byte aligned pieces of one workspace.
+struct Carve {
+  size_t used = 0;
+  char* base = nullptr;
+  template <typename T> T* take(size_t count) {
+    T* p = reinterpret_cast<T*>(base ? base + used : nullptr);
+    used += (count * sizeof(T) + 255) / 256 * 256;
+    return p;
+  }
+};
 }  // namespace fame

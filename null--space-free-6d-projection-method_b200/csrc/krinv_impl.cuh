@@ -66,9 +66,11 @@ template <typename T> struct OpMhat {
   const T* Es;
   static constexpr int nvec = 1;   // vector length in units of NF
   static constexpr int mass_per_matvec = 3;
+  static constexpr bool fused_update = true;  // x/r update inside the next matvec's prologue
+  static constexpr int launches_per_iter = 3;
   int matvec(fame_krinv* K, PcgBuf<T>& B, PcgState* st, cudaStream_t s) const {
-    ProPcgMhat<T> pro{c, B.p, B.r, st};
-    EpiPcgMhat<T> epi{c, B.Ap, B.p, st, reinterpret_cast<T*>(K->partials), K->counter};
+    ProPcgMhat<T> pro{c, B.x, B.r, B.p, B.Ap, st};
+    EpiPcgMhat<T> epi{c, B.Ap, B.p, B.r, st, K->partials, K->counter};
     return run_chain_lin<T, 3>(K->n, pro, epi, B.work, Es, K->NF, s, Gate{&st->active});
   }
   int resid(fame_krinv* K, PcgBuf<T>& B, const C<T>* b, double* out, cudaStream_t s) const {
@@ -82,6 +84,8 @@ template <typename T> struct OpM3 {
   const T* Es;
   static constexpr int nvec = 3;
   static constexpr int mass_per_matvec = 3;
+  static constexpr bool fused_update = false;
+  static constexpr int launches_per_iter = 4;
   int matvec(fame_krinv* K, PcgBuf<T>& B, PcgState* st, cudaStream_t s) const {
     ProPcgM3<T> pro{B.p, B.r, st, K->NF};
     EpiPcgM3<T> epi{B.Ap, B.p, st, K->NF, reinterpret_cast<T*>(K->partials), K->counter};
@@ -107,8 +111,10 @@ int enqueue_iterations(fame_krinv* K, const Op& op, PcgBuf<T>& B, PcgState* st, 
   const long long nlen = (long long)Op::nvec * K->NF;
   for (int it = 0; it < count; ++it) {
     FAME_TRY(op.matvec(K, B, st, s));
-    k_pcg_update<T><<<upd_blocks(nlen), 256, 0, s>>>(B.x, B.r, B.p, B.Ap, nlen, st, partials, K->counter);
-    ::fame::count_launch();
+    if constexpr (!Op::fused_update) {
+      k_pcg_update<T><<<upd_blocks(nlen), 256, 0, s>>>(B.x, B.r, B.p, B.Ap, nlen, st, partials, K->counter);
+      ::fame::count_launch();
+    }
   }
   FAME_CUDA_TRY(cudaGetLastError());
   return FAME_OK;
@@ -149,7 +155,7 @@ int queue_iterations(fame_krinv* K, const Op& op, PcgBuf<T>& B, PcgState* st, in
   }
   for (int done = 0; done < count; done += kGraphIters) {
     FAME_CUDA_TRY(cudaGraphLaunch(ge, s));
-    ::fame::count_launch(4LL * kGraphIters);
+    ::fame::count_launch((long long)Op::launches_per_iter * kGraphIters);
   }
   return FAME_OK;
 }
@@ -173,6 +179,13 @@ int pcg_iterate(fame_krinv* K, const Op& op, PcgBuf<T>& B, PcgState* st, int& la
       if (queued > h.maxit + 4 * every + kGraphIters) return fail(FAME_ERR_CUDA, "PCG state did not stop at maxit");
       chunk = every;
       continue;
+    }
+    if (Op::fused_update && h.pend) {  // apply the last iteration's x/r update
+      const long long nlen = (long long)Op::nvec * K->NF;
+      k_pcg_finish<T><<<vec_blocks(nlen), 256, 0, s>>>(B.x, B.r, B.p, B.Ap, nlen, st);
+      ::fame::count_launch();
+      FAME_CUDA_TRY(cudaMemsetAsync(&st->pend, 0, sizeof(int), s));
+      h.pend = 0;
     }
     if (verify && h.conv && h.flag == 0) {
       FAME_TRY(op.resid(K, B, b, &st->aux, s));

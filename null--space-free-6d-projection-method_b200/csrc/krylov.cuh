@@ -22,6 +22,8 @@ struct PcgState {
   double tolb2;     // (tol*||b||)^2
   double aux;       // last auxiliary reduction (true residual^2, output check)
   int iter, maxit, active, flag, conv, pad;
+  int pend;         // 1: x += alpha p, r -= alpha Ap still to be applied (fused-update PCG)
+  int pad2;
 };
 
 // alpha = rho / p^H A p (complex, as MATLAB pcg); breakdown -> flag 4.
@@ -48,6 +50,7 @@ __device__ __forceinline__ void pcg_init_state(PcgState* st, double rho, double 
   st->iter = 0;
   st->maxit = maxit;
   st->aux = 0.0;
+  st->pend = 0;
   if (!isfinite(rho)) {
     st->flag = -1;
     st->active = 0;
@@ -61,6 +64,7 @@ __device__ __forceinline__ void pcg_init_state(PcgState* st, double rho, double 
 
 // continue after a failed true-residual check (r already replaced by b - A x)
 static __global__ void k_pcg_resume(PcgState* st) {
+  st->pend = 0;
   st->rho = st->aux;
   st->beta = st->aux / st->rho_old;
   st->conv = 0;
@@ -120,45 +124,106 @@ template <typename T, bool LINE> struct EpiMhat {
   __device__ __forceinline__ void finalize(const Red<T, 1>&) const {}
 };
 
-// PCG search-direction update fused into the matvec prologue:
-// p = r (first iteration) or p = r + beta p (stored after all loads), u = C^{-1} p.
+// One PCG iteration on Mhat in two fused halves (no separate update kernel).
+// Prologue (pass A of iteration k): when a previous iteration left its update
+// pending, x += alpha p and r -= alpha Ap first; then p = r (first iteration)
+// or p = r + beta p, u = C^{-1} p.  x, r, p are stored after all loads.
+template <typename T> struct PcgUpd {
+  C<T> x, r, p;
+};
 template <typename T> struct ProPcgMhat {
-  using Ext = C<T>;
+  using Ext = PcgUpd<T>;
   static constexpr bool unit0 = true;
   MhatCoef<T> c;
+  C<T>* x;
+  C<T>* r;
   C<T>* p;
-  const C<T>* r;
+  const C<T>* Ap;
   const PcgState* st;
   __device__ __forceinline__ C<T> load(long long i, long long, Ext& e) const {
-    C<T> pi = ldc<T>(r + i);
-    if (st->iter > 0) pi = cadd<T>(pi, cscale<T>(p[i], (T)st->beta));
-    e = pi;
+    C<T> ri = r[i], pi = p[i];
+    if (st->pend) {
+      const C<T> a = mk<T>((T)st->alpha_re, (T)st->alpha_im);
+      e.x = cadd<T>(x[i], cmul<T>(a, pi));
+      ri = csub<T>(ri, cmul<T>(a, ldc<T>(Ap + i)));
+    }
+    e.r = ri;
+    pi = st->iter > 0 ? cadd<T>(ri, cscale<T>(pi, (T)st->beta)) : ri;
+    e.p = pi;
     return cscale<T>(pi, ldr<T>(c.invC + i));
   }
-  __device__ __forceinline__ void commit(long long i, long long, const Ext& e) const { p[i] = e; }
+  __device__ __forceinline__ void commit(long long i, long long, const Ext& e) const {
+    if (st->pend) {
+      x[i] = e.x;
+      r[i] = e.r;
+    }
+    p[i] = e.p;
+  }
   __device__ __forceinline__ C<T> coef(int f, long long i, long long) const { return MhatLinCoef<T>{c}.a(f, i); }
 };
-// Ap = Mhat p and the reduction p^H Ap -> alpha = rho / p^H Ap.
+// Epilogue (pass C): Ap = Mhat p with the reductions p^H Ap, r^H Ap, ||Ap||^2
+// and ||r||^2 (in FP64).  alpha = ||r||^2 / p^H Ap and the next residual norm
+// follow without touching r again: ||r - alpha Ap||^2 = ||r||^2 -
+// 2 Re(alpha r^H Ap) + |alpha|^2 ||Ap||^2.  Anchoring each step on ||r||^2 of
+// the stored r keeps the rounding error to one step's cancellation (a pure
+// recurrence on rho accumulates an absolute error of eps*||b||^2 and stalls
+// near sqrt(eps) relative residual).  The update itself is left pending for
+// the next prologue (or k_pcg_finish once the iteration stops).
 template <typename T> struct EpiPcgMhat {
-  using Acc = T;
-  static constexpr int K = 2;
+  using Acc = double;
+  static constexpr int K = 6;
   static constexpr bool unit0 = true;
   MhatCoef<T> c;
   C<T>* Ap;
   const C<T>* p;
+  const C<T>* r;
   PcgState* st;
-  T* partials;
+  double* partials;
   unsigned* counter;
   __device__ __forceinline__ C<T> coef(int f, long long i, long long) const { return MhatLinCoef<T>{c}.b(f, i); }
-  __device__ __forceinline__ void store(long long i, long long, C<T> s, Red<T, 2>& acc) const {
+  __device__ __forceinline__ void store(long long i, long long, C<T> s, Red<double, 6>& acc) const {
     const C<T> ap = cscale<T>(s, ldr<T>(c.invC + i));
     Ap[i] = ap;
-    const C<T> d = cmulc<T>(ldc<T>(p + i), ap);
-    acc.v[0] += d.x;
-    acc.v[1] += d.y;
+    const C<T> pi = ldc<T>(p + i), ri = ldc<T>(r + i);
+    acc.v[0] += (double)pi.x * ap.x + (double)pi.y * ap.y;  // p^H Ap
+    acc.v[1] += (double)pi.x * ap.y - (double)pi.y * ap.x;
+    acc.v[2] += (double)ri.x * ap.x + (double)ri.y * ap.y;  // r^H Ap
+    acc.v[3] += (double)ri.x * ap.y - (double)ri.y * ap.x;
+    acc.v[4] += (double)ap.x * ap.x + (double)ap.y * ap.y;  // ||Ap||^2
+    acc.v[5] += (double)ri.x * ri.x + (double)ri.y * ri.y;  // ||r||^2
   }
-  __device__ __forceinline__ void finalize(const Red<T, 2>& tot) const {
-    pcg_alpha_finalize(st, (double)tot.v[0], (double)tot.v[1]);
+  __device__ __forceinline__ void finalize(const Red<double, 6>& tot) const {
+    if (!isfinite(tot.v[5])) {
+      st->flag = 4;
+      st->active = 0;
+      st->pend = 0;
+      return;
+    }
+    st->rho = tot.v[5];
+    pcg_alpha_finalize(st, tot.v[0], tot.v[1]);
+    if (st->flag == 4) {
+      st->pend = 0;
+      return;
+    }
+    const double ar = st->alpha_re, ai = st->alpha_im;
+    double rho = st->rho - 2.0 * (ar * tot.v[2] - ai * tot.v[3]) + (ar * ar + ai * ai) * tot.v[4];
+    if (rho < 0.0) rho = 0.0;  // one-step cancellation at convergence; confirmed on the true residual
+    st->pend = 1;
+    st->rho_old = st->rho;
+    st->rho = rho;
+    st->iter += 1;
+    st->beta = rho / st->rho_old;
+    if (!isfinite(rho)) {
+      st->flag = 4;
+      st->active = 0;
+    } else if (rho <= st->tolb2) {
+      st->conv = 1;
+      st->flag = 0;
+      st->active = 0;
+    } else if (st->iter >= st->maxit) {
+      st->flag = 1;
+      st->active = 0;
+    }
   }
 };
 
@@ -341,6 +406,18 @@ __global__ void __launch_bounds__(256) k_pcg_update(C<T>* x, C<T>* r, const C<T>
       st->active = 0;
     }
   });
+}
+
+// The update left pending by the last fused iteration: x += alpha p,
+// r -= alpha Ap (queued by the host only when PcgState::pend is set).
+template <typename T>
+__global__ void __launch_bounds__(256) k_pcg_finish(C<T>* x, C<T>* r, const C<T>* __restrict__ p,
+                                                   const C<T>* __restrict__ Ap, long long n, PcgState* st) {
+  const C<T> a = mk<T>((T)st->alpha_re, (T)st->alpha_im);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    x[i] = cadd<T>(x[i], cmul<T>(a, p[i]));
+    r[i] = csub<T>(r[i], cmul<T>(a, Ap[i]));
+  }
 }
 
 // PCG start with x0 = 0: r = (T) b, x = 0, rho = ||r||^2.

@@ -89,19 +89,21 @@ int run_chain(int n, const Pro& pro, const Epi& epi, C<T>* work, const TE* Et, l
   }
 }
 
-// Columns per CTA of the linear-field passes (F*G*n^2 threads, F*G cubes).
-template <int n, typename T, int F> struct LinCols {
-  static constexpr int value = n == 2 ? 8 : n == 4 ? 8 : n == 6 ? 4 : n == 8 ? 2 : 1;
-  static_assert((n * n * n) % value == 0 && F * value * n * n <= 1024, "linear chain tiling");
+// Columns per CTA of the linear-field passes (one line per thread).
+// FP64 lines need twice the registers: half the columns per CTA keeps two CTAs per SM.
+template <int n, typename T> struct LinCols {
+  static constexpr int value = sizeof(T) == 8 && n == 10 ? 2
+                               : n == 2 ? 8 : n == 4 ? 16 : n == 6 ? 12 : n == 8 ? 8 : n == 10 ? 4 : n == 12 ? 2 : 2;
+  static_assert((n * n * n) % value == 0 && value * n * n <= 512, "linear chain tiling");
 };
 
 template <int n, typename T, int F, class Pro, class Epi, typename TE>
 int chain_lin_n(const Pro& pro, const Epi& epi, C<T>* work, const TE* Et, long long NF,
                 cudaStream_t st, Gate gate) {
   using Q = Cube<n, T>;
-  constexpr int G = LinCols<n, T, F>::value;
-  const size_t smem = (size_t)F * G * Q::size * sizeof(C<T>);
-  const int threads = LinThreads<n, F, G>::value;
+  constexpr int G = LinCols<n, T>::value;
+  const size_t smem = (size_t)G * Q::size * sizeof(C<T>);
+  const int threads = round32(G * Q::n2);
   static int attrA = ensure_smem(k_passA_lin<n, T, F, G, Pro>, smem);
   static int attrC = ensure_smem(k_passC_lin<n, T, F, G, Epi>, smem);
   if (attrA != FAME_OK) return attrA;

@@ -91,7 +91,8 @@ __global__ void __launch_bounds__(512) k_passB(C<T>* __restrict__ work, const TE
 #pragma unroll 1
   for (int u = u0, i = 0; u < u1; ++u, ++i) {
     const int s = i & 1;
-    if (!mbar_wait(&bar[s], (unsigned)((i >> 1) & 1))) {
+    const bool landed = mbar_wait(&bar[s], (unsigned)((i >> 1) & 1));
+    if (!__syncthreads_and(landed)) {  // bounded wait, agreed on by the whole CTA
       if (fault && tid == 0) atomicOr(fault, 1u);
       return;
     }

@@ -312,13 +312,23 @@ int fame_reconstruct_direct_grid(fame_basis* bs, const void* coeff, const double
   const int N = bs->N, n = 2 * N;
   const long long n2 = (long long)n * n, NF = bs->NF;
   cudaStream_t s = bs->ctx->stream;
-  double2 *Tx = nullptr, *Ty = nullptr, *Tz = nullptr, *Cp = nullptr, *T1 = nullptr, *T2 = nullptr;
-  int st = dalloc((void**)&Tx, (size_t)nx * n2 * sizeof(double2));
-  if (st == FAME_OK) st = dalloc((void**)&Ty, (size_t)ny * n2 * sizeof(double2));
-  if (st == FAME_OK) st = dalloc((void**)&Tz, (size_t)nz * n2 * sizeof(double2));
-  if (st == FAME_OK) st = dalloc((void**)&Cp, (size_t)NF * sizeof(double2));
-  if (st == FAME_OK) st = dalloc((void**)&T1, (size_t)nx * n2 * n2 * sizeof(double2));
-  if (st == FAME_OK) st = dalloc((void**)&T2, (size_t)nx * ny * n2 * sizeof(double2));
+  // workspace pieces: phase tables, permuted coefficients, two GEMM intermediates
+  auto carve = [&](Carve& cv, double2** Tx, double2** Ty, double2** Tz, double2** Cp, double2** T1, double2** T2) {
+    *Tx = cv.take<double2>((size_t)nx * n2);
+    *Ty = cv.take<double2>((size_t)ny * n2);
+    *Tz = cv.take<double2>((size_t)nz * n2);
+    *Cp = cv.take<double2>((size_t)NF);
+    *T1 = cv.take<double2>((size_t)nx * n2 * n2);
+    *T2 = cv.take<double2>((size_t)nx * ny * n2);
+  };
+  double2 *Tx, *Ty, *Tz, *Cp, *T1, *T2;
+  Carve size_only;
+  carve(size_only, &Tx, &Ty, &Tz, &Cp, &T1, &T2);
+  void* ws = nullptr;
+  int st = ctx_workspace(bs->ctx, size_only.used, &ws);
+  Carve cv;
+  cv.base = static_cast<char*>(ws);
+  carve(cv, &Tx, &Ty, &Tz, &Cp, &T1, &T2);
   const double* k = bs->info.kLift;
   if (st == FAME_OK) {
     k_phase_table<<<rblocks((long long)nx * n2), 256, 0, s>>>(xs, nx, N, P[0], k[0], P[3], k[3], Tx);
@@ -340,7 +350,6 @@ int fame_reconstruct_direct_grid(fame_basis* bs, const void* coeff, const double
     if (st == FAME_OK) st = zgemm(g3, 1, s);
     if (st == FAME_OK) st = cudaStreamSynchronize(s) == cudaSuccess ? FAME_OK : fail(FAME_ERR_CUDA, "sync");
   }
-  dfree(Tx); dfree(Ty); dfree(Tz); dfree(Cp); dfree(T1); dfree(T2);
   return st;
 }
 
@@ -369,15 +378,25 @@ int fame_taylor_on_blocks(fame_ctx* ctx, const void* coeff, const double* qModes
   if (L > 512) return fail(FAME_ERR_UNSUPPORTED, "too many Taylor terms");
   const int nChunks = (int)((NF + kTayChunk - 1) / kTayChunk);
   cudaStream_t s = ctx->stream;
-  int* dal = nullptr;
-  double2 *dcf = nullptr, *partial = nullptr, *gamma = nullptr;
-  double *centers = nullptr, *dfix = nullptr;
-  int st = dalloc((void**)&dal, al.size() * sizeof(int));
-  if (st == FAME_OK) st = dalloc((void**)&dcf, cf.size() * sizeof(double2));
-  if (st == FAME_OK) st = dalloc((void**)&partial, (size_t)nChunks * nBlocks * L * sizeof(double2));
-  if (st == FAME_OK) st = dalloc((void**)&gamma, (size_t)nBlocks * L * sizeof(double2));
-  if (st == FAME_OK) st = dalloc((void**)&centers, (size_t)nBlocks * 3 * sizeof(double));
-  if (st == FAME_OK && fixedCenter) st = dalloc((void**)&dfix, 3 * sizeof(double));
+  int* dal;
+  double2 *dcf, *partial, *gamma;
+  double *centers, *dfix;
+  auto carve = [&](Carve& cv) {
+    dal = cv.take<int>(al.size());
+    dcf = cv.take<double2>(cf.size());
+    partial = cv.take<double2>((size_t)nChunks * nBlocks * L);
+    gamma = cv.take<double2>((size_t)nBlocks * L);
+    centers = cv.take<double>((size_t)nBlocks * 3);
+    dfix = cv.take<double>(3);
+  };
+  Carve size_only;
+  carve(size_only);
+  void* ws = nullptr;
+  int st = ctx_workspace(ctx, size_only.used, &ws);
+  Carve cv;
+  cv.base = static_cast<char*>(ws);
+  carve(cv);
+  if (!fixedCenter) dfix = nullptr;
   if (st == FAME_OK) {
     cudaMemcpyAsync(dal, al.data(), al.size() * sizeof(int), cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(dcf, cf.data(), cf.size() * sizeof(double2), cudaMemcpyHostToDevice, s);
@@ -406,7 +425,6 @@ int fame_taylor_on_blocks(fame_ctx* ctx, const void* coeff, const double* qModes
     if (st == FAME_OK && cudaGetLastError() != cudaSuccess) st = fail(FAME_ERR_CUDA, "taylor launch");
     if (st == FAME_OK && cudaStreamSynchronize(s) != cudaSuccess) st = fail(FAME_ERR_CUDA, "taylor sync");
   }
-  dfree(dal); dfree(dcf); dfree(partial); dfree(gamma); dfree(centers); dfree(dfix);
   return st;
 }
 
