@@ -240,6 +240,12 @@ template <typename T, int F> struct FieldsInRegs {
   static constexpr bool value = sizeof(T) == 4 || F == 1;
 };
 
+// Functors whose vectors are mostly in natural order declare
+// `static constexpr bool natural = true`; the staged prologue/epilogue loops
+// then enumerate modes in natural order.
+template <class E, class = void> struct Natural { static constexpr bool value = false; };
+template <class E> struct Natural<E, decltype(void(E::natural))> { static constexpr bool value = E::natural; };
+
 // Natural <-> line order of a global mode index (see the header comment).
 template <int n> __device__ __forceinline__ long long nat_to_line(long long i) {
   constexpr int n2 = n * n, n3 = n * n * n;
@@ -309,13 +315,14 @@ __global__ void __launch_bounds__(512) k_passA(Pro pro, C<T>* __restrict__ work,
       }
     }
   } else {
-    // FP64 multi-field: prologue staged through shared memory in line order, then axis 1 there
+    // FP64 multi-field: prologue staged through shared memory, then axis 1 there;
+    // modes enumerated in the functor's order (consecutive threads, consecutive addresses)
     for (int idx = threadIdx.x; idx < G * Q::n3; idx += blockDim.x) {
       const int cc = idx / Q::n3, q = idx % Q::n3;
-      const int i1 = q / Q::n2, l = q % Q::n2;
+      const int i1 = Natural<Pro>::value ? q % n : q / Q::n2, l = Natural<Pro>::value ? q / n : q % Q::n2;
       const long long cb = (col0 + cc) * Q::n3;
       C<T> v[F];
-      pro.load(cb + q, cb + i1 + (long long)n * l, v);
+      pro.load(cb + l + (long long)Q::n2 * i1, cb + i1 + (long long)n * l, v);
 #pragma unroll
       for (int f = 0; f < F; ++f) s[(cc * F + f) * Q::size + i1 + Q::line1(l)] = v[f];
     }
@@ -433,14 +440,14 @@ __global__ void __launch_bounds__(512) k_passC(Epi epi, const C<T>* __restrict__
       for (int f = 0; f < F; ++f) line_dft<n, -1, T>(sc + f * Q::size, 1);
     }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < G * Q::n3; idx += blockDim.x) {  // epilogue, line order
+    for (int idx = threadIdx.x; idx < G * Q::n3; idx += blockDim.x) {  // epilogue, functor's order
       const int cc = idx / Q::n3, q = idx % Q::n3;
-      const int i1 = q / Q::n2, l = q % Q::n2;
+      const int i1 = Natural<Epi>::value ? q % n : q / Q::n2, l = Natural<Epi>::value ? q / n : q % Q::n2;
       const long long cb = (col0 + cc) * Q::n3;
       C<T> v[F];
 #pragma unroll
       for (int f = 0; f < F; ++f) v[f] = s[(cc * F + f) * Q::size + i1 + Q::line1(l)];
-      epi.store(cb + q, cb + i1 + (long long)n * l, v, acc);
+      epi.store(cb + l + (long long)Q::n2 * i1, cb + i1 + (long long)n * l, v, acc);
     }
   }
   if constexpr (K > 0) {

@@ -17,6 +17,7 @@ namespace fame {
 
 // pre chain: fields r1, r2 of r = V1^{-*} q (q, V, det in natural order)
 struct ProKrPre {
+  static constexpr bool natural = true;
   const double2* q;
   const double2 *V11, *V12, *V21, *V22, *det;
   long long NF;
@@ -68,6 +69,7 @@ struct ProKrPost {
 struct EpiKrPost {
   using Acc = double;
   static constexpr int K = 1;
+  static constexpr bool natural = true;
   const double2 *mr1, *mr2, *V11, *V12, *V21, *V22, *det;
   double2* y;
   long long NF;

@@ -135,6 +135,7 @@ int run_chain_lin(int n, const Pro& pro, const Epi& epi, C<T>* work, const TE* E
 // ------------------------------------------------------------ functors
 // Identity prologue/epilogue (plain mass action, natural order): F columns.
 template <typename T, int F> struct ProCols {
+  static constexpr bool natural = true;
   const C<T>* x[F];
   __device__ __forceinline__ void load(long long, long long i, C<T>* v) const {
 #pragma unroll
@@ -144,6 +145,7 @@ template <typename T, int F> struct ProCols {
 template <typename T, int F> struct EpiCols {
   using Acc = T;
   static constexpr int K = 0;
+  static constexpr bool natural = true;
   C<T>* y[F];
   T* partials = nullptr;
   unsigned* counter = nullptr;
