@@ -176,6 +176,10 @@ typedef struct {
   int checkEvery;    /* PCG iterations queued between host convergence checks (8) */
   int verifyTrueResidual; /* confirm convergence on the true residual, as MATLAB pcg (1) */
   int useGraphs;     /* replay PCG iterations as captured CUDA graphs (1) */
+  int mhatPreconditioner; /* explicit: precondition the Mhat PCG with the same operator on the
+                             material 1/eps, C^{-1} B^H (I3 (x) M^{-1}) B C^{-1}; the stopping
+                             test stays ||b - Mhat u|| <= tolCG ||b|| (1).  0: plain CG as the
+                             reference's pcg(Mhat, ...) in exp1/make_explicit_krinv_compact.m:43 */
 } fame_krinv_opts;
 FAME_API int fame_krinv_default_opts(fame_krinv_opts* o);
 FAME_API int fame_krinv_create(fame_basis* b, fame_mass* m, const fame_krinv_opts* o, fame_krinv** out);

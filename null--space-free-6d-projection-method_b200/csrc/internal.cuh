@@ -22,6 +22,8 @@ struct fame_mass {
   double* Et64 = nullptr;  // E / NF, FP64, pass-B tile order of the FP64 chains (k_tile_E)
   float* Et32 = nullptr;   // E / NF, FP32, pass-B tile order of the FP32 chains
   void* work = nullptr;    // one NF-field of complex128 scratch for the mass modes
+  double* EtInv64 = nullptr;  // NF^-1 / E in the same tile order: the inverse mass operator
+  float* EtInv32 = nullptr;
 };
 
 struct fame_basis {

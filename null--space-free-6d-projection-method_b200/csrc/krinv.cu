@@ -123,7 +123,13 @@ int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
   double relres = 0.0;
   int iters = 0;
   if (K->o.prec_mode == FAME_PREC_FP64) {
-    FAME_TRY(pcg_iterate<double>(K, OpMhat<double>{coef_line_of<double>(bs), es_of<double>(K->m)}, B, st, K->lastIt64, h, K->o.verifyTrueResidual != 0, K->bhat));
+    if (K->o.mhatPreconditioner) {
+      FAME_TRY(pcg_iterate<double>(K, OpMhatPre<double>{coef_line_of<double>(bs), es_of<double>(K->m), K->m->EtInv64},
+                                   B, st, K->lastIt64, h, K->o.verifyTrueResidual != 0, K->bhat));
+    } else {
+      FAME_TRY(pcg_iterate<double>(K, OpMhat<double>{coef_line_of<double>(bs), es_of<double>(K->m)}, B, st,
+                                   K->lastIt64, h, K->o.verifyTrueResidual != 0, K->bhat));
+    }
     if (h.flag == -1) return fail(FAME_ERR_NONFINITE, "Mhat right-hand side contains NaN/Inf");
     iters = h.iter;
     relres = h.bnorm2 > 0 ? std::sqrt(h.rho / h.bnorm2) : 0.0;
@@ -153,7 +159,13 @@ int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
                                                               partials32, K->counter);
       ::fame::count_launch();
       PcgState h32{};
-      FAME_TRY(pcg_iterate<float>(K, OpMhat<float>{coef_line_of<float>(bs), es_of<float>(K->m)}, F, st32, K->lastIt32, h32, false, nullptr));
+      if (K->o.mhatPreconditioner) {
+        FAME_TRY(pcg_iterate<float>(K, OpMhatPre<float>{coef_line_of<float>(bs), es_of<float>(K->m), K->m->EtInv32},
+                                    F, st32, K->lastIt32, h32, false, nullptr));
+      } else {
+        FAME_TRY(pcg_iterate<float>(K, OpMhat<float>{coef_line_of<float>(bs), es_of<float>(K->m)}, F, st32,
+                                    K->lastIt32, h32, false, nullptr));
+      }
       if (h32.flag == -1 || h32.flag == 4)
         return fail(FAME_ERR_NOT_CONVERGED, "FP32 correction solve broke down");
       K->stats.fp32Iterations += h32.iter;
@@ -196,10 +208,11 @@ template <typename T> int alloc_pcgbuf(PcgBuf<T>& B, long long NF, int nvec) {
   FAME_TRY(dalloc((void**)&B.r, nvec * NF * sizeof(C<T>)));
   FAME_TRY(dalloc((void**)&B.p, nvec * NF * sizeof(C<T>)));
   FAME_TRY(dalloc((void**)&B.Ap, nvec * NF * sizeof(C<T>)));
+  if (nvec == 1) FAME_TRY(dalloc((void**)&B.z, NF * sizeof(C<T>)));
   return FAME_OK;
 }
 template <typename T> void free_pcgbuf(PcgBuf<T>& B) {
-  dfree(B.work); dfree(B.x); dfree(B.r); dfree(B.p); dfree(B.Ap);
+  dfree(B.work); dfree(B.x); dfree(B.r); dfree(B.p); dfree(B.Ap); dfree(B.z);
   B = PcgBuf<T>{};
 }
 
@@ -251,6 +264,7 @@ int fame_krinv_default_opts(fame_krinv_opts* o) {
   o->checkEvery = 4;
   o->verifyTrueResidual = 1;
   o->useGraphs = 1;
+  o->mhatPreconditioner = 1;
   return FAME_OK;
 }
 
@@ -281,7 +295,7 @@ int fame_krinv_create(fame_basis* b, fame_mass* m, const fame_krinv_opts* o, fam
   if (s == FAME_OK && !nested) s = dalloc((void**)&K->mr1, NF * sizeof(double2));
   if (s == FAME_OK && !nested) s = dalloc((void**)&K->mr2, NF * sizeof(double2));
   if (s == FAME_OK) s = dalloc((void**)&K->bhat, (nested ? 3 : 1) * NF * sizeof(double2));
-  const long long nparts = std::max<long long>(passC_blocks(K->n), kVecBlocksMax) * 4;
+  const long long nparts = std::max<long long>(passC_blocks(K->n), kVecBlocksMax) * 8;
   if (s == FAME_OK) s = dalloc((void**)&K->partials, nparts * sizeof(double));
   if (s == FAME_OK) s = dalloc((void**)&K->counter, sizeof(unsigned));
   if (s == FAME_OK) s = dalloc((void**)&K->st64, sizeof(PcgState));

@@ -7,6 +7,7 @@ namespace fame {
 
 template <typename T> struct PcgBuf {
   C<T>* work = nullptr;  // 3 fields of NF (mass chain)
+  C<T>* z = nullptr;     // preconditioned residual (Mhat PCG with the inverse-material preconditioner)
   C<T>* x = nullptr;
   C<T>* r = nullptr;
   C<T>* p = nullptr;
@@ -42,7 +43,7 @@ struct fame_krinv {
   fame::OuterState* ost = nullptr;
   void* lanczos_ws = nullptr;  // Lanczos basis workspace reused across solves
   // CUDA graphs of kGraphIters PCG iterations, one per (precision, operator)
-  cudaGraphExec_t graphs[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaGraphExec_t graphs[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
 namespace fame {
@@ -68,6 +69,7 @@ template <typename T> struct OpMhat {
   static constexpr int mass_per_matvec = 3;
   static constexpr bool fused_update = true;  // x/r update inside the next matvec's prologue
   static constexpr int launches_per_iter = 3;
+  static constexpr int kind = 0;
   int matvec(fame_krinv* K, PcgBuf<T>& B, PcgState* st, cudaStream_t s) const {
     ProPcgMhat<T> pro{c, B.x, B.r, B.p, B.Ap, st};
     EpiPcgMhat<T> epi{c, B.Ap, B.p, B.r, st, K->partials, K->counter};
@@ -86,6 +88,7 @@ template <typename T> struct OpM3 {
   static constexpr int mass_per_matvec = 3;
   static constexpr bool fused_update = false;
   static constexpr int launches_per_iter = 4;
+  static constexpr int kind = 1;
   int matvec(fame_krinv* K, PcgBuf<T>& B, PcgState* st, cudaStream_t s) const {
     ProPcgM3<T> pro{B.p, B.r, st, K->NF};
     EpiPcgM3<T> epi{B.Ap, B.p, st, K->NF, reinterpret_cast<T*>(K->partials), K->counter};
@@ -98,11 +101,35 @@ template <typename T> struct OpM3 {
   }
 };
 
+// Mhat with the inverse-material preconditioner (krylov.cuh, ProPcgPre): two
+// chains per iteration, the second material 1/E.
+template <typename T> struct OpMhatPre {
+  MhatCoef<T> c;
+  const T* Es;
+  const T* EsInv;
+  static constexpr int nvec = 1;
+  static constexpr int mass_per_matvec = 6;
+  static constexpr bool fused_update = true;
+  static constexpr int launches_per_iter = 6;
+  static constexpr int kind = 2;
+  int matvec(fame_krinv* K, PcgBuf<T>& B, PcgState* st, cudaStream_t s) const {
+    ProPcgPre<T> pp{c, B.x, B.r, B.p, B.Ap, st};
+    EpiPcgPre<T> ep{c, B.z, B.r, st, K->partials, K->counter};
+    FAME_TRY((run_chain_lin<T, 3>(K->n, pp, ep, B.work, EsInv, K->NF, s, Gate{&st->active})));
+    ProPcgDir<T> pd{c, B.p, B.z, st};
+    EpiPcgMhat<T, true> ea{c, B.Ap, B.p, B.r, st, K->partials, K->counter};
+    return run_chain_lin<T, 3>(K->n, pd, ea, B.work, Es, K->NF, s, Gate{&st->active});
+  }
+  int resid(fame_krinv* K, PcgBuf<T>& B, const C<T>* b, double* out, cudaStream_t s) const {
+    return OpMhat<T>{c, Es}.resid(K, B, b, out, s);
+  }
+};
+
 // PCG iterations per captured graph.
 constexpr int kGraphIters = 4;
 
 template <typename T, class Op> constexpr int graph_slot() {
-  return (sizeof(T) == 8 ? 0 : 1) + (Op::nvec == 3 ? 2 : 0);
+  return (sizeof(T) == 8 ? 0 : 1) + 2 * Op::kind;
 }
 
 template <typename T, class Op>

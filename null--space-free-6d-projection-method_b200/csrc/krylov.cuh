@@ -24,6 +24,7 @@ struct PcgState {
   int iter, maxit, active, flag, conv, pad;
   int pend;         // 1: x += alpha p, r -= alpha Ap still to be applied (fused-update PCG)
   int pad2;
+  double rz, rz_old;  // preconditioned PCG: r^H z of the current and previous iteration
 };
 
 // alpha = rho / p^H A p (complex, as MATLAB pcg); breakdown -> flag 4.
@@ -169,7 +170,7 @@ template <typename T> struct ProPcgMhat {
 // recurrence on rho accumulates an absolute error of eps*||b||^2 and stalls
 // near sqrt(eps) relative residual).  The update itself is left pending for
 // the next prologue (or k_pcg_finish once the iteration stops).
-template <typename T> struct EpiPcgMhat {
+template <typename T, bool PRE = false> struct EpiPcgMhat {
   using Acc = double;
   static constexpr int K = 6;
   static constexpr bool unit0 = true;
@@ -199,20 +200,22 @@ template <typename T> struct EpiPcgMhat {
       st->pend = 0;
       return;
     }
-    st->rho = tot.v[5];
+    const double rr = tot.v[5];
+    // alpha = rho / p^H Ap with rho = r^H r (plain) or r^H z (preconditioned)
+    st->rho = PRE ? st->rz : rr;
     pcg_alpha_finalize(st, tot.v[0], tot.v[1]);
     if (st->flag == 4) {
       st->pend = 0;
       return;
     }
     const double ar = st->alpha_re, ai = st->alpha_im;
-    double rho = st->rho - 2.0 * (ar * tot.v[2] - ai * tot.v[3]) + (ar * ar + ai * ai) * tot.v[4];
+    double rho = rr - 2.0 * (ar * tot.v[2] - ai * tot.v[3]) + (ar * ar + ai * ai) * tot.v[4];
     if (rho < 0.0) rho = 0.0;  // one-step cancellation at convergence; confirmed on the true residual
     st->pend = 1;
-    st->rho_old = st->rho;
-    st->rho = rho;
+    st->rho_old = rr;
+    st->rho = rho;  // predicted ||r||^2 after the pending update
     st->iter += 1;
-    st->beta = rho / st->rho_old;
+    if (!PRE) st->beta = rho / rr;
     if (!isfinite(rho)) {
       st->flag = 4;
       st->active = 0;
@@ -225,6 +228,90 @@ template <typename T> struct EpiPcgMhat {
       st->active = 0;
     }
   }
+};
+
+// Preconditioned PCG on Mhat, P = C^{-1}(M^{-1} + W1^* M^{-1} W1 + W2^* M^{-1} W2) C^{-1}:
+// Mhat = B^H (I3 (x) M) B with the isometry B = [I; W1; W2] C^{-1}, and since
+// M = F diag(E) F^{-1} on the grid, M^{-1} is the same chain with 1/E, so P is
+// the compression of M^{-1}.  One iteration is two chains:
+//   P-chain  prologue applies the pending x += alpha p, r -= alpha Ap, input r;
+//            epilogue z = P r and rz = r^H z (beta = rz / rz_old);
+//   A-chain  prologue p = z + beta p, input p; epilogue Ap, alpha = rz / p^H Ap
+//            and the predicted ||r||^2 for the convergence test (EpiPcgMhat<T, true>).
+// The stopping test is on ||r|| / ||b|| as in MATLAB pcg.
+template <typename T> struct ProPcgPre {
+  using Ext = PcgUpd<T>;
+  static constexpr bool unit0 = true;
+  MhatCoef<T> c;
+  C<T>* x;
+  C<T>* r;
+  const C<T>* p;
+  const C<T>* Ap;
+  const PcgState* st;
+  __device__ __forceinline__ C<T> load(long long i, long long, Ext& e) const {
+    C<T> ri = r[i];
+    if (st->pend) {
+      const C<T> a = mk<T>((T)st->alpha_re, (T)st->alpha_im);
+      e.x = cadd<T>(x[i], cmul<T>(a, ldc<T>(p + i)));
+      ri = csub<T>(ri, cmul<T>(a, ldc<T>(Ap + i)));
+    }
+    e.r = ri;
+    return cscale<T>(ri, ldr<T>(c.invC + i));
+  }
+  __device__ __forceinline__ void commit(long long i, long long, const Ext& e) const {
+    if (st->pend) {
+      x[i] = e.x;
+      r[i] = e.r;
+    }
+  }
+  __device__ __forceinline__ C<T> coef(int f, long long i, long long) const { return MhatLinCoef<T>{c}.a(f, i); }
+};
+template <typename T> struct EpiPcgPre {
+  using Acc = double;
+  static constexpr int K = 2;
+  static constexpr bool unit0 = true;
+  MhatCoef<T> c;
+  C<T>* z;
+  const C<T>* r;
+  PcgState* st;
+  double* partials;
+  unsigned* counter;
+  __device__ __forceinline__ C<T> coef(int f, long long i, long long) const { return MhatLinCoef<T>{c}.b(f, i); }
+  __device__ __forceinline__ void store(long long i, long long, C<T> s, Red<double, 2>& acc) const {
+    const C<T> zi = cscale<T>(s, ldr<T>(c.invC + i));
+    z[i] = zi;
+    const C<T> ri = ldc<T>(r + i);
+    acc.v[0] += (double)ri.x * zi.x + (double)ri.y * zi.y;  // r^H z (real for Hermitian P)
+    acc.v[1] += (double)ri.x * zi.y - (double)ri.y * zi.x;
+  }
+  __device__ __forceinline__ void finalize(const Red<double, 2>& tot) const {
+    st->pend = 0;  // the prologue of this chain has applied it
+    const double rz = tot.v[0];
+    if (!(rz > 0.0) || !isfinite(rz) || !isfinite(tot.v[1])) {
+      st->flag = 4;
+      st->active = 0;
+      return;
+    }
+    st->rz_old = st->rz;
+    st->rz = rz;
+    st->beta = st->iter > 0 ? rz / st->rz_old : 0.0;
+  }
+};
+template <typename T> struct ProPcgDir {
+  using Ext = C<T>;
+  static constexpr bool unit0 = true;
+  MhatCoef<T> c;
+  C<T>* p;
+  const C<T>* z;
+  const PcgState* st;
+  __device__ __forceinline__ C<T> load(long long i, long long, Ext& e) const {
+    C<T> pi = ldc<T>(z + i);
+    if (st->iter > 0) pi = cadd<T>(pi, cscale<T>(p[i], (T)st->beta));
+    e = pi;
+    return cscale<T>(pi, ldr<T>(c.invC + i));
+  }
+  __device__ __forceinline__ void commit(long long i, long long, const Ext& e) const { p[i] = e; }
+  __device__ __forceinline__ C<T> coef(int f, long long i, long long) const { return MhatLinCoef<T>{c}.a(f, i); }
 };
 
 // r = b - Mhat x with ||r||^2 into *out (true residual / refinement residual).

@@ -21,9 +21,10 @@ template <typename T> int work_tt(int n) {
 }
 
 // E*scale in the pass-B tile order of the chains in precision T.
-template <typename T> int tile_E(const double* E, int n, long long NF, double scale, T* out, cudaStream_t st) {
+template <typename T> int tile_E(const double* E, int n, long long NF, double scale, T* out, cudaStream_t st,
+                                  int invert = 0) {
   const int blocks = (int)std::min<long long>((NF + 255) / 256, 148 * 16);
-  k_tile_E<T><<<blocks, 256, 0, st>>>(E, n, work_tt<T>(n), NF, scale, out);
+  k_tile_E<T><<<blocks, 256, 0, st>>>(E, n, work_tt<T>(n), NF, scale, invert, out);
   ::fame::count_launch();
   FAME_CUDA_TRY(cudaGetLastError());
   return FAME_OK;
@@ -189,13 +190,19 @@ int fame_mass_create(fame_ctx* ctx, int N, const double* E, fame_mass** out) {
   int s = dalloc((void**)&m->Et64, m->NF * sizeof(double));
   if (s == FAME_OK) s = dalloc((void**)&m->Et32, m->NF * sizeof(float));
   if (s == FAME_OK) s = dalloc(&m->work, m->NF * sizeof(double2));
+  if (s == FAME_OK) s = dalloc((void**)&m->EtInv64, m->NF * sizeof(double));
+  if (s == FAME_OK) s = dalloc((void**)&m->EtInv32, m->NF * sizeof(float));
   const double scale = 1.0 / (double)m->NF;
   if (s == FAME_OK) s = tile_E<double>(E, m->n, m->NF, scale, m->Et64, ctx->stream);
   if (s == FAME_OK) s = tile_E<float>(E, m->n, m->NF, scale, m->Et32, ctx->stream);
+  if (s == FAME_OK) s = tile_E<double>(E, m->n, m->NF, scale, m->EtInv64, ctx->stream, 1);
+  if (s == FAME_OK) s = tile_E<float>(E, m->n, m->NF, scale, m->EtInv32, ctx->stream, 1);
   if (s != FAME_OK) {
     dfree(m->Et64);
     dfree(m->Et32);
     dfree(m->work);
+    dfree(m->EtInv64);
+    dfree(m->EtInv32);
     delete m;
     return s;
   }
@@ -209,6 +216,8 @@ int fame_mass_destroy(fame_mass* m) {
   dfree(m->Et64);
   dfree(m->Et32);
   dfree(m->work);
+  dfree(m->EtInv64);
+  dfree(m->EtInv32);
   delete m;
   return FAME_OK;
 }

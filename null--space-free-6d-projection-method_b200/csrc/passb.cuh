@@ -175,15 +175,18 @@ __global__ void __launch_bounds__(512) k_passB_inv(C<T>* __restrict__ work, long
 // Material in the order pass B reads it: tile kt holds, for j = i5 and the
 // phase-3 line index kk = t + TT*(i4 + n*i6), the value E(c123, c456)*scale at
 // kt*TT*n^3 + j*TT*n^2 + kk, with c123 = kt*TT + t, c456 = i4 + n*j + n^2*i6.
+// With invert, the tile holds scale / E (the material of the inverse mass operator).
 template <typename TE>
-__global__ void k_tile_E(const double* __restrict__ E, int n, int TT, long long NF, double scale, TE* __restrict__ out) {
+__global__ void k_tile_E(const double* __restrict__ E, int n, int TT, long long NF, double scale, int invert,
+                         TE* __restrict__ out) {
   const long long n3 = (long long)n * n * n, L = (long long)TT * n * n, tile = TT * n3;
   for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < NF; o += (long long)gridDim.x * blockDim.x) {
     const long long kt = o / tile, rem = o % tile;
     const long long j = rem / L, kk = rem % L;
     const long long t = kk % TT, rr = kk / TT, i4 = rr % n, i6 = rr / n;
     const long long c123 = kt * TT + t, c456 = i4 + n * j + (long long)n * n * i6;
-    out[o] = (TE)(E[c123 + n3 * c456] * scale);
+    const double e = E[c123 + n3 * c456];
+    out[o] = (TE)(invert ? scale / e : e * scale);
   }
 }
 

@@ -39,7 +39,7 @@ def test_status_strings_and_default_opts():
     o = _lib.fame_krinv_opts()
     assert L.fame_krinv_default_opts(C.byref(o)) == 0
     assert o.tolCG == 1e-10 and o.maxitCG == 1200 and o.tolM == 1e-12 and o.maxitKr == 600
-    assert o.epsC == 4.0 and o.useKrPreconditioner == 1
+    assert o.epsC == 4.0 and o.useKrPreconditioner == 1 and o.mhatPreconditioner == 1
     assert L.fame_version() >= 100
 
 
@@ -56,7 +56,7 @@ def test_null_arguments_are_rejected_without_gpu():
 def test_struct_layouts_match_header():
     from fame_b200 import _lib
     # field counts mirror include/fame.h
-    assert len(_lib.fame_krinv_opts._fields_) == 15
+    assert len(_lib.fame_krinv_opts._fields_) == 16
     assert len(_lib.fame_krinv_stats._fields_) == 10
     assert C.sizeof(_lib.fame_basis_info) == 8 + 4 + 4 + 8 + 8 + 48 + 8
 

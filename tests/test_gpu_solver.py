@@ -24,19 +24,28 @@ def _systems(N, Pname, q, material, cuda_device):
     return S, F.build_q_system(m, Pm, q)
 
 
+@pytest.mark.parametrize("precond", [1, 0])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_explicit_krinv_matches_oracle(cuda_device, precision):
+def test_explicit_krinv_matches_oracle(cuda_device, precision, precond):
+    """Both the plain Mhat CG of the reference and the inverse-material
+    preconditioned CG reach the oracle's K_r^{-1} q (tolCG 1e-12)."""
     import fame_b200 as F
     S, sg = _systems(2, "reference", (0.13, 0.21, 0.17), "exp", cuda_device)
     rng = np.random.default_rng(5)
     b = rng.standard_normal(S.nr) + 1j * rng.standard_normal(S.nr)
-    op_ref, _ = O.make_explicit_krinv_compact(S, 1e-12, 3000)
+    op_ref, st_ref = O.make_explicit_krinv_compact(S, 1e-12, 3000)
     y_ref = op_ref(b)
-    op, stats = F.make_explicit_krinv_compact(sg, 1e-12, 3000, precision=precision)
+    op, stats = F.make_explicit_krinv_compact(sg, 1e-12, 3000, precision=precision, mhatPreconditioner=precond)
     y = op(torch.as_tensor(b, device=cuda_device)).cpu().numpy()
     assert _rel(y, y_ref) < 1e-10
     st = stats()
     assert st.inverseCalls == 1 and st.totalIterations > 0
+    if precond and precision == "fp64":  # the preconditioner cuts the Mhat CG iterations by >2x
+        assert 2 * st.totalIterations < st_ref()["totalMhatIterations"]
+    for _ in range(3):  # repeated solves on the same workspace (pending-update state, graphs)
+        b2 = rng.standard_normal(S.nr) + 1j * rng.standard_normal(S.nr)
+        y2 = op(torch.as_tensor(b2, device=cuda_device)).cpu().numpy()
+        assert _rel(y2, op_ref(b2)) < 1e-10
     if precision == "mixed":
         assert st.refineSteps >= 1 and st.fp32Iterations > 0
 
