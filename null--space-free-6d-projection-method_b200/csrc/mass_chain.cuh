@@ -90,10 +90,10 @@ int run_chain(int n, const Pro& pro, const Epi& epi, C<T>* work, const TE* Et, l
 }
 
 // Columns per CTA of the linear-field passes (one line per thread).
-// FP64 lines need twice the registers: half the columns per CTA keeps two CTAs per SM.
+// n = 10: two columns (200 lines) per CTA, several CTAs per SM (FP64 lines need twice the registers).
 template <int n, typename T> struct LinCols {
-  static constexpr int value = sizeof(T) == 8 && n == 10 ? 2
-                               : n == 2 ? 8 : n == 4 ? 16 : n == 6 ? 12 : n == 8 ? 8 : n == 10 ? 4 : n == 12 ? 2 : 2;
+  static constexpr int value = n == 10 ? 2
+                               : n == 2 ? 8 : n == 4 ? 16 : n == 6 ? 12 : n == 8 ? 8 : n == 12 ? 2 : 2;
   static_assert((n * n * n) % value == 0 && value * n * n <= 512, "linear chain tiling");
 };
 
