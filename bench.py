@@ -287,6 +287,15 @@ def run_fame(args):
                "taylor_rel_err_vs_direct": err, "timing": "median of 5 repetitions, 3 components each",
                "direct_form": "factorised tensor-grid sum (axis-block cut matrix), FP64",
                "taylor_form": "multi-center Taylor p=10, 4^3 centers, FP64"}
+        # LWRQ validation of the reconstructed field (material sampled on the Yee edges)
+        lam10 = float(np.sort(1.0 / res_fp64[1])[9])
+        F.compute_yee_lwrq_metrics(fields["direct"], lam10, cfg.P_GOLDEN, n_yee, h_yee, ("cos", 12.0))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        lw, _ = F.compute_yee_lwrq_metrics(fields["direct"], lam10, cfg.P_GOLDEN, n_yee, h_yee, ("cos", 12.0))
+        t_lw = time.perf_counter() - t0
+        yee["lwrq"] = {k: lw[k] for k in ("lambda3D", "eta3D", "deltaLambda", "nuLWRQ", "deltaPart")}
+        yee["lwrq"]["seconds"] = round(t_lw, 5)
     except Exception as exc:  # reported, not hidden
         yee = {"error": repr(exc)}
 

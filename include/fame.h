@@ -159,6 +159,19 @@ FAME_API int fame_apply_Mhat_C_scalar_compact(fame_basis* b, fame_mass* m, const
 FAME_API int fame_apply_Mhat_C_scalar_compact_noalloc(fame_basis* b, fame_mass* m, const void* x,
                                                       void* y, int prec);
 
+/* ---- Yee-field physical validation (LWRQ) ---- */
+/* exp3/compute_yee_lwrq_metrics_exp4.m + compute_lwrq_exp4.m + apply_cropped_A_exp3.m +
+   separable_conv3_same_exp4.m + sample_scalar_yee_material_exp4.m.  u1..u3: device complex128
+   fields on the plus-grid, (2n+3)^3 each, x fastest.  P: cut matrix, column-major 6 x 3.
+   material_kind 0: eps = mp0 exp(mp1/6 sum_l cos(P_l.x)) (epsC, alpha); 1: eps = 1 + mp0 prod_l
+   (1 + cos(P_l.x))/2 (delta).  metrics (host, 10): lambdaCrop, lambda3D, eta3D, etaUsing6DLambda,
+   deltaLambda, VLWRQ, nuLWRQ, deltaPart, deltaLWRQIdentity, croppedMass.  slice_z0 / slice_x0
+   (host, (2n+1)^2 each, or NULL): |rho - lambda3D| / |lambda3D| on z = 0 (x fastest) and on
+   x = 0 (y fastest). */
+FAME_API int fame_yee_lwrq_metrics(fame_ctx* ctx, const void* u1, const void* u2, const void* u3, int n,
+                                   double h, const double* P, int material_kind, double mp0, double mp1,
+                                   double lambda6D, double* metrics, double* slice_z0, double* slice_x0);
+
 /* ---- K_r^{-1} actions ---- */
 typedef struct {
   int kind;        /* FAME_KRINV_EXPLICIT | FAME_KRINV_NESTED */

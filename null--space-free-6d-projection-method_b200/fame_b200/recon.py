@@ -11,7 +11,7 @@ from . import _lib as L
 from ._lib import FameError, call
 from .core import QSystem, _ptr, default_context
 
-__all__ = ["recover_original_eigenvectors", "compute_fourier_diagnostics", "build_projected_q_modes",
+__all__ = ["compute_yee_lwrq_metrics", "recover_original_eigenvectors", "compute_fourier_diagnostics", "build_projected_q_modes",
            "build_yee_points", "build_yee_block_partition", "reconstruct_field_direct_blocked",
            "reconstruct_field_direct_grid", "taylor_on_blocks", "reconstruct_field_taylor_multi",
            "reconstruct_field_taylor_single", "reconstruct_three_components"]
@@ -181,3 +181,42 @@ def reconstruct_three_components(X, sys: QSystem, n, h, method="direct", p=10, n
         for c in range(3):
             out.append(taylor_on_blocks(X[c * NF:(c + 1) * NF], Q, pts[c], p, blocks))
     return out, sz
+
+
+LWRQ_KEYS = ("lambdaCrop", "lambda3D", "eta3D", "etaUsing6DLambda", "deltaLambda", "VLWRQ", "nuLWRQ",
+             "deltaPart", "deltaLWRQIdentity", "croppedMass")
+
+
+def compute_yee_lwrq_metrics(fields, lambda6D, P, n, h, material=("exp", 4.0, 1.2), save_spatial=False, ctx=None):
+    """exp3/compute_yee_lwrq_metrics_exp4.m:1-100 on the GPU.
+
+    ``fields``: the three plus-grid components (complex128 device tensors of
+    (2n+3)^3 points, x fastest, as returned by the Yee reconstruction).
+    ``material``: ("exp", epsC, alpha) or ("cos", delta), sampled on the Yee
+    edges with the cut matrix ``P`` (6 x 3).  Returns ``(metrics, spatial)``
+    with the reference's field names; ``spatial`` holds the z = 0 and x = 0
+    slices of |rho - lambda3D| / |lambda3D| when ``save_spatial``.
+    """
+    ctx = ctx or default_context()
+    m = 2 * n + 3
+    us = [f.reshape(-1).to(torch.complex128).contiguous() for f in fields]
+    if any(u.numel() != m ** 3 for u in us):
+        raise FameError(L.FAME_ERR_INVALID, "fieldPlus size does not match requested n=%d." % n)
+    Pc = (C.c_double * 18)(*np.asarray(P, dtype=np.float64).reshape(6, 3).ravel(order="F"))
+    kind = 0 if material[0] == "exp" else 1
+    mp0 = float(material[1])
+    mp1 = float(material[2]) if len(material) > 2 else 0.0
+    out = (C.c_double * 10)()
+    q = 2 * n + 1
+    z0 = (C.c_double * (q * q))() if save_spatial else None
+    x0 = (C.c_double * (q * q))() if save_spatial else None
+    call("fame_yee_lwrq_metrics", ctx.bind(), _ptr(us[0]), _ptr(us[1]), _ptr(us[2]), int(n), float(h), Pc, kind,
+         mp0, mp1, float(lambda6D), out, z0, x0)
+    met = dict(h=h, n=n, halfWidth=n * h, lambda6D=lambda6D)
+    met.update({k: float(out[i]) for i, k in enumerate(LWRQ_KEYS)})
+    spatial = None
+    if save_spatial:
+        spatial = dict(relativeDeviation_z0=np.ctypeslib.as_array(z0).reshape(q, q, order="F").copy(),
+                       relativeDeviation_x0=np.ctypeslib.as_array(x0).reshape(q, q, order="F").copy(),
+                       coord=np.arange(-n, n + 1) * h, lambda3D=met["lambda3D"], lambda6D=lambda6D, h=h, n=n)
+    return met, spatial

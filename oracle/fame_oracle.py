@@ -61,7 +61,8 @@ __all__ = [
     "taylor_coeff_alpha", "taylor_on_blocks", "reconstruct_field_taylor_multi",
     "reconstruct_field_taylor_single", "reconstruct_field_direct_blocked",
     "reconstruct_component_taylor_batch", "solve_modes", "dense_reduced_operator",
-    "mass_adjoint_quadratic", "set_fft_workers",
+    "mass_adjoint_quadratic", "set_fft_workers", "apply_cropped_A", "yee_material",
+    "separable_conv3_same", "compute_lwrq", "compute_yee_lwrq_metrics",
 ]
 
 
@@ -888,3 +889,147 @@ def reconstruct_component_taylor_batch(coeffMat, qModes, rPoints, p, blocks):
                         for a in alphaList], axis=1)
         u[ids] = phi @ mom[:, ib, :]
     return u
+
+
+# ------------------------------------------------------------------ LWRQ (a22)
+# Physical validation of a reconstructed Yee field: cropped curl-curl action,
+# scalar material on the Yee edges, local Gaussian-window Rayleigh quotient.
+# Fields are (m, m, m) arrays on the plus-grid (m = 2n+3), axis 0 = x (the
+# column-major order of exp2/build_yee_edge_points_plus.m:11-17).
+
+def _inner(u, dx, dy, dz):
+    """u at the interior points shifted by (dx, dy, dz) cells."""
+    m = u.shape[0]
+    return u[1 + dx:m - 1 + dx, 1 + dy:m - 1 + dy, 1 + dz:m - 1 + dz]
+
+
+def apply_cropped_A(u1, u2, u3, h):
+    """exp3/apply_cropped_A_exp3.m:1-58 — Yee curl-curl on the (2n+1)^3 interior.
+
+    Second differences along one axis and the mixed forward/backward differences
+    of the curl-curl operator, scaled by 1/h^2.
+    """
+    s = _inner
+
+    def second(u, ax):
+        e = [0, 0, 0]
+        e[ax] = 1
+        return 2 * s(u, 0, 0, 0) - s(u, *[-v for v in e]) - s(u, *e)
+
+    def mixed(u, back, fwd):
+        # backward difference along `back` of the forward difference along `fwd`
+        f = [0, 0, 0]
+        f[fwd] = 1
+        b = [0, 0, 0]
+        b[back] = -1
+        fb = [f[i] + b[i] for i in range(3)]
+        return s(u, *fb) - s(u, *b) - s(u, *f) + s(u, 0, 0, 0)
+
+    h2 = 1.0 / (h * h)
+    A1 = h2 * (second(u1, 1) + second(u1, 2) - mixed(u2, 1, 0) - mixed(u3, 2, 0))
+    A2 = h2 * (second(u2, 0) + second(u2, 2) - mixed(u1, 0, 1) - mixed(u3, 2, 1))
+    A3 = h2 * (second(u3, 0) + second(u3, 1) - mixed(u1, 0, 2) - mixed(u2, 1, 2))
+    return A1, A2, A3
+
+
+def yee_material(P, n, h, material):
+    """exp3/sample_scalar_yee_material_exp4.m:1-21 — eps on the three edge grids.
+
+    material: ("exp", epsC, alpha) -> epsC exp(alpha/6 sum_l cos(P_l . x)), or
+    ("cos", delta) -> 1 + delta prod_l (1 + cos(P_l . x))/2.
+    """
+    idx = np.arange(-n, n + 1, dtype=np.float64) * h
+    P = np.asarray(P, dtype=np.float64)
+    out = []
+    for c in range(3):
+        ax = [idx.copy(), idx.copy(), idx.copy()]
+        ax[c] = ax[c] + h / 2
+        X, Y, Z = np.meshgrid(*ax, indexing="ij")
+        if material[0] == "exp":
+            S = sum(np.cos(P[l, 0] * X + P[l, 1] * Y + P[l, 2] * Z) for l in range(P.shape[0]))
+            out.append(material[1] * np.exp(material[2] / 6.0 * S))
+        else:
+            prod = np.ones_like(X)
+            for l in range(P.shape[0]):
+                prod = prod * (1 + np.cos(P[l, 0] * X + P[l, 1] * Y + P[l, 2] * Z)) / 2
+            out.append(1.0 + material[1] * prod)
+    return out
+
+
+def separable_conv3_same(X, k):
+    """exp3/separable_conv3_same_exp4.m:1-7 — zero-padded separable 3D convolution."""
+    R = (len(k) - 1) // 2
+    Y = X
+    for ax in range(3):
+        Z = np.zeros_like(Y)
+        L = Y.shape[ax]
+        for t in range(len(k)):
+            sh = t - R  # Z(i) += k[t] * Y(i - sh)
+            src = [slice(None)] * 3
+            dst = [slice(None)] * 3
+            if sh >= 0:
+                dst[ax] = slice(sh, L)
+                src[ax] = slice(0, L - sh)
+            else:
+                dst[ax] = slice(0, L + sh)
+                src[ax] = slice(-sh, L)
+            Z[tuple(dst)] += k[t] * Y[tuple(src)]
+        Y = Z
+    return Y
+
+
+def compute_lwrq(a, b, h, radius=3, sigma_factor=2.0, mass_floor=1e-14, return_rho=False):
+    """exp3/compute_lwrq_exp4.m:12-58 — column-normalised local Gaussian RQ."""
+    off = np.arange(-radius, radius + 1) * h
+    sigma = sigma_factor * h
+    k = np.exp(-(off ** 2) / sigma ** 2)
+    den = separable_conv3_same(np.ones_like(a), k)
+    if not np.all(np.isfinite(den)) or np.any(den <= 0):
+        raise ValueError("Invalid LWRQ column-normalization denominator.")
+    E = separable_conv3_same(a / den, k)
+    M = separable_conv3_same(b / den, k)
+    if not np.all(np.isfinite(M)) or np.any(M <= mass_floor * M.max()):
+        raise ValueError("Nonpositive or numerically tiny local LWRQ mass encountered.")
+    sumE, sumM = E.sum(), M.sum()
+    lam = sumE / sumM
+    rho = E / M
+    V = np.sum(M * np.abs(rho - lam) ** 2) / (sumM * abs(lam) ** 2)
+    sumA, sumB = a.sum(), b.sum()
+    tiny = np.finfo(np.float64).eps
+    part = max(abs(sumE - sumA) / max(abs(sumA), tiny), abs(sumM - sumB) / max(abs(sumB), tiny))
+    return dict(lam=lam, V=V, nu=np.sqrt(max(V, 0.0)), partitionError=part, rho=rho if return_rho else None)
+
+
+def compute_yee_lwrq_metrics(u1, u2, u3, lambda6D, P, n, h, material, save_spatial=False):
+    """exp3/compute_yee_lwrq_metrics_exp4.m:1-100 — scalar LWRQ diagnostics of a
+    reconstructed Yee field (u_c: (2n+3)^3 arrays, axis 0 = x)."""
+    A1, A2, A3 = apply_cropped_A(u1, u2, u3, h)
+    c1, c2, c3 = (_inner(u, 0, 0, 0) for u in (u1, u2, u3))
+    e1, e2, e3 = yee_material(P, n, h, material)
+    B1, B2, B3 = e1 * c1, e2 * c2, e3 * c3
+    a = np.real(np.conj(c1) * A1 + np.conj(c2) * A2 + np.conj(c3) * A3)
+    b = np.real(np.conj(c1) * B1 + np.conj(c2) * B2 + np.conj(c3) * B3)
+    sumB = b.sum()
+    if sumB <= 0:
+        raise ValueError("Cropped Yee mass is not positive.")
+    lamCrop = a.sum() / sumB
+    L = compute_lwrq(a, b, h, return_rho=save_spatial)
+    lam3 = float(np.real(L["lam"]))
+    dId = abs(lam3 - lamCrop) / max(abs(lamCrop), np.finfo(np.float64).eps)
+    nA = np.sqrt(sum(np.sum(np.abs(x) ** 2) for x in (A1, A2, A3)))
+    nB = np.sqrt(sum(np.sum(np.abs(x) ** 2) for x in (B1, B2, B3)))
+
+    def rsq(lam):
+        return sum(np.sum(np.abs(Ax - lam * Bx) ** 2) for Ax, Bx in ((A1, B1), (A2, B2), (A3, B3)))
+
+    m = dict(h=h, n=n, halfWidth=n * h, lambda6D=lambda6D, lambdaCrop=lamCrop, lambda3D=lam3,
+             eta3D=np.sqrt(rsq(lam3)) / (nA + abs(lam3) * nB),
+             etaUsing6DLambda=np.sqrt(rsq(lambda6D)) / (nA + abs(lambda6D) * nB),
+             deltaLambda=abs(lam3 - lambda6D) / abs(lambda6D), VLWRQ=L["V"], nuLWRQ=L["nu"],
+             deltaPart=L["partitionError"], deltaLWRQIdentity=dId, croppedMass=sumB)
+    spatial = None
+    if save_spatial:
+        c = n
+        spatial = dict(relativeDeviation_z0=np.abs(L["rho"][:, :, c] - lam3) / abs(lam3),
+                       relativeDeviation_x0=np.abs(L["rho"][c, :, :] - lam3) / abs(lam3))
+    return m, spatial

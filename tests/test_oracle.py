@@ -149,3 +149,55 @@ def test_start_vector_deterministic():
     a = O.start_vector(20260905, 10)
     assert np.array_equal(a, O.start_vector(20260905, 10))
     assert np.all(np.abs(a.real) <= 1) and np.all(np.abs(a.imag) <= 1)
+
+
+# ---------------------------------------------------------------- LWRQ (a22)
+def _yee_rand(n, seed):
+    rng = np.random.default_rng(seed)
+    m = 2 * n + 3
+    return [rng.standard_normal((m, m, m)) + 1j * rng.standard_normal((m, m, m)) for _ in range(3)]
+
+
+def test_cropped_curlcurl_annihilates_discrete_gradients():
+    """The Yee curl-curl of exp3/apply_cropped_A_exp3.m vanishes on forward-difference gradients."""
+    n, h = 5, 0.04
+    idx = np.arange(-(n + 1), n + 2) * h
+    X, Y, Z = np.meshgrid(idx, idx, idx, indexing="ij")
+    phi = lambda x, y, z: np.sin(3 * x + 1) * np.cos(2 * y) * np.exp(z)  # noqa: E731
+    g = [(phi(X + h, Y, Z) - phi(X, Y, Z)) / h, (phi(X, Y + h, Z) - phi(X, Y, Z)) / h,
+         (phi(X, Y, Z + h) - phi(X, Y, Z)) / h]
+    A = O.apply_cropped_A(*(c + 0j for c in g), h)
+    scale = max(np.abs(c).max() for c in g) / h ** 2
+    assert max(np.abs(a).max() for a in A) < 1e-12 * scale
+
+
+def test_separable_window_matches_direct_convolution():
+    from scipy.ndimage import convolve1d
+    rng = np.random.default_rng(3)
+    X = rng.standard_normal((6, 7, 9))
+    k = np.exp(-np.arange(-3, 4) ** 2 / 4.0)
+    Y = X
+    for ax in range(3):
+        Y = convolve1d(Y, k, axis=ax, mode="constant", cval=0.0)
+    assert np.abs(Y - O.separable_conv3_same(X, k)).max() < 1e-13
+
+
+def test_lwrq_partition_of_unity_and_constant_quotient():
+    """Column normalisation preserves the totals; a = lambda b gives rho = lambda, V = 0."""
+    rng = np.random.default_rng(4)
+    b = rng.uniform(0.5, 2.0, (9, 9, 9))
+    a = rng.standard_normal((9, 9, 9))
+    L = O.compute_lwrq(a, b, 0.05)
+    assert L["partitionError"] < 1e-14
+    L2 = O.compute_lwrq(0.37 * b, b, 0.05)
+    assert abs(L2["lam"] - 0.37) < 1e-15 and L2["V"] < 1e-28
+
+
+def test_lwrq_metrics_consistency():
+    n, h = 4, 0.05
+    u = _yee_rand(n, 5)
+    P = np.vstack([np.eye(3), np.diag([np.sqrt(2), np.sqrt(3), np.sqrt(5)])])
+    met, sp = O.compute_yee_lwrq_metrics(*u, 0.5, P, n, h, ("exp", 4.0, 1.2), save_spatial=True)
+    assert met["deltaPart"] < 1e-14 and met["deltaLWRQIdentity"] < 1e-13
+    assert met["croppedMass"] > 0 and 0 <= met["eta3D"] <= met["etaUsing6DLambda"] + 1e-15
+    assert sp["relativeDeviation_z0"].shape == (2 * n + 1, 2 * n + 1)
