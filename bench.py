@@ -264,12 +264,12 @@ def run_fame(args):
                 if method == "direct":
                     out.append(F.reconstruct_field_direct_grid(xc, sysq, axes[c]))
                 else:
-                    out.append(F.taylor_on_blocks(xc, Qm, pts[c], 10, blocks))
+                    out.append(F.taylor_on_blocks(xc, Qm, pts[c], 10, blocks, tensor_cores=(method == "taylor_tc")))
             return out
 
         times = {}
         fields = {}
-        for method in ("direct", "taylor"):
+        for method in ("direct", "taylor", "taylor_tc"):
             recon(method)
             samples = []
             for _ in range(5):  # median of 5 (three components each)
@@ -279,12 +279,18 @@ def run_fame(args):
                 torch.cuda.synchronize()
                 samples.append(time.perf_counter() - t0)
             times[method] = sorted(samples)[len(samples) // 2]
-        err = float(sum(torch.linalg.norm(a - b) ** 2 for a, b in zip(fields["taylor"], fields["direct"])) ** 0.5 /
-                    sum(torch.linalg.norm(b) ** 2 for b in fields["direct"]) ** 0.5)
+        def field_err(x, y):
+            return float(sum(torch.linalg.norm(a - b) ** 2 for a, b in zip(x, y)) ** 0.5 /
+                         sum(torch.linalg.norm(b) ** 2 for b in y) ** 0.5)
+        err = field_err(fields["taylor"], fields["direct"])
         yee = {"points_per_component": M, "n": n_yee, "h": h_yee, "mode": 10,
                "direct_pts_per_s": round(3 * M / times["direct"], 1),
                "taylor_p10_64c_pts_per_s": round(3 * M / times["taylor"], 1),
                "taylor_rel_err_vs_direct": err, "timing": "median of 5 repetitions, 3 components each",
+               "taylor_3xtf32_pts_per_s": round(3 * M / times["taylor_tc"], 1),
+               "taylor_3xtf32_rel_err_vs_fp64_taylor": field_err(fields["taylor_tc"], fields["taylor"]),
+               "taylor_3xtf32_rel_err_vs_direct": field_err(fields["taylor_tc"], fields["direct"]),
+               "taylor_3xtf32_form": "moments as split-FP32 tcgen05 GEMMs (CUTLASS sm100 UMMA), FP64 evaluation",
                "direct_form": "factorised tensor-grid sum (axis-block cut matrix), FP64",
                "taylor_form": "multi-center Taylor p=10, 4^3 centers, FP64"}
         # LWRQ validation of the reconstructed field (material sampled on the Yee edges)

@@ -249,6 +249,15 @@ FAME_API int fame_taylor_on_blocks(fame_ctx* ctx, const void* coeff, const doubl
                                    long long NF, const double* rPoints, long long M, int p,
                                    const long long* blockPtr, const long long* blockIds,
                                    int nBlocks, const double* fixedCenter, void* u);
+/* Same reconstruction with the block moments (the dense contraction over the NF modes) as
+   split-FP32 tensor-core products: each FP32 operand is split into TF32 head + tail and the
+   moments are head*head + head*tail + tail*head (3xTF32), computed by tcgen05 UMMA GEMMs
+   (CUTLASS sm100 collectives) and reduced in FP64.  Relative field error vs the FP64 form ~1e-7.
+   No counterpart in the reference (its Taylor moments are FP64 gpuArray products). */
+FAME_API int fame_taylor_on_blocks_3xtf32(fame_ctx* ctx, const void* coeff, const double* qModes, long long NF,
+                                          const double* rPoints, long long M, int p, const long long* blockPtr,
+                                          const long long* blockIds, int nBlocks, const double* fixedCenter,
+                                          void* u);
 
 /* ---- mass-operator adjoint (no reference function; eigenvalue gradients) ---- */
 /* out[j*nparams + t] = X(:,j)^H (dM/dtheta_t) X(:,j) for the 3-component mass

@@ -61,6 +61,11 @@ int check_fault(fame_ctx* ctx);
 // At least `bytes` of device workspace owned by ctx, reused across calls (grown
 // after a stream synchronisation); valid until the next call on the context.
 int ctx_workspace(fame_ctx* ctx, size_t bytes, void** out);
+// Batched TF32 tensor-core GEMM (tc_gemm.cu): D[l] = A_l B_l^T, A: M x (L*K), B: N x (L*K),
+// both row-major with leading dimension ldk; D: L packed M x N row-major.
+size_t tf32_gemm_workspace(int M, int N, int K, int L, long long ldk);
+int tf32_gemm_batched(int M, int N, int K, int L, long long ldk, const float* A, const float* B, float* D,
+                      void* workspace, cudaStream_t st);
 // Consecutive 256-byte aligned pieces of one workspace.
 struct Carve {
   size_t used = 0;

@@ -96,6 +96,7 @@ SIGNATURES = {
     "fame_reconstruct_direct": [P, P, P, LL, P, LL, P],
     "fame_reconstruct_direct_grid": [P, P, P, I, P, I, P, I, P],
     "fame_taylor_on_blocks": [P, P, P, LL, P, LL, I, P, P, I, C.POINTER(D), P],
+    "fame_taylor_on_blocks_3xtf32": [P, P, P, LL, P, LL, I, P, P, I, C.POINTER(D), P],
     "fame_mass_adjoint": [P, P, I, P, I, C.POINTER(D)],
     "fame_yee_lwrq_metrics": [P, P, P, P, I, D, C.POINTER(D), I, D, D, D, C.POINTER(D), C.POINTER(D), C.POINTER(D)],
     "fame_solve_batch": [I, I, C.POINTER(I), C.POINTER(P), C.POINTER(D), C.POINTER(D),

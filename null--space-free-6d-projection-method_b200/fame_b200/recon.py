@@ -140,8 +140,11 @@ def reconstruct_field_direct_grid(coeff, sys: QSystem, axes):
     return u
 
 
-def taylor_on_blocks(coeff, qModes, rPoints, p, blocks, fixedCenter=None, ctx=None):
-    """exp2/taylor_on_blocks_exp3.m:1-97 — ``blocks`` = (blockPtr, blockIds) CSR tensors."""
+def taylor_on_blocks(coeff, qModes, rPoints, p, blocks, fixedCenter=None, ctx=None, tensor_cores=False):
+    """exp2/taylor_on_blocks_exp3.m:1-97 — ``blocks`` = (blockPtr, blockIds) CSR tensors.
+
+    ``tensor_cores``: block moments as 3xTF32 tensor-core GEMMs (split-FP32) instead of FP64.
+    """
     ctx = ctx or default_context()
     Qc = qModes.t().contiguous()
     Rc, M = _pts(rPoints)
@@ -149,14 +152,15 @@ def taylor_on_blocks(coeff, qModes, rPoints, p, blocks, fixedCenter=None, ctx=No
     ptr, ids = blocks
     u = torch.zeros(M, dtype=torch.complex128, device=c.device)
     fc = (C.c_double * 3)(*fixedCenter) if fixedCenter is not None else None
-    call("fame_taylor_on_blocks", ctx.bind(), _ptr(c), _ptr(Qc), c.numel(), _ptr(Rc), M, int(p),
+    call("fame_taylor_on_blocks_3xtf32" if tensor_cores else "fame_taylor_on_blocks", ctx.bind(), _ptr(c), _ptr(Qc),
+         c.numel(), _ptr(Rc), M, int(p),
          _ptr(ptr), _ptr(ids), ptr.numel() - 1, fc, _ptr(u))
     return u
 
 
-def reconstruct_field_taylor_multi(coeff, qModes, rPoints, p, blocks):
+def reconstruct_field_taylor_multi(coeff, qModes, rPoints, p, blocks, tensor_cores=False):
     """exp2/reconstruct_field_taylor_multi_exp3.m:1-10."""
-    return taylor_on_blocks(coeff, qModes, rPoints, p, blocks, None)
+    return taylor_on_blocks(coeff, qModes, rPoints, p, blocks, None, tensor_cores=tensor_cores)
 
 
 def reconstruct_field_taylor_single(coeff, qModes, rPoints, p, r0=(0.0, 0.0, 0.0)):

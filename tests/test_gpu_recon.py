@@ -126,3 +126,19 @@ def test_batched_bloch_path_matches_single_solves(cuda_device):
         _, th, _, info = F.Lanczos(op, None, None, s.nr, 6, 1e-10, 30, 40, F.start_vector(F.configs.SEED, s.nr))
         assert infos[i]["converged"]
         np.testing.assert_allclose(lam[i], np.sort(1.0 / th), rtol=1e-10)
+
+
+@pytest.mark.parametrize("N,p,nb", [(2, 6, 2), (2, 10, 3), (3, 8, 2)])
+def test_taylor_3xtf32_tensor_cores_vs_fp64(cuda_device, N, p, nb):
+    """Split-FP32 (3xTF32) tensor-core block moments vs the FP64 form (same centers,
+    same evaluation): relative field error at FP32 level."""
+    F, S, sg, m = _sys(N, cuda_device)
+    Q = F.build_projected_q_modes(sg)
+    c = torch.as_tensor(O.start_vector(13, S.NF), device=cuda_device)
+    pts, axes, sz = F.build_yee_points(6, 0.0125)
+    blocks = F.build_yee_block_partition(sz, nb)
+    u64 = F.taylor_on_blocks(c, Q, pts[1], p, blocks).cpu().numpy()
+    utc = F.taylor_on_blocks(c, Q, pts[1], p, blocks, tensor_cores=True).cpu().numpy()
+    assert rel(utc, u64) < 2e-6, rel(utc, u64)
+    utc2 = F.taylor_on_blocks(c, Q, pts[1], p, blocks, tensor_cores=True).cpu().numpy()
+    assert np.array_equal(utc, utc2)  # deterministic
