@@ -290,7 +290,7 @@ def run_fame(args):
                "taylor_3xtf32_pts_per_s": round(3 * M / times["taylor_tc"], 1),
                "taylor_3xtf32_rel_err_vs_fp64_taylor": field_err(fields["taylor_tc"], fields["taylor"]),
                "taylor_3xtf32_rel_err_vs_direct": field_err(fields["taylor_tc"], fields["direct"]),
-               "taylor_3xtf32_form": "moments as split-FP32 tcgen05 GEMMs (CUTLASS sm100 UMMA), FP64 evaluation",
+               "taylor_3xtf32_form": "moments as split-FP32 (3xTF32) tcgen05 MMAs, operands generated in shared memory, FP32 TMEM accumulation over 512-mode slices, FP64 slice sum and evaluation",
                "direct_form": "factorised tensor-grid sum (axis-block cut matrix), FP64",
                "taylor_form": "multi-center Taylor p=10, 4^3 centers, FP64"}
         # LWRQ validation of the reconstructed field (material sampled on the Yee edges)

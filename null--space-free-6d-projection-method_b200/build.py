@@ -46,33 +46,11 @@ def _newest(paths):
     return max(os.path.getmtime(p) for p in paths)
 
 
-def cutlass_includes():
-    """CUTLASS/CuTe header trees (sm100 UMMA collectives) for csrc/tc_gemm.cu:
-    $FAME_CUTLASS_DIR, else the copies vendored by installed Python packages."""
-    cands = [os.environ.get("FAME_CUTLASS_DIR", "")]
-    for mod, sub in (("flashinfer", "data/cutlass"), ("tilelang", "3rdparty/cutlass")):
-        try:
-            import importlib.util
-            spec = importlib.util.find_spec(mod)
-            if spec and spec.submodule_search_locations:
-                cands.append(os.path.join(list(spec.submodule_search_locations)[0], sub))
-        except Exception:
-            pass
-    for c in cands:
-        if c and os.path.exists(os.path.join(c, "include", "cute", "arch", "mma_sm100_umma.hpp")):
-            return ["-I", os.path.join(c, "include"), "-I", os.path.join(c, "tools", "util", "include")]
-    return None
-
-
 def _compile(src, force):
     obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
     if not force and os.path.exists(obj) and os.path.getmtime(obj) >= _newest([src] + headers()):
         return obj
-    extra = []
-    if os.path.basename(src) == "tc_gemm.cu":
-        inc = cutlass_includes()
-        extra = inc + ["-diag-suppress", "20012"] if inc else ["-DFAME_NO_CUTLASS"]
-    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-I", INCLUDE, *extra, "-c", src, "-o", obj]
+    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-I", INCLUDE, "-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("nvcc failed for %s:\n%s\n%s" % (src, r.stdout, r.stderr))

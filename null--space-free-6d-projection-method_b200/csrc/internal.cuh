@@ -61,11 +61,18 @@ int check_fault(fame_ctx* ctx);
 // At least `bytes` of device workspace owned by ctx, reused across calls (grown
 // after a stream synchronisation); valid until the next call on the context.
 int ctx_workspace(fame_ctx* ctx, size_t bytes, void** out);
-// Batched TF32 tensor-core GEMM (tc_gemm.cu): D[l] = A_l B_l^T, A: M x (L*K), B: N x (L*K),
-// both row-major with leading dimension ldk; D: L packed M x N row-major.
-size_t tf32_gemm_workspace(int M, int N, int K, int L, long long ldk);
-int tf32_gemm_batched(int M, int N, int K, int L, long long ldk, const float* A, const float* B, float* D,
-                      void* workspace, cudaStream_t st);
+// Taylor block moments on the tensor cores (taylor_tc.cu): launch shape and the
+// FP32 partial-moment buffer (out_floats) it needs.
+struct TaylorTcPlan {
+  int Npad = 0, stages = 0, ntiles = 0, groups = 0;
+  long long Kc = 0, nslices = 0;
+  size_t smem = 0, out_floats = 0;
+};
+TaylorTcPlan taylor_tc_plan(long long NF, int nB, int L);
+// gamma[b L + a] = coef[a] sum_j c_j e^{i q_j.r_b} q_j^a, with alistPacked[a] = a1 | a2 << 8 | a3 << 16.
+int taylor_moments_tc(const TaylorTcPlan& plan, cudaStream_t s, const double2* c, const double* Q, long long NF,
+                      const double* centers, int nB, const int* alistPacked, int L, int p, const double2* coef,
+                      float* out, double2* gamma);
 // Consecutive 256-byte aligned pieces of one workspace.
 struct Carve {
   size_t used = 0;

@@ -203,18 +203,18 @@ __global__ void __launch_bounds__(512) k_taylor_moments(const double2* __restric
   for (long long j0 = j0c; j0 < j1c; j0 += kTaySub) {
     const int nj = (int)std::min<long long>(kTaySub, j1c - j0);
     __syncthreads();
-    if ((int)threadIdx.x < nj) {
-      const long long j = j0 + threadIdx.x;
+    for (int t = threadIdx.x; t < nj; t += blockDim.x) {
+      const long long j = j0 + t;
       const double qx = Q[j], qy = Q[NF + j], qz = Q[2 * NF + j];
       double s, co;
       sincos(qx * cx + qy * cy + qz * cz, &s, &co);
       const double2 cj = c[j];
-      w[threadIdx.x] = make_double2(cj.x * co - cj.y * s, cj.x * s + cj.y * co);
+      w[t] = make_double2(cj.x * co - cj.y * s, cj.x * s + cj.y * co);
       double px = 1.0, py = 1.0, pz = 1.0;
       for (int k = 0; k <= p; ++k) {
-        pw[0][threadIdx.x][k] = px;
-        pw[1][threadIdx.x][k] = py;
-        pw[2][threadIdx.x][k] = pz;
+        pw[0][t][k] = px;
+        pw[1][t][k] = py;
+        pw[2][t][k] = pz;
         px *= qx;
         py *= qy;
         pz *= qz;
@@ -244,87 +244,6 @@ __global__ void k_taylor_reduce(const double2* partial, int nChunks, int nB, int
     ai += v.y;
   }
   const double2 cf = coef[t % L];
-  gamma[t] = make_double2(cf.x * ar - cf.y * ai, cf.x * ai + cf.y * ar);
-}
-
-// ---- 3xTF32 tensor-core moments: gamma = coef .* (Qalpha (L x NF) * W (NF x 2 nB)), with each
-// FP32 operand split into a TF32 head and a TF32 tail, x = big + small, and the product taken as
-// big*big + big*small + small*big (the tail-tail term is below FP32 resolution).
-__device__ __forceinline__ float tf32_rna(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
-}
-__device__ __forceinline__ void split3(double v, float& big, float& small) {
-  big = tf32_rna((float)v);
-  small = tf32_rna((float)(v - (double)big));
-}
-
-// Ab/As[a*ldk + j] = split of qx^a1 qy^a2 qz^a3 (zero for NF <= j < ldk)
-__global__ void __launch_bounds__(256) k_tc_monomials(const double* __restrict__ Q, long long NF, const int* __restrict__ alist,
-                                                     int L, int p, long long ldk, float* __restrict__ Ab,
-                                                     float* __restrict__ As) {
-  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < ldk; j += (long long)gridDim.x * blockDim.x) {
-    double px[kMaxP + 1], py[kMaxP + 1], pz[kMaxP + 1];
-    const bool in = j < NF;
-    const double qx = in ? Q[j] : 0.0, qy = in ? Q[NF + j] : 0.0, qz = in ? Q[2 * NF + j] : 0.0;
-    px[0] = py[0] = pz[0] = in ? 1.0 : 0.0;
-    for (int k = 1; k <= p; ++k) {
-      px[k] = px[k - 1] * qx;
-      py[k] = py[k - 1] * qy;
-      pz[k] = pz[k - 1] * qz;
-    }
-    for (int a = 0; a < L; ++a) {
-      float big, small;
-      split3(px[alist[3 * a]] * py[alist[3 * a + 1]] * pz[alist[3 * a + 2]], big, small);
-      Ab[(long long)a * ldk + j] = big;
-      As[(long long)a * ldk + j] = small;
-    }
-  }
-}
-
-// Bb/Bs rows 2b, 2b+1 = split of Re, Im of c_j exp(i q_j . r_b); zero rows >= 2 nB, zero j >= NF
-__global__ void __launch_bounds__(256) k_tc_phase(const double2* __restrict__ c, const double* __restrict__ Q, long long NF,
-                                                 const double* __restrict__ centers, int nB, int Npad, long long ldk,
-                                                 float* __restrict__ Bb, float* __restrict__ Bs) {
-  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < ldk; j += (long long)gridDim.x * blockDim.x) {
-    const bool in = j < NF;
-    const double qx = in ? Q[j] : 0.0, qy = in ? Q[NF + j] : 0.0, qz = in ? Q[2 * NF + j] : 0.0;
-    const double2 cj = in ? c[j] : make_double2(0.0, 0.0);
-    for (int b = 0; b < Npad / 2; ++b) {
-      double wr = 0.0, wi = 0.0;
-      if (b < nB) {
-        double s, co;
-        sincos(qx * centers[3 * b] + qy * centers[3 * b + 1] + qz * centers[3 * b + 2], &s, &co);
-        wr = cj.x * co - cj.y * s;
-        wi = cj.x * s + cj.y * co;
-      }
-      float big, small;
-      split3(wr, big, small);
-      Bb[(long long)(2 * b) * ldk + j] = big;
-      Bs[(long long)(2 * b) * ldk + j] = small;
-      split3(wi, big, small);
-      Bb[(long long)(2 * b + 1) * ldk + j] = big;
-      Bs[(long long)(2 * b + 1) * ldk + j] = small;
-    }
-  }
-}
-
-// gamma[b*L + a] = coef[a] * sum over the three products and the nbat K-slices (FP64, fixed order)
-__global__ void k_tc_reduce(const float* __restrict__ D, int nbat, int L, int Npad, int nB, const double2* __restrict__ coef,
-                            double2* __restrict__ gamma) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= (long long)nB * L) return;
-  const int b = (int)(t / L), a = (int)(t % L);
-  const long long per = (long long)nbat * L * Npad;
-  double ar = 0.0, ai = 0.0;
-  for (int g = 0; g < 3; ++g)
-    for (int l = 0; l < nbat; ++l) {
-      const float* d = D + g * per + ((long long)l * L + a) * Npad;
-      ar += (double)d[2 * b];
-      ai += (double)d[2 * b + 1];
-    }
-  const double2 cf = coef[a];
   gamma[t] = make_double2(cf.x * ar - cf.y * ai, cf.x * ai + cf.y * ar);
 }
 
@@ -439,7 +358,8 @@ int fame_reconstruct_direct_grid(fame_basis* bs, const void* coeff, const double
 namespace fame {
 
 // Multi-center Taylor reconstruction (exp2/taylor_on_blocks_exp3.m:1-97); the block
-// moments either in FP64 on the CUDA cores or as 3xTF32 tensor-core GEMMs.
+// moments either in FP64 on the CUDA cores or as 3xTF32 products on the tensor cores
+// (taylor_tc.cu).
 static int taylor_impl(fame_ctx* ctx, const void* coeff, const double* qModes, long long NF, const double* rPoints,
                        long long M, int p, const long long* blockPtr, const long long* blockIds, int nBlocks,
                        const double* fixedCenter, void* u, bool tc) {
@@ -464,33 +384,24 @@ static int taylor_impl(fame_ctx* ctx, const void* coeff, const double* qModes, l
   const int L = (int)cf.size();
   if (L > 512) return fail(FAME_ERR_UNSUPPORTED, "too many Taylor terms");
   const int nChunks = (int)((NF + kTayChunk - 1) / kTayChunk);
-  // tensor-core layout: K split into nbat slices of Kc (multiple of 128), N = 2 nB padded to 4
-  const int Npad = (2 * nBlocks + 3) / 4 * 4;
-  const int tiles = ((L + 127) / 128) * ((Npad + 127) / 128);
-  int nbat = std::max(1, (2 * num_sms() + tiles - 1) / tiles);
-  nbat = (int)std::max<long long>(1, std::min<long long>(nbat, NF / 1024));
-  const long long Kc = ((NF + nbat - 1) / nbat + 127) / 128 * 128;
-  const long long ldk = Kc * nbat;
-  const size_t gws = tc ? tf32_gemm_workspace(L, Npad, (int)Kc, nbat, ldk) : 0;
+  const TaylorTcPlan tp = tc ? taylor_tc_plan(NF, nBlocks, L) : TaylorTcPlan{};
+  std::vector<int> packed;
+  if (tc)
+    for (int a = 0; a < L; ++a) packed.push_back(al[3 * a] | al[3 * a + 1] << 8 | al[3 * a + 2] << 16);
   cudaStream_t s = ctx->stream;
-  int* dal;
+  int *dal, *dpk;
   double2 *dcf, *partial, *gamma;
   double *centers, *dfix;
-  float *Ab, *As, *Bb, *Bs, *D;
-  char* gw;
+  float* tout;
   auto carve = [&](Carve& cv) {
     dal = cv.take<int>(al.size());
+    dpk = cv.take<int>(tc ? packed.size() : 1);
     dcf = cv.take<double2>(cf.size());
     partial = cv.take<double2>(tc ? 1 : (size_t)nChunks * nBlocks * L);
     gamma = cv.take<double2>((size_t)nBlocks * L);
     centers = cv.take<double>((size_t)nBlocks * 3);
     dfix = cv.take<double>(3);
-    Ab = cv.take<float>(tc ? (size_t)L * ldk : 1);
-    As = cv.take<float>(tc ? (size_t)L * ldk : 1);
-    Bb = cv.take<float>(tc ? (size_t)Npad * ldk : 1);
-    Bs = cv.take<float>(tc ? (size_t)Npad * ldk : 1);
-    D = cv.take<float>(tc ? (size_t)3 * nbat * L * Npad : 1);
-    gw = cv.take<char>(gws + 16);
+    tout = cv.take<float>(tc ? tp.out_floats : 1);
   };
   Carve size_only;
   carve(size_only);
@@ -514,18 +425,8 @@ static int taylor_impl(fame_ctx* ctx, const void* coeff, const double* qModes, l
       k_taylor_reduce<<<(nBlocks * L + 255) / 256, 256, 0, s>>>(partial, nChunks, nBlocks, L, dcf, gamma);
       ::fame::count_launch();
     } else {
-      const int gb = (int)std::min<long long>((ldk + 255) / 256, 148 * 8);
-      k_tc_monomials<<<gb, 256, 0, s>>>(qModes, NF, dal, L, p, ldk, Ab, As);
-      k_tc_phase<<<gb, 256, 0, s>>>((const double2*)coeff, qModes, NF, centers, nBlocks, Npad, ldk, Bb, Bs);
-      ::fame::count_launch(2);
-      const long long per = (long long)nbat * L * Npad;
-      st = tf32_gemm_batched(L, Npad, (int)Kc, nbat, ldk, Ab, Bb, D, gw, s);
-      if (st == FAME_OK) st = tf32_gemm_batched(L, Npad, (int)Kc, nbat, ldk, Ab, Bs, D + per, gw, s);
-      if (st == FAME_OK) st = tf32_gemm_batched(L, Npad, (int)Kc, nbat, ldk, As, Bb, D + 2 * per, gw, s);
-      if (st == FAME_OK) {
-        k_tc_reduce<<<(nBlocks * L + 255) / 256, 256, 0, s>>>(D, nbat, L, Npad, nBlocks, dcf, gamma);
-        ::fame::count_launch();
-      }
+      cudaMemcpyAsync(dpk, packed.data(), packed.size() * sizeof(int), cudaMemcpyHostToDevice, s);
+      st = taylor_moments_tc(tp, s, (const double2*)coeff, qModes, NF, centers, nBlocks, dpk, L, p, dcf, tout, gamma);
     }
     // one grid column per block; x-extent covers the largest block
     std::vector<long long> hp(nBlocks + 1);

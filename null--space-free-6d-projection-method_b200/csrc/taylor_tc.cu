@@ -1,0 +1,356 @@
+// Taylor block moments on the tcgen05 tensor cores, operands generated on chip.
+//
+// gamma[b, a] = coef[a] * sum_j c_j exp(i q_j . r_b) q_j^a
+// (exp2/taylor_on_blocks_exp3.m:53-54,65-73: the moment GEMM Qalpha^T (c .* phase)).
+//
+// One CTA owns a slice of Kc modes and a tile of 64 block centers.  Per stage of
+// 32 modes its threads write into shared memory, in the 128-byte swizzled
+// K-major UMMA layout and split into TF32 head + tail (3xTF32):
+//   A (128 x 32): rows 2b, 2b+1 = Re, Im of c_j exp(i q_j . r_b)   (FP64 phase, FP32 sincosf)
+//   B (Npad x 32): row a = qx^a1 qy^a2 qz^a3                          (FP64 products)
+// Fifteen generator warps fill a stage and arrive on its "full" mbarrier; a
+// sixteenth warp waits for it and issues tcgen05.mma kind::tf32 for
+// Ahi*Bhi + Ahi*Blo + Alo*Bhi into one FP32 TMEM accumulator of 128 lanes x Npad
+// columns, committing to the stage's "empty" mbarrier, while the generators fill
+// the other stage (two stages when they fit).  The slice's partial moments
+// go to HBM (FP32) and a second kernel sums the slices in FP64 in a fixed order.
+// Neither Qalpha (L x NF) nor the phase matrix ever exists in HBM: the kernel reads
+// 40 bytes per mode.
+#include "internal.cuh"
+#include "umma.cuh"
+
+namespace fame {
+namespace {
+
+constexpr int kGenWarps = 15;                 // operand generators
+constexpr int kGenThreads = kGenWarps * 32;
+constexpr int kThreads = kGenThreads + 32;    // + the MMA-issuing warp (16 warps: 128 registers)
+constexpr int kKC = 32;        // modes per stage (one swizzle atom of TF32)
+constexpr int kBT = 64;        // block centers per accumulator tile (128 rows)
+constexpr int kBPW = (kBT + kGenWarps - 1) / kGenWarps;  // block centers per generator warp, at most
+constexpr int kBlockCost = 3;  // generation cost of one block center (Re, Im rows) in monomial rows
+constexpr int kPmax = 12;
+constexpr int kLmax = 512;
+// Modes per slice accumulated in one FP32 TMEM accumulator at most.  The tensor
+// cores round that accumulation toward zero, so its error grows with the slice;
+// measured on eigenmode 10 at N = 5 (p = 10, 64 centers), field error vs the FP64
+// moments: 2048 modes 6.2e-6, 1024 3.4e-6, 512 2.4e-6, 256 1.3e-6, at 1.00 / 1.07 /
+// 1.15 / 1.35 times the time of 2048.
+constexpr long long kKcMax = 512;
+constexpr uint32_t kABytes = 128u * 128u;  // one TF32 part of the phase operand
+
+__host__ __device__ inline uint32_t b_bytes(int Npad) { return (uint32_t)Npad * 128u; }
+__host__ __device__ inline uint32_t stage_bytes(int Npad) { return 2u * (kABytes + b_bytes(Npad)); }
+constexpr size_t kTailBytes = kBT * 3 * sizeof(double)               // centers
+                              + kLmax * sizeof(int)                    // packed multi-indices
+                              + 5 * sizeof(uint64_t) + 16;             // mbarriers, TMEM slot, abort flag
+inline size_t tc_smem(int Npad, int stages) { return 1024 + (size_t)stages * stage_bytes(Npad) + kTailBytes; }
+
+struct TcArgs {
+  const double* Q;      // 3 x NF (rows qx, qy, qz)
+  const double2* c;     // NF
+  long long NF;
+  const double* centers;  // nB x 3
+  int nB;
+  const int* alist;     // L packed multi-indices a1 | a2 << 8 | a3 << 16
+  int L, p, Npad, stages;
+  long long Kc;
+  float* out;           // [slice][tile][128][Npad]
+};
+
+__device__ __forceinline__ void put(unsigned char* base, int row, int k, float v) {
+  *reinterpret_cast<float*>(base + umma::sw128_offset(row, k)) = v;
+}
+
+__global__ void __launch_bounds__(kThreads, 1) k_taylor_moments_tc(TcArgs a, unsigned* fault) {
+  extern __shared__ unsigned char smraw[];
+  unsigned char* sm = smraw + ((1024u - (smem_u32(smraw) & 1023u)) & 1023u);
+  const int Npad = a.Npad, S = a.stages;
+  const uint32_t bB = b_bytes(Npad), stB = stage_bytes(Npad);
+  double* cen = reinterpret_cast<double*>(sm + (size_t)S * stB);  // [kBT][3]
+  int* al = reinterpret_cast<int*>(cen + kBT * 3);                  // [kLmax]
+  uint64_t* full = reinterpret_cast<uint64_t*>(al + kLmax);         // [2]: stage written
+  uint64_t* empty = full + 2;                                       // [2]: stage read by the MMAs
+  uint64_t* done = full + 4;                                        // every MMA complete
+  uint32_t* slot = reinterpret_cast<uint32_t*>(full + 5);
+  volatile int* abortf = reinterpret_cast<volatile int*>(slot + 1);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long long z = blockIdx.x;
+  const int bt = blockIdx.y;
+  const long long j0 = z * a.Kc, j1 = j0 + a.Kc < a.NF ? j0 + a.Kc : a.NF;
+  const int nch = (int)((j1 - j0 + kKC - 1) / kKC);
+  const int nbl = a.nB - bt * kBT < kBT ? a.nB - bt * kBT : kBT;
+  const uint32_t ncols = Npad <= 32 ? 32u : Npad <= 64 ? 64u : Npad <= 128 ? 128u : Npad <= 256 ? 256u : 512u;
+
+  for (int t = tid; t < a.L; t += kThreads) al[t] = a.alist[t];
+  for (int t = tid; t < kBT * 3; t += kThreads) cen[t] = t / 3 < nbl ? a.centers[(long long)bt * kBT * 3 + t] : 0.0;
+  if (tid == 0) {
+    for (int s = 0; s < 2; ++s) {
+      mbar_init(&full[s], kGenThreads);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    *abortf = 0;
+    mbar_init_fence();
+  }
+  if (warp == 0) {
+    umma::tmem_alloc(slot, ncols);
+    umma::tmem_relinquish();
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = *slot;
+
+  if (warp < kGenWarps) {
+    // block centers bl = warp + u * kGenWarps are this warp's; monomial rows [r0, r1) too,
+    // sized so that every warp gets the same share of (kBlockCost * blocks + rows)
+    auto row_start = [&](int w) {
+      const int total = kBlockCost * kBT + Npad;
+      int rs = 0;
+      for (int v = 1; v <= w; ++v) {
+        const int blocksBefore = v < kBT % kGenWarps ? v * kBPW : (kBT % kGenWarps) * kBPW + (v - kBT % kGenWarps) * (kBPW - 1);
+        int t = (v * total + kGenWarps / 2) / kGenWarps - kBlockCost * blocksBefore;
+        t = t < rs ? rs : t;
+        rs = t < Npad ? t : Npad;
+      }
+      return w >= kGenWarps ? Npad : rs;
+    };
+    const int r0 = row_start(warp), r1 = row_start(warp + 1);
+    const int e0 = r0 < a.L ? al[r0] : 0;
+    double cx[kBPW], cy[kBPW], cz[kBPW];
+#pragma unroll
+    for (int u = 0; u < kBPW; ++u) {
+      const int bl = warp + u * kGenWarps;
+      cx[u] = bl < kBT ? cen[3 * bl] : 0.0;
+      cy[u] = bl < kBT ? cen[3 * bl + 1] : 0.0;
+      cz[u] = bl < kBT ? cen[3 * bl + 2] : 0.0;
+    }
+    // this lane's mode of the next stage, loaded one stage ahead
+    double nqx = 0.0, nqy = 0.0, nqz = 0.0;
+    double2 ncj = make_double2(0.0, 0.0);
+    if (j0 + lane < j1) {
+      nqx = a.Q[j0 + lane];
+      nqy = a.Q[a.NF + j0 + lane];
+      nqz = a.Q[2 * a.NF + j0 + lane];
+      ncj = a.c[j0 + lane];
+    }
+    for (int i = 0; i < nch; ++i) {
+      const int s = i % S;
+      unsigned char* stg = sm + (size_t)s * stB;
+      const long long j = j0 + (long long)i * kKC + lane;
+      const bool in = j < j1;
+      const double qx = nqx, qy = nqy, qz = nqz;
+      const double2 cj = ncj;
+      if (j + kKC < j1) {
+        nqx = a.Q[j + kKC];
+        nqy = a.Q[a.NF + j + kKC];
+        nqz = a.Q[2 * a.NF + j + kKC];
+        ncj = a.c[j + kKC];
+      }
+      // the MMAs that read this stage last time are done (bounded wait; a miss aborts)
+      bool ok = !*abortf;
+      if (ok && i >= S) ok = mbar_wait(&empty[s], (unsigned)((i / S - 1) & 1));
+      if (!ok) *abortf = 1;
+      if (ok) {
+        // A: rows 2 bl, 2 bl + 1 = Re, Im of c_j exp(i q_j . r_bl)
+        unsigned char* Ahi = stg;
+        unsigned char* Alo = stg + kABytes;
+        // c_j e^{i theta} in FP32: the phase reduced to [-pi, pi] in FP64, then sincosf; the
+        // products carry an absolute error ~2^-23 |c_j|, below the 2^-22 of the TF32 split
+        const float cr = (float)cj.x, ci = (float)cj.y;
+#pragma unroll
+        for (int u = 0; u < kBPW; ++u) {
+          const int bl = warp + u * kGenWarps;
+          if (bl < kBT) {
+            float wr = 0.0f, wi = 0.0f;
+            if (in && bl < nbl) {
+              const double th = qx * cx[u] + qy * cy[u] + qz * cz[u];
+              const double tr = fma(-rint(th * 0.15915494309189535), 6.283185307179586, th);
+              float sf, cf;
+              sincosf((float)tr, &sf, &cf);
+              wr = fmaf(cr, cf, -ci * sf);
+              wi = fmaf(cr, sf, ci * cf);
+            }
+            float h, l;
+            umma::tf32_split_f32(wr, h, l);
+            put(Ahi, 2 * bl, lane, h);
+            put(Alo, 2 * bl, lane, l);
+            umma::tf32_split_f32(wi, h, l);
+            put(Ahi, 2 * bl + 1, lane, h);
+            put(Alo, 2 * bl + 1, lane, l);
+          }
+        }
+        // B: row r = qx^a1 qy^a2 qz^a3 for the r-th multi-index (a1 outer, a3 inner), one
+        // multiplication per row; zero rows past L and for modes past the slice
+        unsigned char* Bhi = stg + 2 * kABytes;
+        unsigned char* Blo = Bhi + bB;
+        const int a1 = e0 & 255, a2 = (e0 >> 8) & 255, a3 = e0 >> 16;
+        double t1 = in ? 1.0 : 0.0;
+        for (int k = 0; k < a1; ++k) t1 *= qx;
+        double t12 = t1;
+        for (int k = 0; k < a2; ++k) t12 *= qy;
+        double m = t12;
+        for (int k = 0; k < a3; ++k) m *= qz;
+        int left1 = a.p - a1, left2 = left1 - a2, left3 = left2 - a3;  // steps left on each axis
+        const int rL = r1 < a.L ? r1 : a.L;
+        for (int r = r0; r < rL; ++r) {
+          float h, l;
+          umma::tf32_split_f32((float)m, h, l);
+          put(Bhi, r, lane, h);
+          put(Blo, r, lane, l);
+          if (left3 > 0) {
+            --left3;
+            m *= qz;
+          } else if (left2 > 0) {
+            left3 = --left2;
+            t12 *= qy;
+            m = t12;
+          } else {
+            left3 = left2 = --left1;
+            t1 *= qx;
+            t12 = t1;
+            m = t1;
+          }
+        }
+        for (int r = rL > r0 ? rL : r0; r < r1; ++r) {
+          put(Bhi, r, lane, 0.0f);
+          put(Blo, r, lane, 0.0f);
+        }
+      }
+      fence_proxy_async_smem();  // generic-proxy writes -> tensor-core reads
+      mbar_arrive(&full[s]);
+    }
+  } else {
+    // MMA warp: wait for each stage, issue its 3xTF32 products, release it on completion
+    const int N0 = Npad < 256 ? Npad : 256, N1 = Npad - N0;
+    const uint32_t id0 = umma::idesc_tf32(128, N0), id1 = umma::idesc_tf32(128, N1 > 0 ? N1 : 16);
+    for (int i = 0; i < nch; ++i) {
+      const int s = i % S;
+      const bool ok = !*abortf && mbar_wait(&full[s], (unsigned)((i / S) & 1));
+      if (!ok) {
+        *abortf = 1;
+        break;
+      }
+      umma::fence_after_sync();
+      if (lane == 0) {
+        const uint32_t sa = smem_u32(sm + (size_t)s * stB);
+        for (int kk = 0; kk < kKC / 8; ++kk)
+          for (int pr = 0; pr < 3; ++pr) {  // hi*hi, hi*lo, lo*hi
+            const uint64_t ad = umma::desc_kmajor_sw128(sa + (pr == 2 ? kABytes : 0u) + kk * 32u);
+            const uint32_t bo = sa + 2u * kABytes + (pr == 1 ? bB : 0u) + kk * 32u;
+            const uint32_t acc = (i | kk | pr) != 0 ? 1u : 0u;
+            umma::mma_tf32(tmem, ad, umma::desc_kmajor_sw128(bo), id0, acc);
+            if (N1 > 0) umma::mma_tf32(tmem + 256u, ad, umma::desc_kmajor_sw128(bo + 256u * 128u), id1, acc);
+          }
+        umma::commit(&empty[s]);
+      }
+      __syncwarp();
+    }
+    if (lane == 0) umma::commit(done);  // arrives once every MMA issued above has completed
+    __syncwarp();
+  }
+  // every thread: the accumulator is final (or the pipeline gave up)
+  const bool fin = mbar_wait(done, 0u);
+  const bool ok = __syncthreads_and(fin && !*abortf);
+  if (ok) {  // all 16 warps: warp w reads lanes 32 (w % 4), column blocks w / 4 + 4 t
+    umma::fence_after_sync();
+    const int q = warp & 3;  // a warp reads TMEM lanes 32 (warp % 4) ...
+    float* orow = a.out + (((long long)z * gridDim.y + bt) * 128 + q * 32 + lane) * (long long)Npad;
+    for (int cc = warp >> 2; cc < Npad / 32; cc += (kGenWarps + 1) / 4) {
+      uint32_t r[32];
+      umma::ld_32x32b_x32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(cc * 32), r);
+      umma::wait_ld(r);
+      float4* o = reinterpret_cast<float4*>(orow + cc * 32);
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        o[u] = make_float4(__uint_as_float(r[4 * u]), __uint_as_float(r[4 * u + 1]), __uint_as_float(r[4 * u + 2]),
+                           __uint_as_float(r[4 * u + 3]));
+    }
+  } else if (!ok && tid == 0 && fault) {
+    atomicOr(fault, 1u);
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    umma::fence_after_sync();
+    umma::tmem_dealloc(tmem, ncols);
+  }
+}
+
+// part[g][e] = sum of the partial moments e (of all tiles) over slice group g (FP64, fixed order)
+__global__ void k_taylor_tc_sum_slices(const float* __restrict__ out, long long nslices, long long per, int groups,
+                                       double* __restrict__ part) {
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (e >= per) return;
+  const int g = blockIdx.y;
+  const long long z0 = nslices * g / groups, z1 = nslices * (g + 1) / groups;
+  double acc = 0.0;
+  for (long long z = z0; z < z1; ++z) acc += (double)out[z * per + e];
+  part[(long long)g * per + e] = acc;
+}
+
+// gamma[b L + a] = coef[a] * (Re + i Im) of the group sums, groups in order
+__global__ void k_taylor_tc_finish(const double* __restrict__ part, int groups, long long per, int Npad, int L, int nB,
+                                   const double2* __restrict__ coef, double2* __restrict__ gamma) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)nB * L) return;
+  const int b = (int)(t / L), al = (int)(t % L);
+  const long long e = ((long long)(b / kBT) * 128 + 2 * (b % kBT)) * Npad + al;
+  double re = 0.0, im = 0.0;
+  for (int g = 0; g < groups; ++g) {
+    re += part[(long long)g * per + e];
+    im += part[(long long)g * per + e + Npad];
+  }
+  const double2 cf = coef[al];
+  gamma[t] = make_double2(cf.x * re - cf.y * im, cf.x * im + cf.y * re);
+}
+
+}  // namespace
+
+TaylorTcPlan taylor_tc_plan(long long NF, int nB, int L) {
+  TaylorTcPlan pl{};
+  pl.Npad = std::max(32, (L + 31) / 32 * 32);
+  pl.stages = tc_smem(pl.Npad, 2) <= 227 * 1024 ? 2 : 1;
+  pl.smem = tc_smem(pl.Npad, pl.stages);
+  pl.ntiles = (nB + kBT - 1) / kBT;
+  const long long sms = num_sms() > 0 ? num_sms() : 148;
+  const long long waves = std::max<long long>(1, (NF * pl.ntiles + sms * kKcMax - 1) / (sms * kKcMax));
+  const long long want = std::max<long long>(1, (waves * sms + pl.ntiles - 1) / pl.ntiles);
+  pl.Kc = std::max<long long>(kKC, ((NF + want - 1) / want + kKC - 1) / kKC * kKC);
+  pl.nslices = (NF + pl.Kc - 1) / pl.Kc;
+  const size_t per = (size_t)pl.ntiles * 128 * pl.Npad;
+  pl.groups = (int)std::min<long long>(pl.nslices, 32);
+  pl.out_floats = (size_t)pl.nslices * per + 2 * (size_t)pl.groups * per;  // FP32 slices + FP64 group sums
+  return pl;
+}
+
+int taylor_moments_tc(const TaylorTcPlan& pl, cudaStream_t s, const double2* c, const double* Q, long long NF,
+                      const double* centers, int nB, const int* alistPacked, int L, int p, const double2* coef,
+                      float* out, double2* gamma) {
+  if (L > kLmax || L > pl.Npad || p > kPmax || pl.Npad > 512 || pl.smem > 227 * 1024)
+    return fail(FAME_ERR_UNSUPPORTED, "tensor-core Taylor moments: order too high");
+  static int attr = [] {
+    return cudaFuncSetAttribute(k_taylor_moments_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) ==
+                   cudaSuccess
+               ? FAME_OK
+               : FAME_ERR_CUDA;
+  }();
+  if (attr != FAME_OK) return fail(attr, "tensor-core Taylor moments: shared-memory limit");
+  TcArgs a{Q, c, NF, centers, nB, alistPacked, L, p, pl.Npad, pl.stages, pl.Kc, out};
+  dim3 grid((unsigned)pl.nslices, (unsigned)pl.ntiles);
+  k_taylor_moments_tc<<<grid, kThreads, pl.smem, s>>>(a, fault_word());
+  ::fame::count_launch();
+  const long long per = (long long)pl.ntiles * 128 * pl.Npad;
+  double* part = reinterpret_cast<double*>(out + pl.nslices * per);
+  k_taylor_tc_sum_slices<<<dim3((unsigned)((per + 255) / 256), (unsigned)pl.groups), 256, 0, s>>>(out, pl.nslices, per,
+                                                                                                pl.groups, part);
+  k_taylor_tc_finish<<<(unsigned)(((long long)nB * L + 255) / 256), 256, 0, s>>>(part, pl.groups, per, pl.Npad, L, nB,
+                                                                                 coef, gamma);
+  ::fame::count_launch(2);
+  FAME_CUDA_TRY(cudaGetLastError());
+  return FAME_OK;
+}
+
+}  // namespace fame

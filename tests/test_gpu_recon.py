@@ -69,10 +69,12 @@ def test_taylor_multi_and_single(cuda_device):
     blocks = F.build_yee_block_partition(sz, 2)
     r1 = pts[0].cpu().numpy()
     ob = O.build_yee_block_partition(sz, 2)
-    for p in (6, 10):
+    for p in (0, 2, 3, 6, 10):  # L = 1, 10, 20 (fewer terms than staged modes), 84, 286
         ut = F.reconstruct_field_taylor_multi(c, Q, pts[0], p, blocks).cpu().numpy()
         uo = O.reconstruct_field_taylor_multi(c.cpu().numpy(), Q.cpu().numpy(), r1, p, ob)
         assert rel(ut, uo) < 1e-11, p
+        ut = F.reconstruct_field_taylor_multi(c, Q, pts[0], p, blocks, tensor_cores=True).cpu().numpy()
+        assert rel(ut, uo) < 2e-6, p
     us = F.reconstruct_field_taylor_single(c, Q, pts[0], 8).cpu().numpy()
     uso = O.reconstruct_field_taylor_single(c.cpu().numpy(), Q.cpu().numpy(), r1, 8)
     assert rel(us, uso) < 1e-11
@@ -128,10 +130,12 @@ def test_batched_bloch_path_matches_single_solves(cuda_device):
         np.testing.assert_allclose(lam[i], np.sort(1.0 / th), rtol=1e-10)
 
 
-@pytest.mark.parametrize("N,p,nb", [(2, 6, 2), (2, 10, 3), (3, 8, 2)])
+@pytest.mark.parametrize("N,p,nb", [(2, 6, 2), (2, 10, 3), (3, 8, 2), (2, 12, 2), (2, 0, 1), (4, 10, 5)])
 def test_taylor_3xtf32_tensor_cores_vs_fp64(cuda_device, N, p, nb):
-    """Split-FP32 (3xTF32) tensor-core block moments vs the FP64 form (same centers,
-    same evaluation): relative field error at FP32 level."""
+    """Split-FP32 (3xTF32) tensor-core block moments (operands generated on chip, FP32
+    TMEM accumulation over at most 512 modes, FP64 sum of the slices) vs the FP64 form
+    (same centers, same evaluation): relative field error below 4e-6 (the tensor cores
+    round the FP32 accumulation toward zero; random unit coefficients, up to 2.6e5 modes)."""
     F, S, sg, m = _sys(N, cuda_device)
     Q = F.build_projected_q_modes(sg)
     c = torch.as_tensor(O.start_vector(13, S.NF), device=cuda_device)
@@ -139,6 +143,6 @@ def test_taylor_3xtf32_tensor_cores_vs_fp64(cuda_device, N, p, nb):
     blocks = F.build_yee_block_partition(sz, nb)
     u64 = F.taylor_on_blocks(c, Q, pts[1], p, blocks).cpu().numpy()
     utc = F.taylor_on_blocks(c, Q, pts[1], p, blocks, tensor_cores=True).cpu().numpy()
-    assert rel(utc, u64) < 2e-6, rel(utc, u64)
+    assert rel(utc, u64) < 4e-6, rel(utc, u64)
     utc2 = F.taylor_on_blocks(c, Q, pts[1], p, blocks, tensor_cores=True).cpu().numpy()
     assert np.array_equal(utc, utc2)  # deterministic
