@@ -261,15 +261,15 @@ def run_fame(args):
             out = []
             for c in range(3):
                 xc = x10[c * NF:(c + 1) * NF]
-                if method == "direct":
-                    out.append(F.reconstruct_field_direct_grid(xc, sysq, axes[c]))
+                if method.startswith("direct"):
+                    out.append(F.reconstruct_field_direct_grid(xc, sysq, axes[c], tensor_cores=(method == "direct_tc")))
                 else:
                     out.append(F.taylor_on_blocks(xc, Qm, pts[c], 10, blocks, tensor_cores=(method == "taylor_tc")))
             return out
 
         times = {}
         fields = {}
-        for method in ("direct", "taylor", "taylor_tc"):
+        for method in ("direct", "direct_tc", "taylor", "taylor_tc"):
             recon(method)
             samples = []
             for _ in range(5):  # median of 5 (three components each)
@@ -287,6 +287,8 @@ def run_fame(args):
                "direct_pts_per_s": round(3 * M / times["direct"], 1),
                "taylor_p10_64c_pts_per_s": round(3 * M / times["taylor"], 1),
                "taylor_rel_err_vs_direct": err, "timing": "median of 5 repetitions, 3 components each",
+               "direct_3xtf32_pts_per_s": round(3 * M / times["direct_tc"], 1),
+               "direct_3xtf32_rel_err_vs_fp64": field_err(fields["direct_tc"], fields["direct"]),
                "taylor_3xtf32_pts_per_s": round(3 * M / times["taylor_tc"], 1),
                "taylor_3xtf32_rel_err_vs_fp64_taylor": field_err(fields["taylor_tc"], fields["taylor"]),
                "taylor_3xtf32_rel_err_vs_direct": field_err(fields["taylor_tc"], fields["direct"]),

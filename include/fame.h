@@ -242,6 +242,12 @@ FAME_API int fame_reconstruct_direct(fame_ctx* ctx, const void* coeff, const dou
 FAME_API int fame_reconstruct_direct_grid(fame_basis* b, const void* coeff, const double* xs, int nx,
                                           const double* ys, int ny, const double* zs, int nz,
                                           void* u);
+/* (No reference counterpart) the same factorised sum with the three complex GEMMs as
+ * split-FP32 (3xTF32) tcgen05 tensor-core products (phase tables and result FP64;
+ * relative field error ~1e-6 against fame_reconstruct_direct_grid). */
+FAME_API int fame_reconstruct_direct_grid_3xtf32(fame_basis* b, const void* coeff, const double* xs, int nx,
+                                                 const double* ys, int ny, const double* zs, int nz,
+                                                 void* u);
 /* exp2/taylor_on_blocks_exp3.m:8-79 (multi-center Taylor, order p <= 12).  Blocks in
  * CSR form: point indices blockIds[blockPtr[b] .. blockPtr[b+1]) (0-based, device);
  * fixedCenter: host 3-vector or NULL (then each block's bounding-box midpoint). */

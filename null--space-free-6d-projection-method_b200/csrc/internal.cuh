@@ -73,6 +73,11 @@ TaylorTcPlan taylor_tc_plan(long long NF, int nB, int L);
 int taylor_moments_tc(const TaylorTcPlan& plan, cudaStream_t s, const double2* c, const double* Q, long long NF,
                       const double* centers, int nB, const int* alistPacked, int L, int p, const double2* coef,
                       float* out, double2* gamma);
+// Batched complex GEMM C = A B (FP64 complex, element strides) as split-FP32
+// (3xTF32) tcgen05 products (zgemm_tc.cu).
+int zgemm_3xtf32(const double2* A, const double2* B, double2* C, int M, int N, int K, long long sam, long long sak,
+                 long long sbk, long long sbn, long long scm, long long scn, long long bA, long long bB, long long bC,
+                 int batch, cudaStream_t s);
 // Consecutive 256-byte aligned pieces of one workspace.
 struct Carve {
   size_t used = 0;

@@ -300,8 +300,8 @@ int fame_reconstruct_direct(fame_ctx* ctx, const void* coeff, const double* qMod
   return FAME_OK;
 }
 
-int fame_reconstruct_direct_grid(fame_basis* bs, const void* coeff, const double* xs, int nx,
-                                 const double* ys, int ny, const double* zs, int nz, void* u) {
+static int direct_grid_impl(fame_basis* bs, const void* coeff, const double* xs, int nx, const double* ys, int ny,
+                            const double* zs, int nz, void* u, bool tc) {
   if (!bs || !coeff || !xs || !ys || !zs || !u || nx <= 0 || ny <= 0 || nz <= 0)
     return fail(FAME_ERR_INVALID, "reconstruct_direct_grid arguments");
   const double* P = bs->P;  // column-major 6 x 3
@@ -341,16 +341,31 @@ int fame_reconstruct_direct_grid(fame_basis* bs, const void* coeff, const double
     ::fame::count_launch();
     // T1[x, (b,c)] = sum_a Tx[x, a] Cp[a, (b,c)]
     GemmArgs g1{Tx, Cp, T1, nx, (int)(n2 * n2), (int)n2, 1, nx, 1, n2, 1, nx, 0, 0, 0};
-    st = zgemm(g1, 1, s);
     // T2[x, y, c] = sum_b T1[x, b, c] Ty[y, b]   (batched over c)
     GemmArgs g2{T1, Ty, T2, nx, ny, (int)n2, 1, nx, ny, 1, 1, nx, (long long)nx * n2, 0, (long long)nx * ny};
-    if (st == FAME_OK) st = zgemm(g2, (int)n2, s);
     // u[(x,y), z] = sum_c T2[(x,y), c] Tz[z, c]
     GemmArgs g3{T2, Tz, (double2*)u, nx * ny, nz, (int)n2, 1, (long long)nx * ny, nz, 1, 1, (long long)nx * ny, 0, 0, 0};
-    if (st == FAME_OK) st = zgemm(g3, 1, s);
+    const GemmArgs* gs[3] = {&g1, &g2, &g3};
+    const int batches[3] = {1, (int)n2, 1};
+    for (int t = 0; t < 3 && st == FAME_OK; ++t) {
+      const GemmArgs& g = *gs[t];
+      st = tc ? zgemm_3xtf32(g.A, g.B, g.C, g.M, g.N, g.K, g.sam, g.sak, g.sbk, g.sbn, g.scm, g.scn, g.bA, g.bB, g.bC,
+                             batches[t], s)
+              : zgemm(g, batches[t], s);
+    }
     if (st == FAME_OK) st = cudaStreamSynchronize(s) == cudaSuccess ? FAME_OK : fail(FAME_ERR_CUDA, "sync");
   }
   return st;
+}
+
+int fame_reconstruct_direct_grid(fame_basis* bs, const void* coeff, const double* xs, int nx, const double* ys, int ny,
+                                 const double* zs, int nz, void* u) {
+  return direct_grid_impl(bs, coeff, xs, nx, ys, ny, zs, nz, u, false);
+}
+
+int fame_reconstruct_direct_grid_3xtf32(fame_basis* bs, const void* coeff, const double* xs, int nx, const double* ys,
+                                        int ny, const double* zs, int nz, void* u) {
+  return direct_grid_impl(bs, coeff, xs, nx, ys, ny, zs, nz, u, true);
 }
 
 }  // extern "C"

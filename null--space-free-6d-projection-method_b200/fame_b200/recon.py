@@ -129,14 +129,18 @@ def reconstruct_field_direct_blocked(coeff, qModes, rPoints, ctx=None):
     return u
 
 
-def reconstruct_field_direct_grid(coeff, sys: QSystem, axes):
-    """The direct sum on a tensor grid for an axis-block cut matrix (factorised GEMMs)."""
+def reconstruct_field_direct_grid(coeff, sys: QSystem, axes, tensor_cores=False):
+    """The direct sum on a tensor grid for an axis-block cut matrix (factorised GEMMs).
+
+    ``tensor_cores=True``: the three complex GEMMs as split-FP32 (3xTF32) tcgen05 products
+    (``fame_reconstruct_direct_grid_3xtf32``); FP64 CUDA-core GEMMs otherwise.
+    """
     xs, ys, zs = (a.contiguous() for a in axes)
     c = coeff.reshape(-1).contiguous()
     u = torch.empty(xs.numel() * ys.numel() * zs.numel(), dtype=torch.complex128, device=c.device)
     sys.ctx.bind()
-    call("fame_reconstruct_direct_grid", sys.h, _ptr(c), _ptr(xs), xs.numel(), _ptr(ys), ys.numel(),
-         _ptr(zs), zs.numel(), _ptr(u))
+    call("fame_reconstruct_direct_grid_3xtf32" if tensor_cores else "fame_reconstruct_direct_grid", sys.h, _ptr(c),
+         _ptr(xs), xs.numel(), _ptr(ys), ys.numel(), _ptr(zs), zs.numel(), _ptr(u))
     return u
 
 
