@@ -42,7 +42,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["fame", "reference"], default="fame")
     ap.add_argument("--N", type=int, default=N_BENCH)
-    ap.add_argument("--case", choices=["chain", "pcg", "solve"], default=None,
+    ap.add_argument("--case", choices=["chain", "pcg", "solve", "yee"], default=None,
                     help="run one piece of the step alone (for profiling), print its device time")
     ap.add_argument("--precision", choices=["fp32", "fp64", "mixed"], default="mixed")
     ap.add_argument("--reps", type=int, default=3)
@@ -455,6 +455,8 @@ def run_case(args):
     sysq = F.build_q_system(mass, cfg.P_GOLDEN, cfg.Q_BASELINE)
     v0 = F.start_vector(cfg.SEED, sysq.nr)
     prec = "fp64" if args.precision == "fp64" else "mixed"
+    if args.case == "yee":
+        return yee_sweep(F, cfg, sysq, v0, args)
     if args.case == "chain":
         x = torch.randn(NF, dtype=torch.complex128 if prec == "fp64" else torch.complex64, device=dev)
         body = lambda: F.apply_Mhat_C_scalar_compact(x, sysq)  # noqa: E731
@@ -479,6 +481,61 @@ def run_case(args):
     print(json.dumps({"case": args.case, "N": N, "precision": prec, "reps": args.reps,
                       "s_per_rep": e0.elapsed_time(e1) / 1e3 / args.reps,
                       "launches_per_rep": (F.kernel_launches() - l0) / args.reps}), flush=True)
+
+
+def yee_sweep(F, cfg, sysq, v0, args):
+    """Yee-field reconstruction of eigenmode 10 over the window sizes n = 40..200 (h =
+    0.0125), Taylor orders p = 6, 8, 10 and m^3 centers, m = 1..6: points/s (median of
+    ``--reps``, three components) and the field error against the FP64 direct sum."""
+    import numpy as np
+    import torch
+    S = cfg.SOLVE
+    op = F.make_explicit_krinv_compact(sysq, S["tolCG"], S["maxitCG"], precision="fp64")[0]
+    Y, theta = F.Lanczos(op, None, None, sysq.nr, S["nev"], S["tol"], S["maxRestart"], S["p"], v0)[:2]
+    th = theta.cpu().numpy() if torch.is_tensor(theta) else np.asarray(theta)
+    i10 = int(np.argsort(1.0 / th)[9])
+    X, _, _ = F.recover_original_eigenvectors(Y[:, i10].reshape(-1, 1).contiguous(), sysq, 1e-12, 3000)
+    NF = sysq.NF
+    xc = [X[c * NF:(c + 1) * NF, 0].contiguous() for c in range(3)]
+    Qm = F.build_projected_q_modes(sysq)
+
+    def timed(fn):
+        fn()
+        ts = []
+        for _ in range(max(1, args.reps)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return sorted(ts)[len(ts) // 2], out
+
+    def err(a, b):
+        return float(sum(torch.linalg.norm(x - y) ** 2 for x, y in zip(a, b)) ** 0.5 /
+                     sum(torch.linalg.norm(y) ** 2 for y in b) ** 0.5)
+
+    for n in (40, 80, 120, 160, 200):
+        pts, axes, sz = F.build_yee_points(n, 0.0125)
+        M3 = sum(int(p.shape[0]) for p in pts)
+        t64, ref = timed(lambda: [F.reconstruct_field_direct_grid(xc[c], sysq, axes[c]) for c in range(3)])
+        ttc, dtc = timed(lambda: [F.reconstruct_field_direct_grid(xc[c], sysq, axes[c], tensor_cores=True)
+                                  for c in range(3)])
+        print(json.dumps({"case": "yee", "n": n, "method": "direct", "pts_per_s_fp64": M3 / t64,
+                          "pts_per_s_3xtf32": M3 / ttc, "rel_err_3xtf32": err(dtc, ref)}), flush=True)
+        for p in (6, 8, 10):
+            for m in range(1, 7):
+                blocks = F.build_yee_block_partition(sz, m)
+                row = {"case": "yee", "n": n, "method": "taylor", "p": p, "m": m}
+                for tc in (False, True):
+                    t, u = timed(lambda: [F.taylor_on_blocks(xc[c], Qm, pts[c], p, blocks, tensor_cores=tc)
+                                          for c in range(3)])
+                    key = "3xtf32" if tc else "fp64"
+                    row["pts_per_s_" + key] = M3 / t
+                    row["rel_err_" + key] = err(u, ref)
+                print(json.dumps(row), flush=True)
+                del u
+        del pts, ref, dtc
+        torch.cuda.empty_cache()
 
 
 def run_reference(args):
