@@ -42,7 +42,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["fame", "reference"], default="fame")
     ap.add_argument("--N", type=int, default=N_BENCH)
-    ap.add_argument("--case", choices=["chain", "pcg", "solve", "yee"], default=None,
+    ap.add_argument("--case", choices=["chain", "pcg", "solve", "yee", "grad"], default=None,
                     help="run one piece of the step alone (for profiling), print its device time")
     ap.add_argument("--precision", choices=["fp32", "fp64", "mixed"], default="mixed")
     ap.add_argument("--reps", type=int, default=3)
@@ -446,6 +446,8 @@ def run_case(args):
     import fame_b200 as F
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
+    if args.case == "grad":
+        return grad_case(F, args)
     N = args.N
     NF = (2 * N) ** 6
     cfg = F.configs
@@ -481,6 +483,34 @@ def run_case(args):
     print(json.dumps({"case": args.case, "N": N, "precision": prec, "reps": args.reps,
                       "s_per_rep": e0.elapsed_time(e1) / 1e3 / args.reps,
                       "launches_per_rep": (F.kernel_launches() - l0) / args.reps}), flush=True)
+
+
+def grad_case(F, args):
+    """Hellmann-Feynman gradients of the 10 smallest eigenvalues with respect to the 7
+    material parameters theta = (delta = 12, a_1..a_6 ~ U[0.5, 1], seeded) at N = 6 (NF =
+    2,985,984): time of solve + eigenvector recovery + mass adjoint, and a central finite
+    difference (step 1e-6) of d lambda / d delta as the check."""
+    import numpy as np
+    import torch
+    N = 6 if args.N == N_BENCH else args.N
+    prec = "fp64" if args.precision == "fp64" else "mixed"
+    kw = dict(nev=10, tolCG=1e-12, tol=1e-10, precision=prec)
+    theta = np.concatenate([[12.0], F.configs.gradient_amplitudes()])
+    F.grad.eigenvalue_gradients(2, theta, **kw)  # warm-up (kernels, workspaces)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    lam, dlam = F.grad.eigenvalue_gradients(N, theta, **kw)
+    torch.cuda.synchronize()
+    t = time.perf_counter() - t0
+    h = 1e-6
+    tp, tm = theta.copy(), theta.copy()
+    tp[0] += h
+    tm[0] -= h
+    fd = (F.grad.eigenpairs(N, tp, **kw)[0] - F.grad.eigenpairs(N, tm, **kw)[0]) / (2 * h)
+    print(json.dumps({"case": "grad", "N": N, "NF": (2 * N) ** 6, "precision": prec, "modes": 10, "params": 7,
+                      "seconds_solve_recover_adjoint": t, "lambda": lam.tolist(),
+                      "dlambda_ddelta": dlam[:, 0].tolist(),
+                      "fd_rel_err_ddelta": float(np.max(np.abs(dlam[:, 0] - fd) / np.abs(fd)))}), flush=True)
 
 
 def yee_sweep(F, cfg, sysq, v0, args):

@@ -52,3 +52,22 @@ def test_krinv_and_eigs_vs_fixture(cuda_device, precision):
     lam = np.sort(1.0 / theta)
     assert info["converged"]
     assert np.max(np.abs(lam - de["n2_tracking"]) / de["n2_tracking"]) < 1e-10
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_reference_kat_n5_tracked_modes(cuda_device, precision):
+    """exp3/make_config_experiment4.m:38-52, exp3/solve_tracked_modes_exp4.m:37-42: the
+    reference's N=5 tracked modes 11 and 114 (material epsC = 4, alpha = 1.2, P = [I;
+    diag(sqrt 2, sqrt 3, sqrt 5)], q = (0.13, 0.21, 0.17)) from its k = 140, p = 188 scan
+    (tolLanczos = tolCG = 1e-10).  The reference checks 5e-7; its values carry 13 digits."""
+    import fame_b200 as F
+    N = 5
+    m = F.MassBackend(F.configs.material_smooth_exp(N, 4.0, 1.2, device=cuda_device), N)
+    s = F.build_q_system(m, F.configs.P_REFERENCE, F.configs.Q_TRACKING)
+    op, _ = F.make_explicit_krinv_compact(s, 1e-10, 3000, precision=precision)
+    v0 = F.start_vector(20260831, s.nr)
+    _, theta, _, info = F.Lanczos(op, None, None, s.nr, 140, 1e-10, 30, 188, v0)
+    assert info["converged"] and info["nconv"] == 140
+    lam = np.sort(1.0 / theta)[[10, 113]]
+    ref = np.array([1.200090550277e-02, 4.462939906027e-02])
+    assert np.max(np.abs(lam - ref) / ref) < 1e-10, lam
