@@ -321,14 +321,19 @@ def run_fame(args):
                                        tolCG=S["tolCG"])
         torch.cuda.synchronize()
         t_batch = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        for i in range(len(Ns)):
-            F.solve_batch([Ns[i]], [mats[i]], [qs[i]], cfg.P_GOLDEN, nev=S["nev"], tol=S["tol"], p=S["p"],
-                          tolCG=S["tolCG"])
-        torch.cuda.synchronize()
-        t_seq = time.perf_counter() - t0
+        def sequential(prec):
+            t0 = time.perf_counter()
+            for i in range(len(Ns)):
+                F.solve_batch([Ns[i]], [mats[i]], [qs[i]], cfg.P_GOLDEN, nev=S["nev"], tol=S["tol"], p=S["p"],
+                              tolCG=S["tolCG"], precision=prec)
+            torch.cuda.synchronize()
+            return time.perf_counter() - t0
+        t_seq = sequential("mixed")
+        t_seq64 = sequential("fp64")
         bloch = {"points": len(Ns), "N": Ns, "batched_s": round(t_batch, 4), "sequential_s": round(t_seq, 4),
                  "batch_speedup": round(t_seq / t_batch, 3),
+                 "fp64_sequential_s": round(t_seq64, 4),
+                 "mixed_batched_vs_fp64_sequential": round(t_seq64 / t_batch, 3),
                  "converged": all(i["converged"] for i in infos_b),
                  "gamma": "q = Gamma + %s (the null-space-free reduction is singular at Gamma)" % list(cfg.GAMMA_SHIFT),
                  "lambda_1": [float(v) for v in lam_b[:, 0]]}

@@ -22,10 +22,32 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 
+// Stream-ordered allocation for this host thread (StreamOrderedAlloc): device
+// memory then comes from the device's default memory pool on that stream, and a
+// free waits for that stream only instead of the whole device.
+static thread_local bool t_ordered = false;
+static thread_local cudaStream_t t_alloc_stream = nullptr;
+
+StreamOrderedAlloc::StreamOrderedAlloc(cudaStream_t s) : prev_on(t_ordered), prev(t_alloc_stream) {
+  t_ordered = true;
+  t_alloc_stream = s;
+}
+StreamOrderedAlloc::~StreamOrderedAlloc() {
+  t_ordered = prev_on;
+  t_alloc_stream = prev;
+}
+
 int dalloc(void** p, size_t bytes) {
   *p = nullptr;
   if (bytes == 0) return FAME_OK;
-  cudaError_t e = cudaMalloc(p, bytes);
+  cudaError_t e;
+  if (t_ordered) {
+    // usable on every stream once the (host-side) pool allocation is ordered
+    e = cudaMallocAsync(p, bytes, t_alloc_stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(t_alloc_stream);
+  } else {
+    e = cudaMalloc(p, bytes);
+  }
   if (e != cudaSuccess) {
     cudaGetLastError();
     *p = nullptr;
@@ -36,7 +58,14 @@ int dalloc(void** p, size_t bytes) {
 }
 
 void dfree(void* p) {
-  if (p) cudaFree(p);
+  if (!p) return;
+  if (t_ordered) {
+    // every use of the block was queued on this thread's stream: wait for it, then free in order
+    cudaStreamSynchronize(t_alloc_stream);
+    cudaFreeAsync(p, t_alloc_stream);
+  } else {
+    cudaFree(p);
+  }
 }
 
 // Per-device state shared by all handles: the device fault word that bounded

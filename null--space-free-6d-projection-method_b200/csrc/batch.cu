@@ -1,9 +1,13 @@
-// Batched solves of independent Bloch points of uneven size (BASELINE's
-// batched Bloch path; the reference solves them one after another,
+// Batched solves of independent Bloch points of uneven size (the batched Bloch
+// path; the reference solves them one after another,
 // exp4/run_exp4_medium.m:37-109).  Each instance gets its own context,
 // stream, mass, basis and K_r^{-1} handles and runs the restarted Lanczos in
 // its own host thread, so the GPU interleaves the kernels of small and large
-// instances; the per-iteration PCG bodies replay captured CUDA graphs.
+// instances; the per-iteration PCG bodies replay captured CUDA graphs.  Device
+// memory is allocated stream-ordered from the default pool on each instance's
+// stream and every handle is released only after all instances finished, so no
+// instance's free synchronises the device under the others.
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <thread>
@@ -27,30 +31,43 @@ struct BatchJob {
   fame_lanczos_info* info = nullptr;
   int status = FAME_OK;
   std::string error;
-};
-
-void run_job(BatchJob* j) {
   fame_ctx* ctx = nullptr;
   fame_mass* m = nullptr;
   fame_basis* b = nullptr;
   fame_krinv* k = nullptr;
   void* v0 = nullptr;
+};
+
+// Set up and solve one instance on its own stream; the handles stay alive until
+// every instance has finished (release_job), so that no instance frees device
+// memory while others run.
+void run_job(BatchJob* j) {
   int s = cudaSetDevice(j->device) == cudaSuccess ? FAME_OK : fail(FAME_ERR_CUDA, "cudaSetDevice");
-  if (s == FAME_OK) s = fame_ctx_create(j->device, &ctx);
-  if (s == FAME_OK) s = fame_mass_create(ctx, j->N, j->E, &m);
-  if (s == FAME_OK) s = fame_basis_create(ctx, j->N, j->P, j->q, &b);
-  if (s == FAME_OK) s = fame_krinv_create(b, m, &j->o, &k);
-  if (s == FAME_OK) s = dalloc(&v0, 2 * (size_t)b->NF * sizeof(double2));
-  if (s == FAME_OK) s = fame_start_vector(ctx, j->seed, 2 * b->NF, v0);
-  if (s == FAME_OK) s = fame_lanczos(k, j->nev, j->tol, j->maxiter, j->p, v0, j->theta, nullptr, j->info);
+  if (s == FAME_OK) s = fame_ctx_create(j->device, &j->ctx);
+  if (s == FAME_OK) {
+    StreamOrderedAlloc ordered(j->ctx->own);
+    s = fame_mass_create(j->ctx, j->N, j->E, &j->m);
+    if (s == FAME_OK) s = fame_basis_create(j->ctx, j->N, j->P, j->q, &j->b);
+    if (s == FAME_OK) s = fame_krinv_create(j->b, j->m, &j->o, &j->k);
+    if (s == FAME_OK) s = dalloc(&j->v0, 2 * (size_t)j->b->NF * sizeof(double2));
+    if (s == FAME_OK) s = fame_start_vector(j->ctx, j->seed, 2 * j->b->NF, j->v0);
+    if (s == FAME_OK) s = fame_lanczos(j->k, j->nev, j->tol, j->maxiter, j->p, j->v0, j->theta, nullptr, j->info);
+    cudaStreamSynchronize(j->ctx->stream);
+  }
   if (s != FAME_OK) j->error = fame_last_error();
   j->status = s;
-  if (ctx) cudaStreamSynchronize(ctx->stream);
-  dfree(v0);
-  fame_krinv_destroy(k);
-  fame_basis_destroy(b);
-  fame_mass_destroy(m);
-  fame_ctx_destroy(ctx);
+}
+
+void release_job(BatchJob* j) {
+  if (!j->ctx) return;
+  cudaSetDevice(j->device);
+  StreamOrderedAlloc ordered(j->ctx->own);  // the context's workspace came from the pool too
+  dfree(j->v0);
+  fame_krinv_destroy(j->k);
+  fame_basis_destroy(j->b);
+  fame_mass_destroy(j->m);
+  fame_ctx_destroy(j->ctx);
+  j->ctx = nullptr;
 }
 
 }  // namespace
@@ -79,10 +96,25 @@ extern "C" int fame_solve_batch(int device, int count, const int* Ns, const doub
     j.theta = theta + (size_t)nev * i;
     j.info = info ? info + i : nullptr;
   }
+  // pool memory stays cached between the instances' frees and allocations and across
+  // calls (mapping gigabytes anew costs more than the small solves themselves); it is
+  // the device's default pool, released by cudaMemPoolTrimTo or at process exit
+  cudaMemPool_t pool = nullptr;
+  if (cudaSetDevice(device) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    unsigned long long keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
+  // largest instances first: they start their long chains of launches earliest
+  std::vector<int> order(count);
+  for (int i = 0; i < count; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return Ns[a] > Ns[b]; });
   std::vector<std::thread> threads;
   threads.reserve(count);
-  for (int i = 0; i < count; ++i) threads.emplace_back(run_job, &jobs[i]);
+  for (int i : order) threads.emplace_back(run_job, &jobs[i]);
   for (auto& t : threads) t.join();
+  for (int i = 0; i < count; ++i) release_job(&jobs[i]);
+  cudaGetLastError();
   int first = FAME_OK;
   std::string msg;
   for (int i = 0; i < count; ++i) {

@@ -54,6 +54,17 @@ namespace fame {
 // device allocation helpers recorded for cleanup by the owner
 int dalloc(void** p, size_t bytes);
 void dfree(void* p);
+// While alive, dalloc/dfree of this host thread allocate from the device's default
+// memory pool in the order of stream s (all work on the blocks must be queued on s):
+// frees then no longer synchronise the whole device.  Used by concurrent solves.
+struct StreamOrderedAlloc {
+  explicit StreamOrderedAlloc(cudaStream_t s);
+  ~StreamOrderedAlloc();
+  StreamOrderedAlloc(const StreamOrderedAlloc&) = delete;
+  StreamOrderedAlloc& operator=(const StreamOrderedAlloc&) = delete;
+  bool prev_on;
+  cudaStream_t prev;
+};
 // copy a small device struct to host (synchronises the stream)
 int read_back(fame_ctx* ctx, const void* dsrc, void* hdst, size_t bytes);
 // FAME_ERR_CUDA (and clears the word) if a bounded device-side wait gave up on ctx's device
