@@ -283,6 +283,37 @@ typedef struct {
 /* n = 2NF; theta: host, k values (descending); Y: device n x k complex128 (may be NULL) */
 FAME_API int fame_lanczos(fame_krinv* k, int nev, double tol, int maxiter, int p, const void* v0,
                  double* theta, void* Y, fame_lanczos_info* info);
+
+/* ---- Method A: original shift-invert without the null-space-free basis ----
+ * exp1/build_experiment1_q_system_A_only.m, exp1/build_original_shift_preconditioner_A_only.m,
+ * exp1/make_A_eigs_top_preconditioned.m, exp1/run_method_A_fig1a.m.  The operator of the
+ * reference's eigs call, T x = (K - sigma M)^{-1} M x on 3NF vectors (components stacked,
+ * natural order), with K the per-mode symbol |q|^2 I - q q^T and the shifted system solved
+ * by preconditioned MINRES (preconditioner (K + tau I)^{-1}, exact per mode; the reference
+ * uses tau = sigma * mean(eps)); the basis handle supplies q (its V blocks are unused). */
+typedef struct fame_osi fame_osi;
+typedef struct fame_osi_stats {
+  long long topApplications;  /* shifted solves (one per T application) */
+  long long minresIterations; /* all MINRES iterations, correction cycles included */
+  long long cycles;           /* MINRES cycles (1 + residual corrections per solve) */
+  double maxTrueRelres;       /* largest final ||b - A x|| / ||b|| */
+  int failures;               /* solves that missed the tolerance and the plateau ceiling */
+  int plateauAccepts;         /* solves whose residual stalled between the tolerance and 1e-9 */
+} fame_osi_stats;
+FAME_API int fame_osi_create(fame_basis* b, fame_mass* m, double sigma, double tau, double tolMinres,
+                             int maxitMinres, fame_osi** out);
+FAME_API int fame_osi_destroy(fame_osi* A);
+/* y = T x for ncols 3NF columns. */
+FAME_API int fame_osi_apply(fame_osi* A, const void* x, void* y, int ncols);
+/* The nev eigenvalues of K x = lambda M x above the shift closest to it (the largest
+ * theta of T; lambda = sigma + 1/theta, ascending) by the restarted Lanczos on the
+ * Hermitian M^(1/2) (K - sigma M)^{-1} M^(1/2); X (3NF x nev, optional) M-normalised. */
+FAME_API int fame_osi_eigs(fame_osi* A, int nev, double tol, int maxiter, int p, const void* v0,
+                           double* lambda, void* X, fame_lanczos_info* info);
+FAME_API int fame_osi_stats_get(fame_osi* A, fame_osi_stats* out);
+/* exp1/build_experiment1_q_system_A_only.m:61-73 (applyK): y = K x, ncols 3NF columns. */
+FAME_API int fame_apply_K_original(fame_basis* b, const void* x, void* y, int ncols);
+
 /* Batched Bloch path: solve `count` independent instances (N[i], eps E[i] on the
  * (2N_i)^6 grid (device), Bloch vector q[3i..3i+2]) for their nev largest theta of
  * K_r^{-1}, concurrently on one device (one context, stream and host thread per

@@ -89,6 +89,18 @@ int taylor_moments_tc(const TaylorTcPlan& plan, cudaStream_t s, const double2* c
 int zgemm_3xtf32(const double2* A, const double2* B, double2* C, int M, int N, int K, long long sam, long long sak,
                  long long sbk, long long sbn, long long scm, long long scn, long long bA, long long bB, long long bC,
                  int batch, cudaStream_t s);
+// A Hermitian operator on n-vectors of complex128 for the restarted Lanczos
+// (lanczos.cu): y = A x on ctx's stream; *ws holds the reusable basis workspace.
+struct LanczosOperator {
+  fame_ctx* ctx;
+  long long n;
+  void** ws;
+  int (*apply)(void* self, const double2* x, double2* y);
+  void* self;
+};
+int lanczos_run(const LanczosOperator& op, int nev, double tol, int maxiter, int p, const void* v0, double* theta,
+                void* Y, fame_lanczos_info* info);
+void lanczos_ws_release(void** ws);
 // Consecutive 256-byte aligned pieces of one workspace.
 struct Carve {
   size_t used = 0;

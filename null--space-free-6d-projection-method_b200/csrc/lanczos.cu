@@ -356,34 +356,33 @@ struct LanczosWs {
   }
 };
 
-void lanczos_ws_free(fame_krinv* K) {
-  delete static_cast<LanczosWs*>(K->lanczos_ws);
-  K->lanczos_ws = nullptr;
+void lanczos_ws_release(void** ws) {
+  delete static_cast<LanczosWs*>(*ws);
+  *ws = nullptr;
 }
 
-}  // namespace fame
+void lanczos_ws_free(fame_krinv* K) { lanczos_ws_release(&K->lanczos_ws); }
 
-using namespace fame;
-
-extern "C" int fame_lanczos(fame_krinv* K, int nev, double tol, int maxiter, int p, const void* v0,
-                            double* theta, void* Y, fame_lanczos_info* info) {
-  if (!K || !v0 || !theta || nev < 1 || p < nev + 1 || p > kMaxCols || maxiter < 1)
-    return fail(FAME_ERR_INVALID, "fame_lanczos arguments (need 1 <= nev < p <= 256)");
-  fame_ctx* ctx = K->ctx;
+// Restarted Lanczos for the largest (algebraic) eigenvalues of a Hermitian operator.
+int lanczos_run(const LanczosOperator& op, int nev, double tol, int maxiter, int p, const void* v0, double* theta,
+                void* Y, fame_lanczos_info* info) {
+  if (!op.ctx || !op.apply || !op.ws || !v0 || !theta || nev < 1 || p < nev + 1 || p > kMaxCols || maxiter < 1)
+    return fail(FAME_ERR_INVALID, "Lanczos arguments (need 1 <= nev < p <= 256)");
+  fame_ctx* ctx = op.ctx;
   cudaStream_t s = ctx->stream;
-  const long long n = 2 * K->NF;
-  // the basis workspace (2 x n x p complex) is kept by the operator handle and reused
-  if (!K->lanczos_ws || static_cast<LanczosWs*>(K->lanczos_ws)->p != p) {
-    lanczos_ws_free(K);
+  const long long n = op.n;
+  // the basis workspace (2 x n x p complex) is kept by the operator's owner and reused
+  if (!*op.ws || static_cast<LanczosWs*>(*op.ws)->p != p || static_cast<LanczosWs*>(*op.ws)->n != n) {
+    lanczos_ws_release(op.ws);
     LanczosWs* w = new LanczosWs();
     const int st = w->alloc(ctx, n, p);
     if (st != FAME_OK) {
       delete w;
       return st;
     }
-    K->lanczos_ws = w;
+    *op.ws = w;
   }
-  LanczosWs& L = *static_cast<LanczosWs*>(K->lanczos_ws);
+  LanczosWs& L = *static_cast<LanczosWs*>(*op.ws);
   const double eps0 = 2.220446049250313e-16;
   // v = v0 / sqrt(v0' v0)   (exp2/Lanczos.m:17-18)
   k_nrm2<<<vec_blocks(n), 256, 0, s>>>((const double2*)v0, n, L.scal, L.partials, L.counter);
@@ -409,7 +408,7 @@ extern "C" int fame_lanczos(fame_krinv* K, int nev, double tol, int maxiter, int
       const int j = jj - 1;
       double2* qj = L.Q + (size_t)n * j;
       FAME_CUDA_TRY(cudaMemcpyAsync(qj, L.v, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
-      FAME_TRY(fame_krinv_apply(K, qj, L.w, 1));  // Aq = fncA(Q(:,jj))
+      FAME_TRY(op.apply(op.self, qj, L.w));  // Aq = fncA(Q(:,jj))
       // alpha = Re(Aq' Q(:,jj)) from the first pass; passes: 2, or 3 after a restart
       FAME_TRY(L.cgs_pass(jj, true));
       FAME_TRY(L.cgs_pass(jj, false));
@@ -508,4 +507,21 @@ extern "C" int fame_lanczos(fame_krinv* K, int nev, double tol, int maxiter, int
   }
   FAME_CUDA_TRY(cudaStreamSynchronize(s));
   return FAME_OK;
+}
+
+}  // namespace fame
+
+using namespace fame;
+
+namespace {
+int krinv_lanczos_apply(void* self, const double2* x, double2* y) {
+  return fame_krinv_apply(static_cast<fame_krinv*>(self), x, y, 1);
+}
+}  // namespace
+
+extern "C" int fame_lanczos(fame_krinv* K, int nev, double tol, int maxiter, int p, const void* v0,
+                            double* theta, void* Y, fame_lanczos_info* info) {
+  if (!K) return fail(FAME_ERR_INVALID, "fame_lanczos: K is NULL");
+  LanczosOperator op{K->ctx, 2 * K->NF, &K->lanczos_ws, krinv_lanczos_apply, K};
+  return lanczos_run(op, nev, tol, maxiter, p, v0, theta, Y, info);
 }

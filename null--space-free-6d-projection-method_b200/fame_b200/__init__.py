@@ -12,3 +12,4 @@ from .core import *  # noqa: F401,F403
 from . import configs  # noqa: F401
 from .recon import *  # noqa: F401,F403
 from . import grad  # noqa: F401
+from .method_a import *  # noqa: F401,F403

@@ -55,6 +55,12 @@ class fame_lanczos_info(C.Structure):
                 ("nconv", C.c_int), ("maxWantedResidual", C.c_double)]
 
 
+class fame_osi_stats(C.Structure):
+    _fields_ = [("topApplications", C.c_longlong), ("minresIterations", C.c_longlong),
+                ("cycles", C.c_longlong), ("maxTrueRelres", C.c_double), ("failures", C.c_int),
+                ("plateauAccepts", C.c_int)]
+
+
 P = C.c_void_p
 I = C.c_int
 LL = C.c_longlong
@@ -88,6 +94,12 @@ SIGNATURES = {
     "fame_krinv_stats_get": [P, C.POINTER(fame_krinv_stats)],
     "fame_krinv_stats_reset": [P],
     "fame_lanczos": [P, I, D, I, I, P, C.POINTER(D), P, C.POINTER(fame_lanczos_info)],
+    "fame_osi_create": [P, P, D, D, D, I, C.POINTER(P)],
+    "fame_osi_destroy": [P],
+    "fame_osi_apply": [P, P, P, I],
+    "fame_osi_eigs": [P, I, D, I, I, P, C.POINTER(D), P, C.POINTER(fame_lanczos_info)],
+    "fame_osi_stats_get": [P, C.POINTER(fame_osi_stats)],
+    "fame_apply_K_original": [P, P, P, I],
     "fame_start_vector": [P, C.c_ulonglong, LL, P],
     "fame_apply_Mhat_C_scalar_compact": [P, P, P, P, I],
     "fame_apply_Mhat_C_scalar_compact_noalloc": [P, P, P, P, I],

@@ -63,6 +63,8 @@ __all__ = [
     "reconstruct_component_taylor_batch", "solve_modes", "dense_reduced_operator",
     "mass_adjoint_quadratic", "set_fft_workers", "apply_cropped_A", "yee_material",
     "separable_conv3_same", "compute_lwrq", "compute_yee_lwrq_metrics",
+    "apply_K_original", "apply_shift_preconditioner", "minres", "osi_top_apply",
+    "dense_original_operators", "dense_original_gevp",
 ]
 
 
@@ -1033,3 +1035,111 @@ def compute_yee_lwrq_metrics(u1, u2, u3, lambda6D, P, n, h, material, save_spati
         spatial = dict(relativeDeviation_z0=np.abs(L["rho"][:, :, c] - lam3) / abs(lam3),
                        relativeDeviation_x0=np.abs(L["rho"][c, :, :] - lam3) / abs(lam3))
     return m, spatial
+
+
+# ---------------------------------------------------------------------------
+# Method A: original shift-invert on the full 3NF space (comparison path)
+# ---------------------------------------------------------------------------
+
+def apply_K_original(x, S):
+    """exp1/build_experiment1_q_system_A_only.m:61-73 (applyK): per mode
+    K_q = |q|^2 I - q q^*, components stacked [x1; x2; x3]."""
+    n = S.NF
+    x1, x2, x3 = x[:n], x[n:2 * n], x[2 * n:]
+    q1, q2, q3 = S.q1, S.q2, S.q3
+    y1 = (np.abs(q2) ** 2 + np.abs(q3) ** 2) * x1 - (q1 * np.conj(q2)) * x2 - (q1 * np.conj(q3)) * x3
+    y2 = -(q2 * np.conj(q1)) * x1 + (np.abs(q1) ** 2 + np.abs(q3) ** 2) * x2 - (q2 * np.conj(q3)) * x3
+    y3 = -(q3 * np.conj(q1)) * x1 - (q3 * np.conj(q2)) * x2 + (np.abs(q1) ** 2 + np.abs(q2) ** 2) * x3
+    return np.concatenate([y1, y2, y3])
+
+
+def apply_shift_preconditioner(x, S, tau):
+    """exp1/build_original_shift_preconditioner_A_only.m:24-54: (K + tau I)^{-1} x mode by mode,
+    1/(Q+tau) x + (1/tau - 1/(Q+tau)) q (q^* x) / Q."""
+    if not tau > 0:
+        raise ValueError("Preconditioner tau must be finite and positive.")
+    n = S.NF
+    q1, q2, q3 = S.q1, S.q2, S.q3
+    Q = np.abs(q1) ** 2 + np.abs(q2) ** 2 + np.abs(q3) ** 2
+    invTrans = 1.0 / (Q + tau)
+    corr = (1.0 / tau - invTrans) / Q
+    x1, x2, x3 = x[:n], x[n:2 * n], x[2 * n:]
+    cqx = corr * (np.conj(q1) * x1 + np.conj(q2) * x2 + np.conj(q3) * x3)
+    return np.concatenate([invTrans * x1 + q1 * cqx, invTrans * x2 + q2 * cqx, invTrans * x3 + q3 * cqx])
+
+
+def minres(A, b, tol, maxit, M=None):
+    """Preconditioned MINRES for Hermitian A and SPD preconditioner (the callable M
+    applies its inverse), x0 = 0, restating the Paige-Saunders recurrences that MATLAB's
+    minres implements (the reference's shifted solve, exp1/make_A_eigs_top_preconditioned.m:
+    285-286).  Stops when the recursive preconditioned residual norm phibar <= tol*beta1;
+    returns (x, iterations, true relative residual)."""
+    Minv = M if M is not None else (lambda r: r)
+    x = np.zeros_like(b)
+    r1 = b.copy()
+    y = Minv(r1)
+    beta1 = math.sqrt(max(np.real(np.vdot(r1, y)), 0.0))
+    if beta1 == 0.0:
+        return x, 0, 0.0
+    oldb, beta, dbar, epsln, phibar, cs, sn = 0.0, beta1, 0.0, 0.0, beta1, -1.0, 0.0
+    w = np.zeros_like(b)
+    w2 = np.zeros_like(b)
+    r2 = r1.copy()
+    it = 0
+    for it in range(1, maxit + 1):
+        v = y / beta
+        y = A(v)
+        if it >= 2:
+            y = y - (beta / oldb) * r1
+        alfa = np.real(np.vdot(v, y))
+        y = y - (alfa / beta) * r2
+        r1, r2 = r2, y
+        y = Minv(r2)
+        oldb, beta = beta, math.sqrt(max(np.real(np.vdot(r2, y)), 0.0))
+        oldeps = epsln
+        delta = cs * dbar + sn * alfa
+        gbar = sn * dbar - cs * alfa
+        epsln = sn * beta
+        dbar = -cs * beta
+        gamma = max(math.hypot(gbar, beta), 1e-300)
+        cs, sn = gbar / gamma, beta / gamma
+        phi = cs * phibar
+        phibar = sn * phibar
+        w1, w2 = w2, w
+        w = (v - oldeps * w1 - delta * w2) / gamma
+        x = x + phi * w
+        if phibar <= tol * beta1 or beta == 0.0:
+            break
+    relres = np.linalg.norm(b - A(x)) / np.linalg.norm(b)
+    return x, it, relres
+
+
+def osi_top_apply(x, S, sigma, tau, tol=1e-12, maxit=4000):
+    """exp1/make_A_eigs_top_preconditioned.m:61-113: T x = (K - sigma M)^{-1} M x by
+    preconditioned MINRES with the spectral preconditioner (K + tau I)^{-1}."""
+    rhs = S.mass.full(x)
+    A = lambda u: apply_K_original(u, S) - sigma * S.mass.full(u)  # noqa: E731
+    return minres(A, rhs, tol, maxit, lambda r: apply_shift_preconditioner(r, S, tau))
+
+
+def dense_original_operators(S):
+    """Dense K (block 3x3 per mode) and M3 = blkdiag(M, M, M) of the original GEVP
+    K x = lambda M x (small N only)."""
+    n = S.NF
+    I3n = np.eye(3 * n, dtype=np.complex128)
+    K = np.stack([apply_K_original(I3n[:, j], S) for j in range(3 * n)], axis=1)
+    Ms = np.stack([S.mass.scalar(np.eye(n, dtype=np.complex128)[:, j]) for j in range(n)], axis=1)
+    M3 = np.zeros((3 * n, 3 * n), dtype=np.complex128)
+    for c in range(3):
+        M3[c * n:(c + 1) * n, c * n:(c + 1) * n] = Ms
+    return K, M3
+
+
+def dense_original_gevp(S):
+    """All eigenvalues (ascending) of K x = lambda M x: NF zeros (gradient fields) and the
+    2NF positive eigenvalues that the null-space-free methods compute."""
+    K, M3 = dense_original_operators(S)
+    Lc = np.linalg.cholesky((M3 + M3.conj().T) / 2)
+    Li = np.linalg.inv(Lc)
+    H = Li @ ((K + K.conj().T) / 2) @ Li.conj().T
+    return np.sort(np.linalg.eigvalsh((H + H.conj().T) / 2))

@@ -201,3 +201,36 @@ def test_lwrq_metrics_consistency():
     assert met["deltaPart"] < 1e-14 and met["deltaLWRQIdentity"] < 1e-13
     assert met["croppedMass"] > 0 and 0 <= met["eta3D"] <= met["etaUsing6DLambda"] + 1e-15
     assert sp["relativeDeviation_z0"].shape == (2 * n + 1, 2 * n + 1)
+
+
+def test_method_a_spectrum_equals_null_space_free_n1():
+    """Method A (exp1/build_experiment1_q_system_A_only.m) and methods B/C share the
+    positive spectrum: the dense original GEVP K x = lambda M x has NF zero eigenvalues
+    (gradient fields) and 2NF positive ones equal to those of K_r = V^* M^-1 V
+    (exp1/check_fig1bc_results.m:23-25 checks 1e-7 across methods)."""
+    N = 1
+    S = O.build_q_system(N, P_REF, (0.13, 0.21, 0.17), O.material_smooth_exp(N))
+    ev = O.dense_original_gevp(S)
+    n = S.NF
+    assert np.sum(np.abs(ev) < 1e-10) == n and np.sum(ev > 1e-10) == 2 * n
+    kr = np.sort(np.linalg.eigvalsh(O.dense_reduced_operator(S)))
+    assert np.max(np.abs(ev[ev > 1e-10] - kr) / kr) < 1e-11
+
+
+def test_method_a_minres_top_vs_dense_n1():
+    """T x = (K - sigma M)^{-1} M x by the restated preconditioned MINRES
+    (exp1/make_A_eigs_top_preconditioned.m:61-113, tau = sigma mean(eps)) vs a dense solve."""
+    N = 1
+    E = O.material_smooth_exp(N)
+    S = O.build_q_system(N, P_REF, (0.13, 0.21, 0.17), E)
+    sigma = 1e-4
+    x = O.start_vector(3, 3 * S.NF)
+    y, it, relres = O.osi_top_apply(x, S, sigma, sigma * E.mean(), tol=1e-12)
+    K, M3 = O.dense_original_operators(S)
+    yd = np.linalg.solve(K - sigma * M3, M3 @ x)
+    assert relres < 1e-11 and it < 200
+    assert _rel(y, yd) < 1e-10
+    # the preconditioner is the exact inverse of K + tau I
+    tau = 0.37
+    z = O.apply_shift_preconditioner(x, S, tau)
+    assert _rel((K + tau * np.eye(3 * S.NF)) @ z, x) < 1e-13
