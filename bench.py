@@ -42,7 +42,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["fame", "reference"], default="fame")
     ap.add_argument("--N", type=int, default=N_BENCH)
-    ap.add_argument("--case", choices=["chain", "pcg", "solve", "yee", "grad"], default=None,
+    ap.add_argument("--case", choices=["chain", "pcg", "solve", "yee", "grad", "osi"], default=None,
                     help="run one piece of the step alone (for profiling), print its device time")
     ap.add_argument("--precision", choices=["fp32", "fp64", "mixed"], default="mixed")
     ap.add_argument("--reps", type=int, default=3)
@@ -453,6 +453,8 @@ def run_case(args):
     torch.cuda.set_device(dev)
     if args.case == "grad":
         return grad_case(F, args)
+    if args.case == "osi":
+        return osi_case(F, args)
     N = args.N
     NF = (2 * N) ** 6
     cfg = F.configs
@@ -516,6 +518,50 @@ def grad_case(F, args):
                       "seconds_solve_recover_adjoint": t, "lambda": lam.tolist(),
                       "dlambda_ddelta": dlam[:, 0].tolist(),
                       "fd_rel_err_ddelta": float(np.max(np.abs(dlam[:, 0] - fd) / np.abs(fd)))}), flush=True)
+
+
+def osi_case(F, args):
+    """Method A (the original shift-invert, exp1/run_method_A_fig1a.m) against method C on
+    the same Bloch point: reference material (epsC = 4, alpha = 1.2), P = [I; diag(sqrt 2,
+    sqrt 3, sqrt 5)], q = (0.13, 0.21, 0.17), 10 eigenvalues to 1e-10, sigma = 1e-4,
+    MINRES and CG tolerance 1e-10; N = 3 and 5 (or --N)."""
+    import numpy as np
+    import torch
+    cfg = F.configs
+    dev = torch.device("cuda", 0)
+    for N in ([3, 5] if args.N == N_BENCH else [args.N]):
+        E = cfg.material_smooth_exp(N, 4.0, 1.2, device=dev)
+        eMean, eMax = float(E.mean()), float(E.max())
+        m = F.MassBackend(E, N)
+        s = F.build_q_system(m, cfg.P_REFERENCE, cfg.Q_TRACKING)
+        F.eigs_method_A(s, nev=10, sigma=1e-4, epsMean=eMean, epsMax=eMax, tol=1e-10, p=40)  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        lamA, _, infoA, stA = F.eigs_method_A(s, nev=10, sigma=1e-4, epsMean=eMean, epsMax=eMax, tol=1e-10, p=40)
+        torch.cuda.synchronize()
+        tA = time.perf_counter() - t0
+        out = {}
+        for prec in ("fp64", "mixed"):
+            op = F.make_explicit_krinv_compact(s, 1e-10, 3000, precision=prec)[0]
+            v0 = F.start_vector(cfg.SEED, s.nr)
+            F.Lanczos(op, None, None, s.nr, 10, 1e-10, 30, 40, v0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            _, th, _, infoC = F.Lanczos(op, None, None, s.nr, 10, 1e-10, 30, 40, v0)
+            torch.cuda.synchronize()
+            out[prec] = (time.perf_counter() - t0, np.sort(1.0 / th), infoC)
+        lamC = out["fp64"][1]
+        print(json.dumps({"case": "osi", "N": N, "NF": (2 * N) ** 6, "method_A_s": round(tA, 4),
+                          "method_A_lanczos_steps": infoA["steps"], "method_A_converged": infoA["converged"],
+                          "method_A_minres_iterations": stA["totalMINRESIterations"],
+                          "method_A_shifted_solves": stA["topVectorApplications"],
+                          "method_A_plateau_accepts": stA["totalPlateauAccepts"],
+                          "method_A_max_true_relres": stA["maxTrueRelres"],
+                          "method_C_fp64_s": round(out["fp64"][0], 4), "method_C_mixed_s": round(out["mixed"][0], 4),
+                          "method_C_lanczos_steps": out["fp64"][2]["steps"],
+                          "speedup_C_mixed_over_A": round(tA / out["mixed"][0], 2),
+                          "lambda_rel_diff_A_vs_C": float(np.max(np.abs(lamA - lamC) / lamC)),
+                          "lambda": lamC.tolist()}), flush=True)
 
 
 def yee_sweep(F, cfg, sysq, v0, args):

@@ -82,20 +82,47 @@ __device__ __forceinline__ void apply_Pinv(const ModeQ& m, double tau, const dou
     y[c] = make_double2(it * x[c].x + qc[c] * corr * qx.x, it * x[c].y + qc[c] * corr * qx.y);
 }
 
+// The solution is accumulated in two parts per mode, x = xp + qhat psi with qhat = q/|q|:
+// its gradient-field part psi (about 1/sigma times larger than the rest) and the
+// transverse part xp, so that K acts on xp alone and the transverse digits are not
+// lost to the large gradient component sharing the same entries.
+//
 // pending w/x update of the last MINRES iteration for mode i (uses v of that iteration):
-// w1 <- w2, w2 <- w, w <- (v - oldeps w1 - delta w2) / gamma, x += phi w
-__device__ __forceinline__ void pending_update(const OsiState* st, long long NF, long long i, const double2* v,
-                                               double2* x, double2* w, double2* w1, double2* w2) {
+// w1 <- w2, w2 <- w, w <- (v - oldeps w1 - delta w2) / gamma, x += phi w (split)
+__device__ __forceinline__ void pending_update(const OsiState* st, long long NF, long long i, const ModeQ& m,
+                                               const double2* v, double2* xp, double2* psi, double2* w, double2* w1,
+                                               double2* w2) {
   const double g = 1.0 / st->p_gamma, oe = st->p_oldeps, de = st->p_delta, ph = st->p_phi;
+  const double rq = rsqrt(m.Q), qh[3] = {m.q1 * rq, m.q2 * rq, m.q3 * rq};
+  double2 wn[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     const long long k = c * NF + i;
     const double2 b = w2[k], wc = w[k], vc = v[k];
-    const double2 wn = make_double2((vc.x - oe * b.x - de * wc.x) * g, (vc.y - oe * b.y - de * wc.y) * g);
+    wn[c] = make_double2((vc.x - oe * b.x - de * wc.x) * g, (vc.y - oe * b.y - de * wc.y) * g);
     w1[k] = b;
     w2[k] = wc;
-    w[k] = wn;
-    x[k] = make_double2(x[k].x + ph * wn.x, x[k].y + ph * wn.y);
+    w[k] = wn[c];
+  }
+  const double2 sw = make_double2(qh[0] * wn[0].x + qh[1] * wn[1].x + qh[2] * wn[2].x,
+                                  qh[0] * wn[0].y + qh[1] * wn[1].y + qh[2] * wn[2].y);
+  psi[i] = make_double2(psi[i].x + ph * sw.x, psi[i].y + ph * sw.y);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const long long k = c * NF + i;
+    xp[k] = make_double2(xp[k].x + ph * (wn[c].x - qh[c] * sw.x), xp[k].y + ph * (wn[c].y - qh[c] * sw.y));
+  }
+}
+
+// x = xp + qhat psi for mode i (three components)
+__device__ __forceinline__ void assemble_x(const ModeQ& m, long long NF, long long i, const double2* xp,
+                                           const double2* psi, double2* out) {
+  const double rq = rsqrt(m.Q), qh[3] = {m.q1 * rq, m.q2 * rq, m.q3 * rq};
+  const double2 p = psi[i];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double2 a = xp[c * NF + i];
+    out[c] = make_double2(a.x + qh[c] * p.x, a.y + qh[c] * p.y);
   }
 }
 
@@ -103,11 +130,13 @@ __device__ __forceinline__ void pending_update(const OsiState* st, long long NF,
 struct ProOsi {
   static constexpr bool natural = true;
   const OsiState* st;
+  const double* q[3];
+  const double* Qq;
   const double2* y;
-  double2 *v, *x, *w, *w1, *w2;
+  double2 *v, *xp, *psi, *w, *w1, *w2;
   long long NF;
   __device__ __forceinline__ void load(long long, long long i, double2* out) const {
-    if (st->pend) pending_update(st, NF, i, v, x, w, w1, w2);
+    if (st->pend) pending_update(st, NF, i, mode_q(q, Qq, i), v, xp, psi, w, w1, w2);
     const double ib = 1.0 / st->beta;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -156,14 +185,29 @@ struct EpiOsi {
   }
 };
 
-// Epilogue of the residual check: r1 = b - (K x - sigma M x), ||r1||^2 and ||b||^2.
+// Prologue of the residual check: x = xp + qhat psi, also stored as the solution.
+struct ProOsiX {
+  static constexpr bool natural = true;
+  const double* q[3];
+  const double* Qq;
+  const double2 *xp, *psi;
+  double2* x;
+  long long NF;
+  __device__ __forceinline__ void load(long long, long long i, double2* out) const {
+    assemble_x(mode_q(q, Qq, i), NF, i, xp, psi, out);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) x[c * NF + i] = out[c];
+  }
+};
+
+// Epilogue of the residual check: r1 = b - (K xp - sigma M x), ||r1||^2 and ||b||^2.
 struct EpiOsiResid {
   using Acc = double;
   static constexpr int K = 2;
   static constexpr bool natural = true;
   const double* q[3];
   const double* Qq;
-  const double2* x;
+  const double2* xp;
   const double2* b;
   double2* r1;
   double sigma;
@@ -175,8 +219,8 @@ struct EpiOsiResid {
     const ModeQ m = mode_q(q, Qq, i);
     double2 xc[3], kx[3];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) xc[c] = x[c * NF + i];
-    apply_K(m, xc, kx);
+    for (int c = 0; c < 3; ++c) xc[c] = xp[c * NF + i];
+    apply_K(m, xc, kx);  // K (qhat psi) = 0
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const long long k = c * NF + i;
@@ -295,11 +339,12 @@ __global__ void k_osi_update(const double* const* q, const double* Qq, double ta
 }
 
 // the last pending w/x update once MINRES stopped; the last block clears the flag
-__global__ void k_osi_finish(long long NF, const double2* v, double2* x, double2* w, double2* w1, double2* w2,
-                             OsiState* st, unsigned* counter) {
+__global__ void k_osi_finish(const double* const* q, const double* Qq, long long NF, const double2* v, double2* xp,
+                             double2* psi, double2* w, double2* w1, double2* w2, OsiState* st, unsigned* counter) {
   if (!*((volatile const int*)&st->pend)) return;
+  const double* qq[3] = {q[0], q[1], q[2]};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < NF; i += (long long)gridDim.x * blockDim.x)
-    pending_update(st, NF, i, v, x, w, w1, w2);
+    pending_update(st, NF, i, mode_q(qq, Qq, i), v, xp, psi, w, w1, w2);
   __shared__ bool last;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -340,7 +385,7 @@ struct fame_osi {
   double sigma = 0, tau = 0, tol = 1e-10, plateau = 1e-9;
   int maxit = 4000, maxCycles = 8;
   double *EtSqrt = nullptr, *EtInvSqrt = nullptr;
-  double2 *x = nullptr, *r1 = nullptr, *r2 = nullptr, *y = nullptr, *v = nullptr, *w = nullptr, *w1 = nullptr,
+  double2 *x = nullptr, *xp = nullptr, *psi = nullptr, *r1 = nullptr, *r2 = nullptr, *y = nullptr, *v = nullptr, *w = nullptr, *w1 = nullptr,
           *w2 = nullptr, *Av = nullptr, *rhs = nullptr, *work = nullptr;
   OsiState* st = nullptr;
   double* partials = nullptr;
@@ -361,20 +406,20 @@ int osi_solve(fame_osi* A) {
   const size_t vb = 3 * NF * sizeof(double2);
   const int nb = osi_blocks(NF);
   const double* q[3] = {A->b->q[0], A->b->q[1], A->b->q[2]};
-  FAME_CUDA_TRY(cudaMemsetAsync(A->x, 0, vb, s));
+  FAME_CUDA_TRY(cudaMemsetAsync(A->xp, 0, vb, s));
+  FAME_CUDA_TRY(cudaMemsetAsync(A->psi, 0, NF * sizeof(double2), s));
   FAME_CUDA_TRY(cudaMemcpyAsync(A->r1, A->rhs, vb, cudaMemcpyDeviceToDevice, s));
   double rtol = A->tol, relres = 1.0, prev = 1e300;
   long long iters = 0;
   int cycles = 0, converged = 0;
-  ProCols<double, 3> pc;
-  for (int c = 0; c < 3; ++c) pc.x[c] = A->x + c * NF;
-  EpiOsiResid er{{q[0], q[1], q[2]}, A->b->Qq, A->x, A->rhs, A->r1, A->sigma, NF, A->st, A->partials, A->counter};
+  ProOsiX pc{{q[0], q[1], q[2]}, A->b->Qq, A->xp, A->psi, A->x, NF};
+  EpiOsiResid er{{q[0], q[1], q[2]}, A->b->Qq, A->xp, A->rhs, A->r1, A->sigma, NF, A->st, A->partials, A->counter};
   for (int cyc = 0; cyc < A->maxCycles; ++cyc) {
     ++cycles;
     k_osi_init<<<nb, 256, 0, s>>>(A->qdev, A->b->Qq, A->tau, NF, A->r1, A->r2, A->y, A->w, A->w1, A->w2, rtol,
                                   A->maxit, A->st, A->partials, A->counter);
     ::fame::count_launch();
-    ProOsi pro{A->st, A->y, A->v, A->x, A->w, A->w1, A->w2, NF};
+    ProOsi pro{A->st, {q[0], q[1], q[2]}, A->b->Qq, A->y, A->v, A->xp, A->psi, A->w, A->w1, A->w2, NF};
     EpiOsi epi{{q[0], q[1], q[2]}, A->b->Qq, A->v, A->r1, A->Av, A->sigma, NF, A->st, A->partials, A->counter};
     int chunk = A->chunk, done = 0;
     OsiState h{};
@@ -391,9 +436,10 @@ int osi_solve(fame_osi* A) {
     }
     iters += h.iter;
     A->chunk = std::max(4, std::min(64, h.iter / 2));
-    k_osi_finish<<<nb, 256, 0, s>>>(NF, A->v, A->x, A->w, A->w1, A->w2, A->st, A->counter);
+    k_osi_finish<<<nb, 256, 0, s>>>(A->qdev, A->b->Qq, NF, A->v, A->xp, A->psi, A->w, A->w1, A->w2, A->st,
+                                    A->counter);
     ::fame::count_launch();
-    // true residual r1 = b - A x
+    // x = xp + qhat psi and the true residual r1 = b - A x
     FAME_TRY((run_chain<double, 3>(A->n, pc, er, A->work, A->m->Et64, NF, s)));
     FAME_CUDA_TRY(cudaGetLastError());
     FAME_TRY(read_back(A->ctx, A->st, &h, sizeof(h)));
@@ -452,7 +498,7 @@ void osi_free(fame_osi* A) {
   if (A->ctx) cudaStreamSynchronize(A->ctx->stream);
   lanczos_ws_release(&A->lanczos_ws);
   dfree(A->EtSqrt); dfree(A->EtInvSqrt);
-  dfree(A->x); dfree(A->r1); dfree(A->r2); dfree(A->y); dfree(A->v); dfree(A->w); dfree(A->w1); dfree(A->w2);
+  dfree(A->x); dfree(A->xp); dfree(A->psi); dfree(A->r1); dfree(A->r2); dfree(A->y); dfree(A->v); dfree(A->w); dfree(A->w1); dfree(A->w2);
   dfree(A->Av); dfree(A->rhs); dfree(A->work); dfree(A->st); dfree(A->partials); dfree(A->counter);
   dfree(A->qdev);
   delete A;
@@ -482,9 +528,10 @@ int fame_osi_create(fame_basis* b, fame_mass* m, double sigma, double tau, doubl
   const size_t vb = 3 * NF * sizeof(double2);
   int s = dalloc((void**)&A->EtSqrt, NF * sizeof(double));
   if (s == FAME_OK) s = dalloc((void**)&A->EtInvSqrt, NF * sizeof(double));
-  double2** vecs[] = {&A->x, &A->r1, &A->r2, &A->y, &A->v, &A->w, &A->w1, &A->w2, &A->Av, &A->rhs, &A->work};
+  double2** vecs[] = {&A->x, &A->xp, &A->r1, &A->r2, &A->y, &A->v, &A->w, &A->w1, &A->w2, &A->Av, &A->rhs, &A->work};
   for (double2** p : vecs)
     if (s == FAME_OK) s = dalloc((void**)p, vb);
+  if (s == FAME_OK) s = dalloc((void**)&A->psi, NF * sizeof(double2));
   if (s == FAME_OK) s = dalloc((void**)&A->st, sizeof(OsiState));
   // reduction partials: the element-wise kernels and pass C of the chains (one per CTA, 2 values)
   const long long red = std::max<long long>(kOsiBlocksMax, passC_blocks(A->n)) + 16;
