@@ -286,7 +286,6 @@ struct LanczosWs {
     nblk = (int)((n + kGemvThreads * kGemvRows - 1) / (kGemvThreads * kGemvRows));
     const int M = p + 1;
     FAME_TRY(dalloc((void**)&Q, (size_t)n * p * sizeof(double2)));
-    FAME_TRY(dalloc((void**)&Q2, (size_t)n * p * sizeof(double2)));
     FAME_TRY(dalloc((void**)&w, n * sizeof(double2)));
     FAME_TRY(dalloc((void**)&v, n * sizeof(double2)));
     FAME_TRY(dalloc((void**)&coef, kMaxCols * sizeof(double2)));
@@ -306,6 +305,12 @@ struct LanczosWs {
       return fail(FAME_ERR_OOM, "pinned host buffer for Lanczos");
     }
     FAME_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned), ctx->stream));
+    return FAME_OK;
+  }
+  // the second basis, target of the thick-restart GEMM: allocated at the first restart
+  // (a solve that converges within its first p steps never needs it)
+  int ensure_q2() {
+    if (!Q2) FAME_TRY(dalloc((void**)&Q2, (size_t)n * p * sizeof(double2)));
     return FAME_OK;
   }
   int sync_read(const void* d, void* h, size_t bytes) {
@@ -482,6 +487,7 @@ int lanczos_run(const LanczosOperator& op, int nev, double tol, int maxiter, int
       for (int i = 0; i < m; ++i) Uk[i + (size_t)m * cc] = Us[i + (size_t)m * ind[cc]];
       c[cc] = beta * Us[(m - 1) + (size_t)m * ind[cc]];
     }
+    FAME_TRY(L.ensure_q2());
     FAME_TRY(L.combine(m, Uk, k, L.Q2, n));  // Q(:,1:k) = Q*Ukeep
     std::swap(L.Q, L.Q2);
     d.resize(k);
