@@ -68,6 +68,11 @@ FAME_API const char* fame_last_error(void);
 FAME_API int fame_version(void);
 /* Kernels launched by this library since load (instrumentation for benchmarks). */
 FAME_API long long fame_kernel_launches(void);
+/* (No reference counterpart) the library takes its device memory from the device's
+ * default memory pool and keeps freed blocks cached for its next handles (a free still
+ * waits for the device, as cudaFree does); this returns the cached memory of a device
+ * to the driver. */
+FAME_API int fame_device_trim_memory(int device);
 
 /* ---- context (replaces gpu_initialize / wait_for_gpu: exp1/wait_for_gpu.m:5-11) ---- */
 FAME_API int fame_ctx_create(int device, fame_ctx** out);

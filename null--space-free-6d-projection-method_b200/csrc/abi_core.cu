@@ -37,6 +37,46 @@ StreamOrderedAlloc::~StreamOrderedAlloc() {
   t_alloc_stream = prev;
 }
 
+// Per-device state shared by all handles: the device fault word that bounded
+// in-kernel waits set when they give up, the SM count, and the stream on which
+// the library's device allocations are ordered.
+constexpr int kMaxDevices = 64;
+static std::atomic<unsigned*> g_fault[kMaxDevices];
+static std::atomic<int> g_sms[kMaxDevices];
+static std::mutex g_dev_mu;
+
+static int current_device() {
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= kMaxDevices) return -1;
+  return d;
+}
+static std::atomic<cudaStream_t> g_pool_stream[kMaxDevices];
+
+// Device memory of the library comes from the device's default memory pool, kept
+// cached between a free and the next allocation (creating and destroying handles
+// then costs no new mappings of device memory); fame_device_trim_memory returns it.
+static cudaStream_t pool_stream(int dev) {
+  if (dev < 0) return nullptr;
+  cudaStream_t s = g_pool_stream[dev].load();
+  if (s) return s;
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  s = g_pool_stream[dev].load();
+  if (!s) {
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    cudaMemPool_t pool = nullptr;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      unsigned long long keep = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+    g_pool_stream[dev].store(s);
+  }
+  return s;
+}
+
 int dalloc(void** p, size_t bytes) {
   *p = nullptr;
   if (bytes == 0) return FAME_OK;
@@ -46,7 +86,10 @@ int dalloc(void** p, size_t bytes) {
     e = cudaMallocAsync(p, bytes, t_alloc_stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(t_alloc_stream);
   } else {
-    e = cudaMalloc(p, bytes);
+    // from the pool; the host wait makes the block usable on every stream
+    cudaStream_t ps = pool_stream(current_device());
+    e = ps ? cudaMallocAsync(p, bytes, ps) : cudaErrorNotReady;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ps);
   }
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -64,22 +107,12 @@ void dfree(void* p) {
     cudaStreamSynchronize(t_alloc_stream);
     cudaFreeAsync(p, t_alloc_stream);
   } else {
-    cudaFree(p);
+    // the same device-wide wait as cudaFree, then back to the pool instead of the driver
+    cudaDeviceSynchronize();
+    cudaFreeAsync(p, pool_stream(current_device()));
   }
 }
 
-// Per-device state shared by all handles: the device fault word that bounded
-// in-kernel waits set when they give up, and the SM count.
-constexpr int kMaxDevices = 64;
-static std::atomic<unsigned*> g_fault[kMaxDevices];
-static std::atomic<int> g_sms[kMaxDevices];
-static std::mutex g_dev_mu;
-
-static int current_device() {
-  int d = 0;
-  if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= kMaxDevices) return -1;
-  return d;
-}
 
 int ensure_device_state(int device) {
   if (device < 0 || device >= kMaxDevices) return fail(FAME_ERR_INVALID, "device index out of range");
@@ -187,6 +220,21 @@ const char* fame_last_error(void) { return g_last_error.c_str(); }
 int fame_version(void) { return 100; }
 
 long long fame_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int fame_device_trim_memory(int device) {
+  int prev = 0, count = 0;
+  FAME_CUDA_TRY(cudaGetDeviceCount(&count));
+  if (device < 0 || device >= count) return fail(FAME_ERR_INVALID, "bad device index");
+  FAME_CUDA_TRY(cudaGetDevice(&prev));
+  FAME_CUDA_TRY(cudaSetDevice(device));
+  cudaMemPool_t pool = nullptr;
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaDeviceGetDefaultMemPool(&pool, device);
+  if (e == cudaSuccess) e = cudaMemPoolTrimTo(pool, 0);
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) return fail(FAME_ERR_CUDA, std::string("fame_device_trim_memory: ") + cudaGetErrorString(e));
+  return FAME_OK;
+}
 
 int fame_ctx_create(int device, fame_ctx** out) {
   if (!out) return fail(FAME_ERR_INVALID, "out is NULL");

@@ -93,6 +93,7 @@ SIGNATURES = {
     "fame_krinv_apply": [P, P, P, I],
     "fame_krinv_stats_get": [P, C.POINTER(fame_krinv_stats)],
     "fame_krinv_stats_reset": [P],
+    "fame_device_trim_memory": [I],
     "fame_lanczos": [P, I, D, I, I, P, C.POINTER(D), P, C.POINTER(fame_lanczos_info)],
     "fame_osi_create": [P, P, D, D, D, I, C.POINTER(P)],
     "fame_osi_destroy": [P],

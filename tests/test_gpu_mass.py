@@ -133,3 +133,22 @@ def test_start_vector_matches_oracle(cuda_device):
     import fame_b200 as F
     v = F.start_vector(20260905, 1000).cpu().numpy()
     assert np.array_equal(v, O.start_vector(20260905, 1000))
+
+
+def test_cached_device_memory_reuse_and_trim(cuda_device):
+    """Handles created and destroyed repeatedly take their device memory from the
+    library's cached pool (same results each time); fame_device_trim_memory returns it."""
+    import fame_b200 as F
+    from fame_b200 import _lib as L
+    N = 2
+    E = torch.as_tensor(O.material_smooth_exp(N), device=cuda_device)
+    x = torch.as_tensor(O.start_vector(4, (2 * N) ** 6), device=cuda_device)
+    outs = []
+    for _ in range(3):
+        m = F.MassBackend(E, N)
+        outs.append(m.MscalarOp(x).cpu().numpy())
+        m.close()
+    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[1], outs[2])
+    assert L.lib.fame_device_trim_memory(cuda_device.index or 0) == 0
+    m = F.MassBackend(E, N)
+    assert np.array_equal(m.MscalarOp(x).cpu().numpy(), outs[0])
