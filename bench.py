@@ -136,6 +136,26 @@ def ncu_traffic(kind):
 
 
 # ----------------------------------------------------------------- fame arm
+def reduce_max_over_ranks(x, world, device):
+    """The largest value of x over the ranks of the process group (every rank calls it
+    at the same point); the job's time is the slowest replica's."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_line(world, rank, seconds_per_step, steps, device):
+    """Whole-job figures of independent replicas (one solve per rank and step): the
+    step time is the maximum over ranks and the throughput counts every rank's solves."""
+    t = reduce_max_over_ranks(seconds_per_step, world, device)
+    return {"seconds_per_step": t, "ms_per_step": round(t * 1e3, 3), "solves_per_s_all_gpus": round(world / t, 4),
+            "n_gpus": world, "steps": steps}
+
+
 def run_fame(args):
     import numpy as np
     import torch
@@ -161,11 +181,7 @@ def run_fame(args):
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max_over_ranks(x, world, dev)
 
     # ---- setup (untimed)
     E = cfg.material_separable_cos(N, 12.0, device=dev)
@@ -211,7 +227,8 @@ def run_fame(args):
     t_mixed, launches, res_mixed = timed_steps("mixed", args.steps)
     st_mixed = ops["mixed"].stats()
     clocks = sampler.stop()
-    step_s = max_over_ranks(sum(t_mixed) / len(t_mixed))
+    job = replica_line(world, rank, sum(t_mixed) / len(t_mixed), args.steps, dev)
+    step_s = job["seconds_per_step"]
     t_fp64, _, res_fp64 = timed_steps("fp64", 1)
     fp64_s = max_over_ranks(t_fp64[0])
     st_fp64 = ops["fp64"].stats()
@@ -393,7 +410,7 @@ def run_fame(args):
                                 "fp64_refinements_per_call": round(st_mixed.refineSteps / max(1, st_mixed.inverseCalls), 2)},
                       "fp64": {"krinv_calls": st_fp64.inverseCalls,
                                "pcg_iters_per_call": round(st_fp64.totalIterations / max(1, st_fp64.inverseCalls), 2)}},
-            "solves_per_s_all_gpus": round(world / step_s, 4),
+            "solves_per_s_all_gpus": job["solves_per_s_all_gpus"],
             "yee_pts_per_s": (yee or {}).get("direct_pts_per_s"),
             "yee": yee,
             "bloch_path": bloch,
