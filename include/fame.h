@@ -191,7 +191,7 @@ typedef struct {
   int useKrPreconditioner; /* nested (1) */
   double tolInner32; /* mixed: relative tolerance of each FP32 correction solve (1e-5) */
   int maxRefine;     /* mixed: max FP64 refinement steps per solve (20) */
-  int checkEvery;    /* PCG iterations queued between host convergence checks (8) */
+  int checkEvery;    /* PCG iterations queued between host convergence checks (4) */
   int verifyTrueResidual; /* confirm convergence on the true residual, as MATLAB pcg (1) */
   int useGraphs;     /* replay PCG iterations as captured CUDA graphs (1) */
   int mhatPreconditioner; /* explicit: precondition the Mhat PCG with the same operator on the

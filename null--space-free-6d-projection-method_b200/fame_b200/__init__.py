@@ -13,3 +13,4 @@ from . import configs  # noqa: F401
 from .recon import *  # noqa: F401,F403
 from . import grad  # noqa: F401
 from .method_a import *  # noqa: F401,F403
+from . import autotune  # noqa: F401

@@ -145,3 +145,19 @@ def test_pivoted_split_when_v1_is_singular(cuda_device):
         S = O.build_q_system(N, F.configs.P_GOLDEN, q, E)
     yo = O.make_nested_krinv_instrumented(S, 4.0, 1e-12, 1e-13)[0](b)
     assert _rel(yb, yo) < 1e-9
+
+
+@pytest.mark.parametrize("N", [2, 3])
+def test_launch_schedule_autotuner(cuda_device, N):
+    """The launch-schedule candidates (host-check cadence, graph replay) give bitwise-
+    identical K_r^{-1} actions (the tuner raises otherwise) and the tuner returns the
+    fastest as make_explicit_krinv_compact options."""
+    import fame_b200 as F
+    E = torch.as_tensor(O.material_smooth_exp(N), device=cuda_device)
+    s = F.build_q_system(F.MassBackend(E, N), F.configs.P_REFERENCE, F.configs.Q_TRACKING)
+    best, table = F.autotune.tune_krinv_schedule(s, precision="mixed", reps=2)
+    assert len(table) == len(F.autotune.DEFAULT_CANDIDATES)
+    fastest = min(table, key=lambda r: r["seconds"])
+    assert best == {"checkEvery": fastest["checkEvery"], "useGraphs": fastest["useGraphs"]}
+    op, _ = F.make_explicit_krinv_compact(s, 1e-10, 3000, precision="mixed", **best)
+    assert op(F.start_vector(7, s.nr).reshape(-1, 1)).isfinite().all()
