@@ -107,9 +107,16 @@ void dfree(void* p) {
     cudaStreamSynchronize(t_alloc_stream);
     cudaFreeAsync(p, t_alloc_stream);
   } else {
-    // the same device-wide wait as cudaFree, then back to the pool instead of the driver
+    // the same device-wide wait as cudaFree, then back to the pool instead of the driver,
+    // on the device that owns the block (which need not be the current one)
+    int owner = current_device(), prev = owner;
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) == cudaSuccess && at.device >= 0) owner = at.device;
+    cudaGetLastError();
+    if (owner != prev) cudaSetDevice(owner);
     cudaDeviceSynchronize();
-    cudaFreeAsync(p, pool_stream(current_device()));
+    cudaFreeAsync(p, pool_stream(owner));
+    if (owner != prev) cudaSetDevice(prev);
   }
 }
 
