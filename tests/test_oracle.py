@@ -234,3 +234,44 @@ def test_method_a_minres_top_vs_dense_n1():
     tau = 0.37
     z = O.apply_shift_preconditioner(x, S, tau)
     assert _rel((K + tau * np.eye(3 * S.NF)) @ z, x) < 1e-13
+
+
+def test_mass_adjoint_matches_finite_differences_n1():
+    """The oracle's x^H (dM/dtheta_t) x (the checker of the GPU adjoint, no reference
+    function) against central differences of x^H M(theta) x in each of the 7 material
+    parameters theta = (delta, a_1..a_6) of eps = 1 + delta prod (1 + a cos)/(1 + a)."""
+    N = 1
+    theta = np.array([12.0, 0.6, 0.7, 0.8, 0.9, 0.55, 0.95])
+    eps, grads = O.material_cos_param(N, theta[0], theta[1:])
+    n = (2 * N) ** 6
+    X = np.stack([O.start_vector(40 + j, 3 * n) for j in range(2)], 1)
+    quad = O.mass_adjoint_quadratic(X, grads, N)
+
+    def xMx(th, x):
+        e, _ = O.material_cos_param(N, th[0], th[1:])
+        m = O.MassOp(e, N)
+        return float(np.real(np.vdot(x, m.full(x))))
+
+    h = 1e-6
+    for t in range(7):
+        tp, tm = theta.copy(), theta.copy()
+        tp[t] += h
+        tm[t] -= h
+        for j in range(2):
+            fd = (xMx(tp, X[:, j]) - xMx(tm, X[:, j])) / (2 * h)
+            assert abs(quad[j, t] - fd) <= 1e-6 * max(1.0, abs(fd)), (t, j, quad[j, t], fd)
+
+
+def test_recovered_eigenvectors_solve_the_original_gevp_n1():
+    """exp2/recover_original_eigenvectors_exp2.m: x = M^-1 V y from the null-space-free
+    eigenvectors, M-normalised, satisfies the original K x = lambda M x (dense operators)."""
+    N = 1
+    S = O.build_q_system(N, P_REF, (0.13, 0.21, 0.17), O.material_smooth_exp(N))
+    sol = O.solve_modes(S, nev=4, p=20, tol=1e-10, tolCG=1e-12)
+    X, MX, _ = O.recover_original_eigenvectors(sol["Y"], S, 1e-12, 3000)
+    K, M3 = O.dense_original_operators(S)
+    for j, lam in enumerate(sol["lam"]):
+        x = X[:, j]
+        assert abs(np.vdot(x, M3 @ x) - 1.0) < 1e-10
+        r = np.linalg.norm(K @ x - lam * (M3 @ x)) / (np.linalg.norm(K @ x) + lam * np.linalg.norm(M3 @ x))
+        assert r < 1e-9, (j, r)
