@@ -186,7 +186,7 @@ def run_fame(args):
     # ---- setup (untimed)
     E = cfg.material_separable_cos(N, 12.0, device=dev)
     mass = F.MassBackend(E, N)
-    sysq = F.build_q_system(mass, cfg.P_GOLDEN, cfg.Q_BASELINE)
+    sysq = F.build_q_system(mass, cfg.P_GOLDEN, cfg.Q_PHYS)
     v0 = F.start_vector(cfg.SEED, sysq.nr)
     ops = {}
     for prec in ("mixed", "fp64"):
@@ -372,7 +372,7 @@ def run_fame(args):
             Ed = E_h.to(dev, non_blocking=True)
             vd = v0_h.to(dev, non_blocking=True)
             m2 = F.MassBackend(Ed, N)
-            s2 = F.build_q_system(m2, cfg.P_GOLDEN, cfg.Q_BASELINE)
+            s2 = F.build_q_system(m2, cfg.P_GOLDEN, cfg.Q_PHYS)
             op2, _ = F.make_explicit_krinv_compact(s2, S["tolCG"], S["maxitCG"], precision="mixed")
             Y, theta, _, _ = F.Lanczos(op2, None, None, s2.nr, S["nev"], S["tol"], S["maxRestart"],
                                        S["p"], vd)
@@ -443,7 +443,7 @@ def cpu_baseline(N, steps_in_solve=40, kind="port"):
         pass
     E = O.material_separable_cos(N, 12.0)
     from fame_b200 import configs as cfg
-    S = O.build_q_system(N, cfg.P_GOLDEN, cfg.Q_BASELINE, E)
+    S = O.build_q_system(N, cfg.P_GOLDEN, cfg.Q_PHYS, E)
     op, stats = O.make_explicit_krinv_compact(S, 1e-10, 3000)
     v0 = O.start_vector(cfg.SEED, S.nr)
     v0 = v0 / np.linalg.norm(v0)
@@ -478,7 +478,7 @@ def run_case(args):
     S = cfg.SOLVE
     E = cfg.material_separable_cos(N, 12.0, device=dev)
     mass = F.MassBackend(E, N)
-    sysq = F.build_q_system(mass, cfg.P_GOLDEN, cfg.Q_BASELINE)
+    sysq = F.build_q_system(mass, cfg.P_GOLDEN, cfg.Q_PHYS)
     v0 = F.start_vector(cfg.SEED, sysq.nr)
     prec = "fp64" if args.precision == "fp64" else "mixed"
     if args.case == "yee":

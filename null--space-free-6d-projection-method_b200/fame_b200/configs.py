@@ -16,7 +16,7 @@ import torch
 PHI = (1.0 + math.sqrt(5.0)) / 2.0
 P_GOLDEN = np.vstack([np.eye(3), np.diag([PHI, 1.0 / PHI, PHI ** 2])])
 P_REFERENCE = np.vstack([np.eye(3), np.diag([math.sqrt(2.0), math.sqrt(3.0), math.sqrt(5.0)])])
-Q_BASELINE = (0.05, 0.04, 0.03)          # exp1/make_config_exp1bc.m:34
+Q_PHYS = (0.05, 0.04, 0.03)          # exp1/make_config_exp1bc.m:34
 Q_TRACKING = (0.13, 0.21, 0.17)          # exp3/make_config_experiment4.m:26
 SEED = 20260905                          # exp1/make_config_BC_fig1a.m:42
 # Reference KAT: N=2, modes 1 and 10 of the tracking system (exp3/make_config_experiment4.m:38-40)

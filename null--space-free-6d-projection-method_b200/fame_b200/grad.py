@@ -37,7 +37,7 @@ def eigenpairs(N, theta, P=None, q=None, nev=10, p=40, tol=1e-8, tolCG=1e-10, pr
                device="cuda"):
     """Smallest eigenpairs for the parametrised material eps(theta) = 1 + delta prod (1+a cos)/(1+a)."""
     P = configs.P_GOLDEN if P is None else P
-    q = configs.Q_BASELINE if q is None else q
+    q = configs.Q_PHYS if q is None else q
     theta = np.asarray(theta, dtype=np.float64)
     eps, grads = configs.material_cos_param(N, float(theta[0]), theta[1:7], device=device)
     mass = MassBackend(eps, N)

@@ -20,7 +20,7 @@ import oracle as O  # noqa: E402
 PHI = (1 + 5 ** 0.5) / 2
 P_GOLDEN = np.vstack([np.eye(3), np.diag([PHI, 1 / PHI, PHI ** 2])])
 P_REF = np.vstack([np.eye(3), np.diag([np.sqrt(2), np.sqrt(3), np.sqrt(5)])])
-Q_BASELINE = (0.05, 0.04, 0.03)
+Q_PHYS = (0.05, 0.04, 0.03)
 Q_TRACKING = (0.13, 0.21, 0.17)
 
 
@@ -32,7 +32,7 @@ def main():
     x = O.start_vector(7, (2 * N) ** 6)
     out["mass_n2"] = dict(E=E, x=x, y=O.applyMij_fft(x, E, N))
     # basis diagonals, N=2, golden-ratio cut matrix at the benchmark Bloch vector
-    S = O.build_q_system(N, P_GOLDEN, Q_BASELINE, O.material_separable_cos(N))
+    S = O.build_q_system(N, P_GOLDEN, Q_PHYS, O.material_separable_cos(N))
     out["basis_n2_golden"] = dict(V11=S.V11, V12=S.V12, V21=S.V21, V22=S.V22, V31=S.V31,
                                   V32=S.V32, detV1=S.detV1, W1=S.W1, W2=S.W2, invC=S.invC,
                                   kLift=S.kLift)
@@ -43,12 +43,12 @@ def main():
     out["krinv_n2_tracking"] = dict(b=b, y=y)
     # 10 smallest eigenvalues: N=2 tracking system (reference KAT) and N=3 benchmark system
     lam2 = O.solve_modes(St, nev=10, p=40, tol=1e-10, tolCG=1e-12)["lam"]
-    S3 = O.build_q_system(3, P_GOLDEN, Q_BASELINE, O.material_separable_cos(3))
+    S3 = O.build_q_system(3, P_GOLDEN, Q_PHYS, O.material_separable_cos(3))
     lam3 = O.solve_modes(S3, nev=10, p=40, tol=1e-10, tolCG=1e-12)["lam"]
     out["eigs"] = dict(n2_tracking=lam2, n3_baseline=lam3,
                        kat_n2=np.array([1.201276300237e-02, 4.496454358674e-02]))
     # Yee-field reconstruction, N=1: direct and multi-center Taylor (p=6, 8 centers)
-    S1 = O.build_q_system(1, P_GOLDEN, Q_BASELINE, O.material_separable_cos(1))
+    S1 = O.build_q_system(1, P_GOLDEN, Q_PHYS, O.material_separable_cos(1))
     Qm = O.build_projected_q_modes(P_GOLDEN, S1.kLift, 1)
     c = O.start_vector(13, S1.NF)
     r1, _, _, sz = O.build_yee_points(4, 0.0125)

@@ -31,7 +31,7 @@ def test_basis_vs_fixture(cuda_device):
     import fame_b200 as F
     d = load("basis_n2_golden")
     m = F.MassBackend(F.configs.material_separable_cos(2, device=cuda_device), 2)
-    s = F.build_q_system(m, F.configs.P_GOLDEN, F.configs.Q_BASELINE)
+    s = F.build_q_system(m, F.configs.P_GOLDEN, F.configs.Q_PHYS)
     np.testing.assert_allclose(s.kLift, d["kLift"], rtol=1e-14, atol=1e-16)
     for k in ("V11", "V12", "V21", "V22", "V31", "V32", "detV1", "W1", "W2"):
         assert rel(getattr(s, k).cpu().numpy(), d[k]) < 1e-10, k

@@ -18,7 +18,7 @@ def rel(a, b):
 def _sys(N, dev, material="cos", Pname="golden", q=None):
     import fame_b200 as F
     P = F.configs.P_GOLDEN if Pname == "golden" else F.configs.P_REFERENCE
-    q = F.configs.Q_BASELINE if q is None else q
+    q = F.configs.Q_PHYS if q is None else q
     E = O.material_separable_cos(N) if material == "cos" else O.material_smooth_exp(N)
     m = F.MassBackend(torch.as_tensor(E, device=dev), N)
     return F, O.build_q_system(N, P, q, E), F.build_q_system(m, P, q), m

@@ -103,7 +103,7 @@ def test_lanczos_baseline_n3_fp64_and_mixed(cuda_device):
     the 10th eigenvalue), so two FP64 implementations agree to ~1e-9 there."""
     import fame_b200 as F
     N = 3
-    S, sg = _systems(N, "golden", F.configs.Q_BASELINE, "cos", cuda_device)
+    S, sg = _systems(N, "golden", F.configs.Q_PHYS, "cos", cuda_device)
     sol = O.solve_modes(S, nev=10, p=40, tol=1e-10, maxRestart=30, tolCG=1e-12)
     v0 = F.start_vector(F.configs.SEED, sg.nr)
     lams = {}

@@ -20,7 +20,7 @@ pytestmark = pytest.mark.gpu
 def _system(N, dev):
     import fame_b200 as F
     m = F.MassBackend(F.configs.material_separable_cos(N, device=dev), N)
-    s = F.build_q_system(m, F.configs.P_GOLDEN, F.configs.Q_BASELINE)
+    s = F.build_q_system(m, F.configs.P_GOLDEN, F.configs.Q_PHYS)
     return F, m, s
 
 
