@@ -53,12 +53,27 @@ def test_null_arguments_are_rejected_without_gpu():
     assert L.fame_basis_get(None, 0, None) == 1
 
 
+def test_method_a_entry_points_reject_bad_arguments_without_gpu():
+    from fame_b200 import _lib
+    L = _lib.lib
+    out = C.c_void_p()
+    assert L.fame_osi_create(None, None, 1e-4, 1e-4, 1e-10, 100, C.byref(out)) == 1
+    assert b"fame_osi_create" in L.fame_last_error()
+    assert L.fame_osi_apply(None, None, None, 1) == 1
+    lam = (C.c_double * 1)()
+    assert L.fame_osi_eigs(None, 1, 1e-8, 10, 20, None, lam, None, None) == 1
+    assert L.fame_osi_stats_get(None, None) == 1
+    assert L.fame_apply_K_original(None, None, None, 1) == 1
+    assert L.fame_osi_destroy(None) == 0
+
+
 def test_struct_layouts_match_header():
     from fame_b200 import _lib
     # field counts mirror include/fame.h
     assert len(_lib.fame_krinv_opts._fields_) == 16
     assert len(_lib.fame_krinv_stats._fields_) == 10
     assert C.sizeof(_lib.fame_basis_info) == 8 + 4 + 4 + 8 + 8 + 48 + 8
+    assert C.sizeof(_lib.fame_osi_stats) == 3 * 8 + 8 + 4 + 4
 
 
 def test_twiddle_header_is_generated_and_exact():
