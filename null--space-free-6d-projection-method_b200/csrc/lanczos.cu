@@ -118,6 +118,84 @@ __global__ void __launch_bounds__(256) k_gemv_n_sub(const double2* __restrict__ 
   grid_sum_finalize<double, 1>(acc, partials, counter, [&](const Red<double, 1>& t) { scal[0] = t.v[0]; });
 }
 
+// Between two Gram-Schmidt passes: w -= Q c (c = the previous pass's coefficients),
+// then this block's share of the next pass's Q^H w, both from one read of Q.  Each
+// warp stages the 32 x m tile of its 32 rows in shared memory (cp.async; row stride
+// m|1, so the sweep along a row and the sweep along a column are both free of bank
+// conflicts), subtracts along its rows, and accumulates the inner products along the
+// columns: lane l owns columns l and l + 32 (m <= 64).  partial[b*m + j] as k_gemv_h.
+constexpr int kFuseWarps = 4;
+constexpr int kFuseMaxCols = 64;
+constexpr size_t kFuseSmemMax = (size_t)kFuseWarps * 32 * (kFuseMaxCols + 1) * sizeof(double2);
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+__global__ void __launch_bounds__(kFuseWarps * 32) k_cgs_sub_dot(const double2* __restrict__ Q, long long ldq, int m,
+                                                                 const double2* __restrict__ coef,
+                                                                 double2* __restrict__ w, long long n,
+                                                                 double2* __restrict__ partial) {
+  extern __shared__ double2 tiles[];  // [kFuseWarps][32][m|1]
+  __shared__ double2 c[kFuseMaxCols];
+  __shared__ double2 red[kFuseWarps][kFuseMaxCols];
+  const int ms = m | 1;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double2* tile = tiles + (size_t)wid * 32 * ms;
+  double2* mine = tile + lane * ms;
+  for (int j = threadIdx.x; j < m; j += blockDim.x) c[j] = coef[j];
+  __syncthreads();
+  double a0r = 0.0, a0i = 0.0, a1r = 0.0, a1i = 0.0;
+  const long long groups = (n + 31) >> 5;
+  for (long long g = (long long)blockIdx.x * kFuseWarps + wid; g < groups; g += (long long)gridDim.x * kFuseWarps) {
+    const long long row = (g << 5) + lane;
+    const bool live = row < n;
+    __syncwarp();  // the previous group's column sweep is done with the tile
+    if (live) {
+      const double2* src = Q + row;
+      for (int j = 0; j < m; ++j) cp_async16(mine + j, src + ldq * j);
+    } else {
+      for (int j = 0; j < m; ++j) mine[j] = make_double2(0.0, 0.0);
+    }
+    double2 v = live ? w[row] : make_double2(0.0, 0.0);
+    cp_async_wait_all();
+    __syncwarp();
+    for (int j = 0; j < m; ++j) {
+      const double2 q = mine[j], cj = c[j];
+      v.x -= q.x * cj.x - q.y * cj.y;
+      v.y -= q.x * cj.y + q.y * cj.x;
+    }
+    if (live) w[row] = v;
+    for (int r = 0; r < 32; ++r) {
+      const double vx = __shfl_sync(0xffffffffu, v.x, r), vy = __shfl_sync(0xffffffffu, v.y, r);
+      const double2* tr = tile + r * ms;
+      if (lane < m) {
+        const double2 q = tr[lane];
+        a0r += q.x * vx + q.y * vy;
+        a0i += q.x * vy - q.y * vx;
+      }
+      if (lane + 32 < m) {
+        const double2 q = tr[lane + 32];
+        a1r += q.x * vx + q.y * vy;
+        a1i += q.x * vy - q.y * vx;
+      }
+    }
+  }
+  if (lane < m) red[wid][lane] = make_double2(a0r, a0i);
+  if (lane + 32 < m) red[wid][lane + 32] = make_double2(a1r, a1i);
+  __syncthreads();
+  for (int j = threadIdx.x; j < m; j += blockDim.x) {
+    double sr = 0.0, si = 0.0;
+    for (int k = 0; k < kFuseWarps; ++k) {
+      sr += red[k][j].x;
+      si += red[k][j].y;
+    }
+    partial[(long long)blockIdx.x * m + j] = make_double2(sr, si);
+  }
+}
+
 // ||x||^2 -> scal[0]
 __global__ void k_nrm2(const double2* x, long long n, double* scal, double* partials, unsigned* counter) {
   Red<double, 1> acc{};
@@ -290,6 +368,7 @@ struct LanczosWs {
     FAME_TRY(dalloc((void**)&v, n * sizeof(double2)));
     FAME_TRY(dalloc((void**)&coef, kMaxCols * sizeof(double2)));
     FAME_TRY(dalloc((void**)&partial, (size_t)nblk * p * sizeof(double2)));
+    FAME_CUDA_TRY(cudaFuncSetAttribute(k_cgs_sub_dot, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFuseSmemMax));
     FAME_TRY(dalloc((void**)&scal, 8 * sizeof(double)));
     FAME_TRY(dalloc((void**)&partials, 4 * kVecBlocksMax * sizeof(double)));
     FAME_TRY(dalloc((void**)&counter, sizeof(unsigned)));
@@ -319,13 +398,41 @@ struct LanczosWs {
     std::memcpy(h, hbuf, bytes);
     return FAME_OK;
   }
-  // one classical Gram-Schmidt pass against Q(:,0:m); ||w||^2 -> scal[0]
-  int cgs_pass(int m, bool write_alpha) {
+  // blocks of k_cgs_sub_dot: persistent over the row groups, as many as fit at once,
+  // and no more than the partial buffer's nblk rows
+  int fuse_blocks(int m) const {
+    const size_t smem = (size_t)kFuseWarps * 32 * (m | 1) * sizeof(double2) + 6 * 1024;
+    const long long per_sm = std::max<long long>(1, std::min<long long>(16, (227 * 1024) / (long long)smem));
+    const long long need = ((n + 31) / 32 + kFuseWarps - 1) / kFuseWarps;
+    return (int)std::max<long long>(1, std::min<long long>({need, 148 * per_sm, (long long)nblk}));
+  }
+  // `passes` classical Gram-Schmidt passes against Q(:,0:m): alpha = Re of the first
+  // pass's last coefficient -> scal[1]; ||w||^2 after the last pass -> scal[0].  The
+  // subtraction of one pass and the inner products of the next share one read of Q
+  // (k_cgs_sub_dot, m <= 64), so two passes read Q three times instead of four.
+  int cgs(int m, int passes) {
     cudaStream_t s = ctx->stream;
     k_gemv_h<<<nblk, kGemvThreads, 0, s>>>(Q, n, m, w, n, partial);
     ::fame::count_launch();
-    k_gemv_h_reduce<<<m, 256, 0, s>>>(partial, nblk, m, coef, scal, write_alpha ? 1 : 0);
+    k_gemv_h_reduce<<<m, 256, 0, s>>>(partial, nblk, m, coef, scal, 1);
     ::fame::count_launch();
+    for (int pass = 1; pass < passes; ++pass) {
+      if (m <= kFuseMaxCols) {
+        const int g = fuse_blocks(m);
+        const size_t smem = (size_t)kFuseWarps * 32 * (m | 1) * sizeof(double2);
+        k_cgs_sub_dot<<<g, kFuseWarps * 32, smem, s>>>(Q, n, m, coef, w, n, partial);
+        ::fame::count_launch();
+        k_gemv_h_reduce<<<m, 256, 0, s>>>(partial, g, m, coef, scal, 0);
+        ::fame::count_launch();
+      } else {
+        k_gemv_n_sub<<<vec_blocks(n), 256, 0, s>>>(Q, n, m, coef, w, n, scal, partials, counter);
+        ::fame::count_launch();
+        k_gemv_h<<<nblk, kGemvThreads, 0, s>>>(Q, n, m, w, n, partial);
+        ::fame::count_launch();
+        k_gemv_h_reduce<<<m, 256, 0, s>>>(partial, nblk, m, coef, scal, 0);
+        ::fame::count_launch();
+      }
+    }
     k_gemv_n_sub<<<vec_blocks(n), 256, 0, s>>>(Q, n, m, coef, w, n, scal, partials, counter);
     ::fame::count_launch();
     FAME_CUDA_TRY(cudaGetLastError());
@@ -415,12 +522,8 @@ int lanczos_run(const LanczosOperator& op, int nev, double tol, int maxiter, int
       FAME_CUDA_TRY(cudaMemcpyAsync(qj, L.v, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
       FAME_TRY(op.apply(op.self, qj, L.w));  // Aq = fncA(Q(:,jj))
       // alpha = Re(Aq' Q(:,jj)) from the first pass; passes: 2, or 3 after a restart
-      FAME_TRY(L.cgs_pass(jj, true));
-      FAME_TRY(L.cgs_pass(jj, false));
-      if (justRestarted) {
-        FAME_TRY(L.cgs_pass(jj, false));
-        justRestarted = false;
-      }
+      FAME_TRY(L.cgs(jj, justRestarted ? 3 : 2));
+      justRestarted = false;
       double sc[2];
       FAME_TRY(L.sync_read(L.scal, sc, 2 * sizeof(double)));
       const double alpha = sc[1], beta2 = sc[0];
