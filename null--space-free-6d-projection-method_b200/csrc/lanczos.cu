@@ -3,8 +3,9 @@
 //
 // Device side: the basis Q (n x p, FP64 complex) stays in HBM; each step's
 // full reorthogonalisation is classical Gram-Schmidt applied twice (three
-// times right after a restart) as two streaming kernels per pass
-// (c = Q^H w, then w -= Q c with ||w||^2 fused), replacing the reference's
+// times right after a restart) as streaming kernels (c = Q^H w; between two
+// passes w -= Q c and the next Q^H w from one read of Q; after the last pass
+// w -= Q c with ||w||^2 fused), replacing the reference's
 // column-by-column modified Gram-Schmidt with one host sync per dot
 // (exp2/Lanczos.m:150-155).  The projected (arrowhead + tridiagonal) matrix
 // H is diagonalised on the GPU by a one-CTA parallel cyclic Jacobi method;
