@@ -262,8 +262,10 @@ FAME_API int fame_taylor_on_blocks(fame_ctx* ctx, const void* coeff, const doubl
                                    int nBlocks, const double* fixedCenter, void* u);
 /* Same reconstruction with the block moments (the dense contraction over the NF modes) as
    split-FP32 tensor-core products: each FP32 operand is split into TF32 head + tail and the
-   moments are head*head + head*tail + tail*head (3xTF32), computed by tcgen05 UMMA GEMMs
-   (CUTLASS sm100 collectives) and reduced in FP64.  Relative field error vs the FP64 form ~1e-7.
+   moments are head*head + head*tail + tail*head (3xTF32), computed by hand-written tcgen05
+   kind::tf32 MMAs on operands generated in shared memory from qModes and coeff (slices of at
+   most 512 modes, FP32 accumulation in TMEM) and summed over slices in FP64.  Relative field
+   error vs the FP64 form ~2e-6 (the tensor cores' FP32 accumulation sets it).
    No counterpart in the reference (its Taylor moments are FP64 gpuArray products). */
 FAME_API int fame_taylor_on_blocks_3xtf32(fame_ctx* ctx, const void* coeff, const double* qModes, long long NF,
                                           const double* rPoints, long long M, int p, const long long* blockPtr,
