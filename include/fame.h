@@ -68,10 +68,10 @@ FAME_API const char* fame_last_error(void);
 FAME_API int fame_version(void);
 /* Kernels launched by this library since load (instrumentation for benchmarks). */
 FAME_API long long fame_kernel_launches(void);
-/* (No reference counterpart) the library takes its device memory from the device's
- * default memory pool and keeps freed blocks cached for its next handles (a free still
- * waits for the device, as cudaFree does); this returns the cached memory of a device
- * to the driver. */
+/* (No reference counterpart) the library takes its device memory from a memory pool it
+ * creates per device (the device's default pool and its settings are left alone) and keeps
+ * freed blocks cached for its next handles (a free still waits for the device, as cudaFree
+ * does); this returns the cached memory of a device to the driver. */
 FAME_API int fame_device_trim_memory(int device);
 
 /* ---- context (replaces gpu_initialize / wait_for_gpu: exp1/wait_for_gpu.m:5-11) ---- */
@@ -290,6 +290,17 @@ typedef struct {
 /* n = 2NF; theta: host, k values (descending); Y: device n x k complex128 (may be NULL) */
 FAME_API int fame_lanczos(fame_krinv* k, int nev, double tol, int maxiter, int p, const void* v0,
                  double* theta, void* Y, fame_lanczos_info* info);
+
+/* (No reference counterpart; the reference reports lambda = 1/theta of the Lanczos Ritz
+ * values, exp2/Lanczos.m:140-147, whose error follows the inner tolerance of K_r^{-1}.)
+ * Rayleigh-Ritz refinement of k (1..32) approximate eigenvectors Y (device, 2NF x k,
+ * complex128, e.g. the Y of fame_lanczos) with the exact K_r = V^* M^{-1} V: on the (2N)^6
+ * grid M^{-1} is the mass chain on the material 1/eps, so K_r applies to rounding error.
+ * Solves Y^H K_r Y u = lambda Y^H Y u, overwrites Y with the refined vectors (Y u) and
+ * returns lambda (host, k, ascending) and, if relres is not NULL, ||K_r y - lambda y|| /
+ * ||K_r y|| per refined vector (host, k).  The eigenvalue error is quadratic in the
+ * eigenvector error of the input. */
+FAME_API int fame_rayleigh_ritz(fame_basis* b, fame_mass* m, void* Y, int k, double* lambda, double* relres);
 
 /* ---- Method A: original shift-invert without the null-space-free basis ----
  * exp1/build_experiment1_q_system_A_only.m, exp1/build_original_shift_preconditioner_A_only.m,

@@ -52,9 +52,13 @@ static int current_device() {
 }
 static std::atomic<cudaStream_t> g_pool_stream[kMaxDevices];
 
-// Device memory of the library comes from the device's default memory pool, kept
-// cached between a free and the next allocation (creating and destroying handles
-// then costs no new mappings of device memory); fame_device_trim_memory returns it.
+// Device memory of the library comes from a memory pool the library creates per
+// device (not the device's default pool, so the retention set here affects no other
+// user of the process), kept cached between a free and the next allocation (creating
+// and destroying handles then costs no new mappings of device memory);
+// fame_device_trim_memory returns it to the driver.
+static std::atomic<cudaMemPool_t> g_pool[kMaxDevices];
+
 static cudaStream_t pool_stream(int dev) {
   if (dev < 0) return nullptr;
   cudaStream_t s = g_pool_stream[dev].load();
@@ -62,16 +66,25 @@ static cudaStream_t pool_stream(int dev) {
   std::lock_guard<std::mutex> lk(g_dev_mu);
   s = g_pool_stream[dev].load();
   if (!s) {
-    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
       cudaGetLastError();
       return nullptr;
     }
-    cudaMemPool_t pool = nullptr;
-    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-      unsigned long long keep = ~0ull;
-      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    unsigned long long keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      cudaMemPoolDestroy(pool);
+      return nullptr;
     }
     cudaGetLastError();
+    g_pool[dev].store(pool);
     g_pool_stream[dev].store(s);
   }
   return s;
@@ -81,14 +94,18 @@ int dalloc(void** p, size_t bytes) {
   *p = nullptr;
   if (bytes == 0) return FAME_OK;
   cudaError_t e;
-  if (t_ordered) {
+  const int dev = current_device();
+  cudaStream_t ps = pool_stream(dev);
+  cudaMemPool_t pool = dev >= 0 ? g_pool[dev].load() : nullptr;
+  if (!ps || !pool) {
+    e = cudaErrorNotReady;
+  } else if (t_ordered) {
     // usable on every stream once the (host-side) pool allocation is ordered
-    e = cudaMallocAsync(p, bytes, t_alloc_stream);
+    e = cudaMallocFromPoolAsync(p, bytes, pool, t_alloc_stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(t_alloc_stream);
   } else {
-    // from the pool; the host wait makes the block usable on every stream
-    cudaStream_t ps = pool_stream(current_device());
-    e = ps ? cudaMallocAsync(p, bytes, ps) : cudaErrorNotReady;
+    // the host wait makes the block usable on every stream
+    e = cudaMallocFromPoolAsync(p, bytes, pool, ps);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ps);
   }
   if (e != cudaSuccess) {
@@ -234,10 +251,9 @@ int fame_device_trim_memory(int device) {
   if (device < 0 || device >= count) return fail(FAME_ERR_INVALID, "bad device index");
   FAME_CUDA_TRY(cudaGetDevice(&prev));
   FAME_CUDA_TRY(cudaSetDevice(device));
-  cudaMemPool_t pool = nullptr;
+  cudaMemPool_t pool = g_pool[device].load();
   cudaError_t e = cudaDeviceSynchronize();
-  if (e == cudaSuccess) e = cudaDeviceGetDefaultMemPool(&pool, device);
-  if (e == cudaSuccess) e = cudaMemPoolTrimTo(pool, 0);
+  if (e == cudaSuccess && pool) e = cudaMemPoolTrimTo(pool, 0);
   cudaSetDevice(prev);
   if (e != cudaSuccess) return fail(FAME_ERR_CUDA, std::string("fame_device_trim_memory: ") + cudaGetErrorString(e));
   return FAME_OK;

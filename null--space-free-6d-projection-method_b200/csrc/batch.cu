@@ -96,15 +96,13 @@ extern "C" int fame_solve_batch(int device, int count, const int* Ns, const doub
     j.theta = theta + (size_t)nev * i;
     j.info = info ? info + i : nullptr;
   }
-  // pool memory stays cached between the instances' frees and allocations and across
-  // calls (mapping gigabytes anew costs more than the small solves themselves); it is
-  // the device's default pool, released by cudaMemPoolTrimTo or at process exit
-  cudaMemPool_t pool = nullptr;
-  if (cudaSetDevice(device) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
-    unsigned long long keep = ~0ull;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  // the instances allocate from the library's own pool of the device, which keeps freed
+  // blocks cached between the instances and across calls (mapping gigabytes anew costs
+  // more than the small solves themselves); fame_device_trim_memory releases it
+  if (cudaSetDevice(device) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(FAME_ERR_CUDA, "fame_solve_batch: cannot select the device");
   }
-  cudaGetLastError();
   // largest instances first: they start their long chains of launches earliest
   std::vector<int> order(count);
   for (int i = 0; i < count; ++i) order[i] = i;

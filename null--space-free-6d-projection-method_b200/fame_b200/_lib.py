@@ -95,6 +95,7 @@ SIGNATURES = {
     "fame_krinv_stats_reset": [P],
     "fame_device_trim_memory": [I],
     "fame_lanczos": [P, I, D, I, I, P, C.POINTER(D), P, C.POINTER(fame_lanczos_info)],
+    "fame_rayleigh_ritz": [P, P, P, I, C.POINTER(D), C.POINTER(D)],
     "fame_osi_create": [P, P, D, D, D, I, C.POINTER(P)],
     "fame_osi_destroy": [P],
     "fame_osi_apply": [P, P, P, I],

@@ -22,6 +22,7 @@ __all__ = [
     "solveV1_blockdiag", "solveV1H_blockdiag", "QSystem", "build_q_system",
     "make_explicit_krinv_compact", "make_nested_krinv_instrumented", "KrInv", "Lanczos",
     "start_vector", "FameError", "apply_Mhat_C_scalar_compact", "kernel_launches", "solve_batch",
+    "rayleigh_ritz",
 ]
 
 
@@ -453,6 +454,25 @@ def Lanczos(fncA, fncB, fncBinv, n, k, tol, maxiter, p, v0, flag_gpu=True, verbo
     return Y.t(), ew, info.steps, dict(steps=info.steps, restarts=info.restarts,
                                        converged=bool(info.converged), nconv=info.nconv,
                                        maxWantedResidual=info.maxWantedResidual)
+
+
+def rayleigh_ritz(sys: QSystem, Y):
+    """Rayleigh-Ritz refinement with the exact K_r = V^* M^{-1} V (no reference counterpart).
+
+    ``Y``: complex128 device matrix (2NF x k, k <= 32), e.g. the eigenvectors returned by
+    ``Lanczos``; it is overwritten with the refined vectors.  Returns ``(lam, relres)``:
+    ascending eigenvalues lambda of K_r and ||K_r y - lambda y|| / ||K_r y|| per vector.
+    """
+    if Y.dim() != 2 or Y.shape[0] != sys.nr or Y.dtype != torch.complex128 or not Y.is_cuda:
+        raise FameError(L.FAME_ERR_INVALID, "Y must be a complex128 CUDA matrix with 2*NF rows")
+    k = int(Y.shape[1])
+    if Y.stride(0) != 1 or Y.stride(1) != sys.nr:
+        raise ValueError("Y must be column-major (Y.t() contiguous), as Lanczos returns it")
+    lam = (C.c_double * k)()
+    rel = (C.c_double * k)()
+    sys.ctx.bind()
+    call("fame_rayleigh_ritz", sys.h, sys.mass.h, _ptr(Y), k, lam, rel)
+    return np.array(lam[:]), np.array(rel[:])
 
 
 def solve_batch(Ns, materials, qs, P, nev=10, tol=1e-8, maxiter=30, p=40, tolCG=1e-10,

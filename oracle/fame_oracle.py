@@ -64,7 +64,7 @@ __all__ = [
     "mass_adjoint_quadratic", "set_fft_workers", "apply_cropped_A", "yee_material",
     "separable_conv3_same", "compute_lwrq", "compute_yee_lwrq_metrics",
     "apply_K_original", "apply_shift_preconditioner", "minres", "osi_top_apply",
-    "dense_original_operators", "dense_original_gevp",
+    "dense_original_operators", "dense_original_gevp", "apply_Kr_exact", "rayleigh_ritz_Kr",
 ]
 
 
@@ -253,6 +253,11 @@ class MassOp:
     def full(self, U):  # Mop: 3NF -> 3NF, component-first
         n = self.NF
         return np.concatenate([self.scalar(U[k * n:(k + 1) * n]) for k in range(3)])
+
+    def inverse_scalar(self, x):
+        """M^{-1} x = fftn(ifftn(x) ./ E): on the (2N)^6 grid the convolution of
+        exp1/applyMij_fft.m:11 is diagonal in real space, so its inverse is exact."""
+        return applyMij_fft(x, 1.0 / self.E, self.N)
 
 
 # ---------------------------------------------------------------------------
@@ -723,6 +728,34 @@ def solve_modes(S, nev=10, p=40, tol=1e-8, maxRestart=30, tolCG=1e-10, seed=2026
     order = np.argsort(lam, kind="stable")
     return dict(lam=lam[order], Y=Y[:, order], theta=theta[order], steps=steps,
                 info=info, stats=getStats())
+
+
+def apply_Kr_exact(y, S):
+    """K_r y = V^* M^{-1} V y (exp1/make_nested_krinv_instrumented.m:4-13) with the exact
+    grid inverse of the mass instead of the inner PCG on M."""
+    n = S.NF
+    v = apply_V_blockdiag(y, S)
+    w = np.concatenate([S.mass.inverse_scalar(v[c * n:(c + 1) * n]) for c in range(3)])
+    return apply_VH_blockdiag(w, S)
+
+
+def rayleigh_ritz_Kr(Y, S):
+    """Rayleigh-Ritz refinement of approximate eigenvectors Y (2NF x k) of K_r with the
+    exact K_r (no reference counterpart; the reference reports 1/theta of the Lanczos
+    Ritz values, exp2/Lanczos.m:140-147).  Returns (lam ascending, Y refined, relres)."""
+    Y = np.asarray(Y, dtype=np.complex128)
+    Z = np.stack([apply_Kr_exact(Y[:, j], S) for j in range(Y.shape[1])], axis=1)
+    G = Y.conj().T @ Z
+    B = Y.conj().T @ Y
+    G = 0.5 * (G + G.conj().T)
+    B = 0.5 * (B + B.conj().T)
+    L = np.linalg.cholesky(B)
+    Li = np.linalg.inv(L)
+    lam, U = np.linalg.eigh(Li @ G @ Li.conj().T)
+    R = Li.conj().T @ U
+    Yr, Zr = Y @ R, Z @ R
+    relres = np.linalg.norm(Zr - Yr * lam, axis=0) / np.linalg.norm(Zr, axis=0)
+    return lam, Yr, relres
 
 
 def dense_reduced_operator(S):

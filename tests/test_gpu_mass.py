@@ -152,3 +152,12 @@ def test_cached_device_memory_reuse_and_trim(cuda_device):
     assert L.lib.fame_device_trim_memory(cuda_device.index or 0) == 0
     m = F.MassBackend(E, N)
     assert np.array_equal(m.MscalarOp(x).cpu().numpy(), outs[0])
+    # the library keeps its own pool: the device's default pool keeps its release threshold
+    try:
+        from cuda.bindings import runtime as rt
+    except ImportError:
+        from cuda import cudart as rt
+    err, pool = rt.cudaDeviceGetDefaultMemPool(cuda_device.index or 0)
+    assert int(err) == 0
+    err, thr = rt.cudaMemPoolGetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrReleaseThreshold)
+    assert int(err) == 0 and int(thr) == 0

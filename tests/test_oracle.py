@@ -110,6 +110,39 @@ def test_dense_eigs_n1():
     assert np.max(np.abs(sol["lam"] - lam_dense) / lam_dense) < 1e-10
 
 
+def test_exact_grid_inverse_and_Kr_n1():
+    """M^{-1} as the chain on 1/eps inverts the mass exactly, and the exact K_r matches
+    the dense V^* M^{-1} V at N=1."""
+    N = 1
+    S = O.build_q_system(N, P_GOLD, (0.05, 0.04, 0.03), O.material_separable_cos(N))
+    x = O.start_vector(3, S.NF)
+    assert _rel(S.mass.inverse_scalar(S.mass.scalar(x)), x) < 1e-14
+    K = O.dense_reduced_operator(S)
+    y = O.start_vector(4, S.nr)
+    assert _rel(O.apply_Kr_exact(y, S), K @ y) < 1e-12
+
+
+def test_rayleigh_ritz_removes_the_inner_tolerance_error_n2():
+    """Ritz vectors of a Lanczos run on a loose K_r^{-1} (tolCG 1e-8: eigenvalues off by
+    ~1e-8) refined with the exact K_r agree with a refined tight solve (tolCG 1e-13) to
+    1e-10 (the refined error is quadratic in the eigenvector error); at N=1 the refined
+    values equal a dense eigensolve of K_r."""
+    N = 2
+    S = O.build_q_system(N, P_GOLD, (0.05, 0.04, 0.03), O.material_separable_cos(N))
+    sol_t = O.solve_modes(S, nev=10, p=40, tol=1e-8, tolCG=1e-13)
+    tight = O.rayleigh_ritz_Kr(sol_t["Y"], S)[0]
+    sol = O.solve_modes(S, nev=10, p=40, tol=1e-8, tolCG=1e-8)
+    raw = np.max(np.abs(np.sort(sol["lam"]) - tight) / tight)
+    lam, Yr, relres = O.rayleigh_ritz_Kr(sol["Y"], S)
+    assert np.max(np.abs(lam - tight) / tight) < 1e-10 < 1e-9 < raw
+    assert np.max(np.abs(np.sort(sol_t["lam"]) - tight) / tight) < 1e-11
+    assert np.all(relres < 1e-4)
+    S1 = O.build_q_system(1, P_GOLD, (0.05, 0.04, 0.03), O.material_separable_cos(1))
+    lam_dense = np.sort(np.linalg.eigvalsh(O.dense_reduced_operator(S1)))[:10]
+    lam1 = O.rayleigh_ritz_Kr(O.solve_modes(S1, nev=10, p=40, tol=1e-8, tolCG=1e-10)["Y"], S1)[0]
+    assert np.max(np.abs(lam1 - lam_dense) / lam_dense) < 1e-12
+
+
 def test_explicit_equals_nested_n1():
     """exp1/smoke_test_rank1_lowmem.m:29-39 spirit: two K_r^{-1} realisations agree."""
     N = 1
@@ -275,3 +308,13 @@ def test_recovered_eigenvectors_solve_the_original_gevp_n1():
         assert abs(np.vdot(x, M3 @ x) - 1.0) < 1e-10
         r = np.linalg.norm(K @ x - lam * (M3 @ x)) / (np.linalg.norm(K @ x) + lam * np.linalg.norm(M3 @ x))
         assert r < 1e-9, (j, r)
+
+
+def test_workload_constants_agree_with_the_product():
+    """The checker's copy of the benchmark inputs equals the product's (fame_b200.configs)."""
+    import fame_b200 as F
+    from oracle import workloads as W
+    np.testing.assert_array_equal(W.P_GOLDEN, F.configs.P_GOLDEN)
+    np.testing.assert_array_equal(W.P_REFERENCE, F.configs.P_REFERENCE)
+    assert W.Q_PHYS == F.configs.Q_PHYS and W.Q_TRACKING == F.configs.Q_TRACKING
+    assert W.SEED == F.configs.SEED and W.SOLVE == F.configs.SOLVE
