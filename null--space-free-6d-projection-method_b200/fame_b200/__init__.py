@@ -14,3 +14,4 @@ from .recon import *  # noqa: F401,F403
 from . import grad  # noqa: F401
 from .method_a import *  # noqa: F401,F403
 from . import autotune  # noqa: F401
+from . import results  # noqa: F401
