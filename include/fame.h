@@ -97,6 +97,14 @@ FAME_API int fame_mass_destroy(fame_mass* m);
 /* mode: FAME_MASS_*; prec: FAME_F64 / FAME_F32 (x,y complex128 / complex64) */
 FAME_API int fame_mass_apply(fame_mass* m, int mode, const void* x, void* y, int nrhs, int prec);
 
+/* (No reference counterpart) fault-path self-test of the bounded device-side waits: runs
+ * pass B of the FP32 chain with every stage barrier armed for bytes that no copy delivers
+ * (no copy is issued), so each CTA's wait runs out after poll_limit polls (1..2^20), sets
+ * the device's fault word and returns.  Returns what the next synchronisation reports:
+ * FAME_ERR_CUDA when the timeout was detected (the expected outcome); the fault word is
+ * cleared and the context stays usable.  The mass handle's scratch field is overwritten. */
+FAME_API int fame_selftest_bounded_wait(fame_mass* m, unsigned poll_limit);
+
 /* Replaces applyMij_rank1_exact(x,kernelFFT,plan) — exp1/applyMij_rank1_exact.m:1-6
  * with rank1_exact_fft_scatter / rank1_exact_ifft_gather
  * (exp1/rank1_exact_fft_scatter.m:1-13, exp1/rank1_exact_ifft_gather.m:1-11).

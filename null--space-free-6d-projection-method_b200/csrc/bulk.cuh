@@ -48,10 +48,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
 }
 
 // Bounded wait for the phase with the given parity to complete: false after
-// ~2^22 polls (well above any legitimate copy latency), so that a copy that
-// never lands ends the kernel with an error flag instead of a hang.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
-  for (unsigned i = 0; i < (1u << 22); ++i) {
+// `limit` polls (default ~2^22, well above any legitimate copy latency), so that a
+// copy that never lands ends the kernel with an error flag instead of a hang.
+constexpr unsigned kMbarPollLimit = 1u << 22;
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsigned limit = kMbarPollLimit) {
+  for (unsigned i = 0; i < limit; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
     if (i >= 8) __nanosleep(64);
   }

@@ -222,6 +222,30 @@ int fame_mass_destroy(fame_mass* m) {
   return FAME_OK;
 }
 
+int fame_selftest_bounded_wait(fame_mass* m, unsigned poll_limit) {
+  if (!m) return fail(FAME_ERR_INVALID, "fame_selftest_bounded_wait: mass is NULL");
+  if (poll_limit < 1 || poll_limit > (1u << 20)) return fail(FAME_ERR_INVALID, "poll_limit must be in [1, 2^20]");
+  fame_ctx* ctx = m->ctx;
+  FAME_TRY(check_fault(ctx));  // start from a clear fault word
+  // one FP32 field in the handle's scratch (8 NF bytes of its 16 NF); every stage barrier
+  // expects bytes that no copy delivers, so each CTA's first wait runs out and returns
+  float2* w = reinterpret_cast<float2*>(m->work);
+  const Gate g{nullptr};
+  int s = FAME_OK;
+  switch (m->n) {
+    case 2: s = launch_passB_pk<2>(w, 1, m->Et32, m->NF, ctx->stream, g, poll_limit, 1); break;
+    case 4: s = launch_passB_pk<4>(w, 1, m->Et32, m->NF, ctx->stream, g, poll_limit, 1); break;
+    case 6: s = launch_passB_pk<6>(w, 1, m->Et32, m->NF, ctx->stream, g, poll_limit, 1); break;
+    case 8: s = launch_passB_pk<8>(w, 1, m->Et32, m->NF, ctx->stream, g, poll_limit, 1); break;
+    case 10: s = launch_passB_pk<10>(w, 1, m->Et32, m->NF, ctx->stream, g, poll_limit, 1); break;
+    case 12: s = launch_passB_pk<12>(w, 1, m->Et32, m->NF, ctx->stream, g, poll_limit, 1); break;
+    default: s = launch_passB_pk<14>(w, 1, m->Et32, m->NF, ctx->stream, g, poll_limit, 1); break;
+  }
+  FAME_TRY(s);
+  FAME_CUDA_TRY(cudaGetLastError());
+  return check_fault(ctx);  // FAME_ERR_CUDA: the timeout was detected and reported
+}
+
 int fame_mass_apply(fame_mass* m, int mode, const void* x, void* y, int nrhs, int prec) {
   if (!m || !x || !y || nrhs < 0) return fail(FAME_ERR_INVALID, "fame_mass_apply arguments");
   if (prec == FAME_F64) return mass_apply_typed<double>(m, mode, (const double2*)x, (double2*)y, nrhs);

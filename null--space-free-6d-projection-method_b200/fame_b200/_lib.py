@@ -78,6 +78,7 @@ SIGNATURES = {
     "fame_mass_create": [P, I, P, C.POINTER(P)],
     "fame_mass_destroy": [P],
     "fame_mass_apply": [P, I, P, P, I, I],
+    "fame_selftest_bounded_wait": [P, C.c_uint],
     "fame_applyMij_rank1_exact": [P, P, P, LL, P, P, I],
     "fame_apply_V_blockdiag": [P, P, P, P, P, P, P, P, LL, I, P],
     "fame_apply_VH_blockdiag": [P, P, P, P, P, P, P, P, LL, I, P],

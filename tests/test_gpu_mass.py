@@ -161,3 +161,24 @@ def test_cached_device_memory_reuse_and_trim(cuda_device):
     assert int(err) == 0
     err, thr = rt.cudaMemPoolGetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrReleaseThreshold)
     assert int(err) == 0 and int(thr) == 0
+
+
+@pytest.mark.parametrize("N", [2, 5])
+def test_bounded_wait_timeout_is_reported(cuda_device, N):
+    """The bounded mbarrier wait of pass B runs out (stage barriers armed for bytes that no
+    copy delivers; nothing is in flight), every CTA sets the fault word and returns, the host
+    reports FAME_ERR_CUDA at the next synchronisation, and the context stays usable: a mass
+    action afterwards matches the oracle."""
+    import fame_b200 as F
+    from fame_b200 import _lib as L
+    E = O.material_separable_cos(N, 12.0)
+    m = F.MassBackend(torch.as_tensor(E, device=cuda_device), N)
+    m.ctx.bind()
+    st = L.lib.fame_selftest_bounded_wait(m.h, 4096)
+    assert st == 2 and b"bounded device-side wait" in L.lib.fame_last_error()
+    x = O.start_vector(12, (2 * N) ** 6)
+    for dtype, tol in ((torch.complex128, 1e-13), (torch.complex64, 2e-6)):
+        y = m.MscalarOp(torch.as_tensor(x, device=cuda_device).to(dtype)).cpu().numpy().astype(np.complex128)
+        ref = O.applyMij_fft(x.astype(np.complex64).astype(np.complex128) if dtype == torch.complex64 else x, E, N)
+        assert np.linalg.norm(y - ref) / np.linalg.norm(ref) < tol
+    m.ctx.sync()  # nothing left on the fault word
