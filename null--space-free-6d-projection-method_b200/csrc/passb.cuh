@@ -5,9 +5,11 @@
 // Persistent kernel: each CTA owns a contiguous range of units (tile k,
 // field f) and streams them through two shared-memory stages.  One thread
 // pulls a unit with n bulk copies (one per i6-plane, completed on the stage's
-// mbarrier) plus, at the first unit of a tile, the material tile; the copy of
-// unit i+2 is issued as soon as unit i has been read out of its stage, so
-// global latency overlaps the transforms of the next unit.  In shared memory
+// mbarrier); the copy of unit i+2 is issued as soon as unit i has been read out
+// of its stage, so global latency overlaps the transforms of the next unit.  The
+// material values of a thread's axis-5 line are read from global memory (L2) in
+// that phase, which keeps the shared memory of a CTA to its two stages.  This
+// generic kernel runs the FP64 chains; FP32 uses k_passB_pk below.  In shared memory
 // element (t, i4, i5, i6) of a unit sits at t + TT*i4 + P5*i5 + P6*i6 with
 // P5 = TT*n and P6 = TT*n^2 + TT (one padding row per plane); each phase
 // transforms one line per thread in place:
@@ -36,40 +38,38 @@ template <int n, typename T> struct PassBGeom {
   static constexpr int tile = TT * n3;     // elements per tile (global)
   static constexpr unsigned plane_bytes = (unsigned)(TT * n2 * sizeof(C<T>));
   static constexpr int threads = (L + 31) / 32 * 32;
+  // registers per thread: three CTAs of 7 warps per SM at n = 10 (21 x 32 x 96 <= 65536)
+  static constexpr int max_regs = n == 10 ? 96 : 255;
   static_assert((P6 * sizeof(C<T>)) % 16 == 0 && (stage * sizeof(C<T>)) % 16 == 0, "bulk-copy alignment");
   static_assert(plane_bytes % 16 == 0, "bulk-copy size");
   template <typename TE> static constexpr size_t smem_bytes() {
-    return 2 * stage * sizeof(C<T>) + 2 * (size_t)tile * sizeof(TE) + 2 * sizeof(uint64_t);
+    return 2 * stage * sizeof(C<T>) + 2 * sizeof(uint64_t);
   }
 };
 
 template <int n, typename T, typename TE>
-__global__ void __launch_bounds__(512) k_passB(C<T>* __restrict__ work, const TE* __restrict__ Et, int nfields,
+__global__ void __launch_bounds__(512) __maxnreg__((PassBGeom<n, T>::max_regs))
+    k_passB(C<T>* __restrict__ work, const TE* __restrict__ Et, int nfields,
                                               long long NF, Gate gate, unsigned* fault) {
   if (gate.off()) return;
   using G = PassBGeom<n, T>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   C<T>* stg = reinterpret_cast<C<T>*>(smem_raw);
-  TE* es = reinterpret_cast<TE*>(smem_raw + 2 * G::stage * sizeof(C<T>));
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * G::stage * sizeof(C<T>) + 2 * G::tile * sizeof(TE));
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * G::stage * sizeof(C<T>));
   constexpr int tiles = G::n3 / G::TT;
   const int U = tiles * nfields;
   const int u0 = (int)((long long)blockIdx.x * U / gridDim.x);
   const int u1 = (int)((long long)(blockIdx.x + 1) * U / gridDim.x);
   if (u0 >= u1) return;
-  const int k0 = u0 / nfields;
   const int tid = threadIdx.x;
 
   auto issue = [&](int u, int s) {
     const int k = u / nfields, f = u - k * nfields;
-    const bool needE = (u == u0) || (f == 0);
-    mbar_arrive_expect_tx(&bar[s], n * G::plane_bytes + (needE ? (unsigned)(G::tile * sizeof(TE)) : 0u));
+    mbar_arrive_expect_tx(&bar[s], n * G::plane_bytes);
     const C<T>* src = work + (long long)f * NF + (long long)k * G::tile;
     C<T>* dst = stg + s * G::stage;
 #pragma unroll 1
     for (int p = 0; p < n; ++p) bulk_g2s(dst + p * G::P6, src + p * G::TT * G::n2, G::plane_bytes, &bar[s]);
-    if (needE)
-      bulk_g2s(es + ((k - k0) & 1) * G::tile, Et + (long long)k * G::tile, (unsigned)(G::tile * sizeof(TE)), &bar[s]);
   };
 
   if (tid == 0) {
@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(512) k_passB(C<T>* __restrict__ work, const TE
     }
     C<T>* S = stg + s * G::stage;
     const int k = u / nfields, f = u - k * nfields;
-    const TE* E = es + ((k - k0) & 1) * G::tile;
+    const TE* E = Et + (long long)k * G::tile;  // material tile, read from L2 in the axis-5 phase
     if (act) line_dft<n, +1, T>(S + b1, G::TT);
     __syncthreads();
     if (act) line_dft<n, +1, T>(S + b2, G::P6);
@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(512) k_passB(C<T>* __restrict__ work, const TE
       Dft<n, +1, T>::run(re, im);
 #pragma unroll
       for (int j = 0; j < n; ++j) {
-        const T e = (T)E[j * G::L + tid];
+        const T e = (T)__ldg(E + j * G::L + tid);
         re[j] *= e;
         im[j] *= e;
       }

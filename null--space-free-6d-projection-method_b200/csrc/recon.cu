@@ -375,6 +375,31 @@ namespace fame {
 // Multi-center Taylor reconstruction (exp2/taylor_on_blocks_exp3.m:1-97); the block
 // moments either in FP64 on the CUDA cores or as 3xTF32 products on the tensor cores
 // (taylor_tc.cu).
+// Whether the nB centers (x, y, z per block) form a tensor grid in block order
+// b = i + m1 (j + m2 k) with axis values X[i], Y[j], Z[k] (exact equality); on success
+// grid.m1..m3 are set and ax = [X, Y, Z].
+static bool tensor_grid_of(const std::vector<double>& c, int nB, TaylorTcGrid& grid, std::vector<double>& ax) {
+  int m1 = 1, m2 = 1;
+  while (m1 < nB && c[3 * m1 + 1] == c[1] && c[3 * m1 + 2] == c[2]) ++m1;
+  while (m1 * m2 < nB && c[3 * (m1 * m2) + 2] == c[2]) ++m2;
+  if (nB % (m1 * m2) != 0) return false;
+  const int m3 = nB / (m1 * m2);
+  if (m1 + m2 + m3 > kTaylorTcMaxAxis) return false;
+  for (int b = 0; b < nB; ++b) {
+    const int i = b % m1, j = (b / m1) % m2, k = b / (m1 * m2);
+    if (c[3 * b] != c[3 * i] || c[3 * b + 1] != c[3 * (m1 * j) + 1] || c[3 * b + 2] != c[3 * (m1 * m2 * k) + 2])
+      return false;
+  }
+  ax.clear();
+  for (int i = 0; i < m1; ++i) ax.push_back(c[3 * i]);
+  for (int j = 0; j < m2; ++j) ax.push_back(c[3 * (m1 * j) + 1]);
+  for (int k = 0; k < m3; ++k) ax.push_back(c[3 * (m1 * m2 * k) + 2]);
+  grid.m1 = m1;
+  grid.m2 = m2;
+  grid.m3 = m3;
+  return true;
+}
+
 static int taylor_impl(fame_ctx* ctx, const void* coeff, const double* qModes, long long NF, const double* rPoints,
                        long long M, int p, const long long* blockPtr, const long long* blockIds, int nBlocks,
                        const double* fixedCenter, void* u, bool tc) {
@@ -406,7 +431,7 @@ static int taylor_impl(fame_ctx* ctx, const void* coeff, const double* qModes, l
   cudaStream_t s = ctx->stream;
   int *dal, *dpk;
   double2 *dcf, *partial, *gamma;
-  double *centers, *dfix;
+  double *centers, *dfix, *dax;
   float* tout;
   auto carve = [&](Carve& cv) {
     dal = cv.take<int>(al.size());
@@ -416,6 +441,7 @@ static int taylor_impl(fame_ctx* ctx, const void* coeff, const double* qModes, l
     gamma = cv.take<double2>((size_t)nBlocks * L);
     centers = cv.take<double>((size_t)nBlocks * 3);
     dfix = cv.take<double>(3);
+    dax = cv.take<double>(kTaylorTcMaxAxis);
     tout = cv.take<float>(tc ? tp.out_floats : 1);
   };
   Carve size_only;
@@ -441,7 +467,18 @@ static int taylor_impl(fame_ctx* ctx, const void* coeff, const double* qModes, l
       ::fame::count_launch();
     } else {
       cudaMemcpyAsync(dpk, packed.data(), packed.size() * sizeof(int), cudaMemcpyHostToDevice, s);
-      st = taylor_moments_tc(tp, s, (const double2*)coeff, qModes, NF, centers, nBlocks, dpk, L, p, dcf, tout, gamma);
+      // centers on a tensor grid (the Yee block partition's are): the moment kernel then
+      // factorises the phases per axis
+      TaylorTcGrid grid;
+      std::vector<double> hc((size_t)nBlocks * 3), hax;
+      if (cudaMemcpyAsync(hc.data(), centers, hc.size() * sizeof(double), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+          cudaStreamSynchronize(s) == cudaSuccess && tensor_grid_of(hc, nBlocks, grid, hax)) {
+        cudaMemcpyAsync(dax, hax.data(), hax.size() * sizeof(double), cudaMemcpyHostToDevice, s);
+        grid.ax = dax;
+      }
+      cudaGetLastError();
+      st = taylor_moments_tc(tp, s, (const double2*)coeff, qModes, NF, centers, nBlocks, dpk, L, p, dcf, tout, gamma,
+                             grid);
     }
     // one grid column per block; x-extent covers the largest block
     std::vector<long long> hp(nBlocks + 1);

@@ -3,19 +3,27 @@
 // gamma[b, a] = coef[a] * sum_j c_j exp(i q_j . r_b) q_j^a
 // (exp2/taylor_on_blocks_exp3.m:53-54,65-73: the moment GEMM Qalpha^T (c .* phase)).
 //
-// One CTA owns a slice of Kc modes and a tile of 64 block centers.  Per stage of
-// 32 modes its threads write into shared memory, in the 128-byte swizzled
-// K-major UMMA layout and split into TF32 head + tail (3xTF32):
-//   A (128 x 32): rows 2b, 2b+1 = Re, Im of c_j exp(i q_j . r_b)   (FP64 phase, FP32 sincosf)
-//   B (Npad x 32): row a = qx^a1 qy^a2 qz^a3                          (FP64 products)
-// Fifteen generator warps fill a stage and arrive on its "full" mbarrier; a
-// sixteenth warp waits for it and issues tcgen05.mma kind::tf32 for
-// Ahi*Bhi + Ahi*Blo + Alo*Bhi into one FP32 TMEM accumulator of 128 lanes x Npad
-// columns, committing to the stage's "empty" mbarrier, while the generators fill
-// the other stage (two stages when they fit).  The slice's partial moments
-// go to HBM (FP32) and a second kernel sums the slices in FP64 in a fixed order.
-// Neither Qalpha (L x NF) nor the phase matrix ever exists in HBM: the kernel reads
-// 40 bytes per mode.
+// One CTA owns a slice of Kc modes, a tile of 64 block centers and Nc of the
+// monomial columns (the columns are split over two CTAs when 2 Nc would exceed the
+// 512 TMEM columns).  Per stage of 32 modes its threads write into shared memory, in
+// the 128-byte swizzled K-major UMMA layout and split into TF32 head + tail (3xTF32):
+//   A (128 x 32): rows 2b, 2b+1 = Re, Im of c_j exp(i q_j . r_b)
+//   B (Nc x 32):  row a = qx^a1 qy^a2 qz^a3                           (FP64 products)
+// When the block centers form a tensor grid (the Yee block partition does), the
+// phase factorises per axis, exp(i q.r_b) = ex(bx) ey(by) ez(bz): the generators
+// first tabulate the m1 + m2 + m3 axis phases of the stage's 32 modes in shared
+// memory (3m sincosf per mode instead of m^3), then combine them with two complex
+// products per center; otherwise each center's phase is reduced in FP64 and taken
+// by sincosf.  Fifteen generator warps fill a stage and arrive on its "full"
+// mbarrier; a sixteenth warp waits for it and issues tcgen05.mma kind::tf32 with
+// Ahi*Bhi into one FP32 TMEM accumulator (columns [0, Nc)) and Ahi*Blo + Alo*Bhi into
+// a second one (columns [Nc, 2 Nc)): the tensor cores round each FP32 accumulation
+// toward zero, and keeping the 2^-11 smaller cross products apart leaves the large
+// head*head sum with a third of the roundings.  It commits to the stage's "empty"
+// mbarrier while the generators fill the other stage.  The epilogue adds the two
+// accumulators and writes the slice's partial moments (FP32); a second kernel sums
+// the slices in FP64 in a fixed order.  Neither Qalpha (L x NF) nor the phase matrix
+// ever exists in HBM: the kernel reads 40 bytes per mode.
 #include "internal.cuh"
 #include "umma.cuh"
 
@@ -31,20 +39,20 @@ constexpr int kBPW = (kBT + kGenWarps - 1) / kGenWarps;  // block centers per ge
 constexpr int kBlockCost = 3;  // generation cost of one block center (Re, Im rows) in monomial rows
 constexpr int kPmax = 12;
 constexpr int kLmax = 512;
-// Modes per slice accumulated in one FP32 TMEM accumulator at most.  The tensor
-// cores round that accumulation toward zero, so its error grows with the slice;
-// measured on eigenmode 10 at N = 5 (p = 10, 64 centers), field error vs the FP64
-// moments: 2048 modes 6.2e-6, 1024 3.4e-6, 512 2.4e-6, 256 1.3e-6, at 1.00 / 1.07 /
-// 1.15 / 1.35 times the time of 2048.
+// Modes per slice accumulated in one FP32 TMEM accumulator at most (the tensor cores'
+// toward-zero rounding of that accumulation sets the error of the moments).
 constexpr long long kKcMax = 512;
 constexpr uint32_t kABytes = 128u * 128u;  // one TF32 part of the phase operand
+constexpr int kMaxAxis = kTaylorTcMaxAxis;
 
-__host__ __device__ inline uint32_t b_bytes(int Npad) { return (uint32_t)Npad * 128u; }
-__host__ __device__ inline uint32_t stage_bytes(int Npad) { return 2u * (kABytes + b_bytes(Npad)); }
-constexpr size_t kTailBytes = kBT * 3 * sizeof(double)               // centers
-                              + kLmax * sizeof(int)                    // packed multi-indices
-                              + 5 * sizeof(uint64_t) + 16;             // mbarriers, TMEM slot, abort flag
-inline size_t tc_smem(int Npad, int stages) { return 1024 + (size_t)stages * stage_bytes(Npad) + kTailBytes; }
+__host__ __device__ inline uint32_t b_bytes(int Nc) { return (uint32_t)Nc * 128u; }
+__host__ __device__ inline uint32_t stage_bytes(int Nc) { return 2u * (kABytes + b_bytes(Nc)); }
+constexpr size_t kTailBytes = kBT * 3 * sizeof(double)                 // centers
+                              + kLmax * sizeof(int)                      // packed multi-indices
+                              + 2 * kMaxAxis * kKC * sizeof(float2)      // axis phase tables (two stages)
+                              + kMaxAxis * sizeof(double)                // axis center values
+                              + 5 * sizeof(uint64_t) + 16;               // mbarriers, TMEM slot, abort flag
+inline size_t tc_smem(int Nc, int stages) { return 1024 + (size_t)stages * stage_bytes(Nc) + kTailBytes; }
 
 struct TcArgs {
   const double* Q;      // 3 x NF (rows qx, qy, qz)
@@ -53,23 +61,38 @@ struct TcArgs {
   const double* centers;  // nB x 3
   int nB;
   const int* alist;     // L packed multi-indices a1 | a2 << 8 | a3 << 16
-  int L, p, Npad, stages;
+  int L, p, Npad, Nc, stages;
   long long Kc;
   float* out;           // [slice][tile][128][Npad]
+  const double* ax;     // tensor-grid centers (or nullptr)
+  int m1, m2, m3;
 };
 
 __device__ __forceinline__ void put(unsigned char* base, int row, int k, float v) {
   *reinterpret_cast<float*>(base + umma::sw128_offset(row, k)) = v;
 }
 
+// exp(i th) in FP32 with th reduced to [-pi, pi] in FP64 first
+__device__ __forceinline__ float2 cis(double th) {
+  const double tr = fma(-rint(th * 0.15915494309189535), 6.283185307179586, th);
+  float sf, cf;
+  sincosf((float)tr, &sf, &cf);
+  return make_float2(cf, sf);
+}
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+
 __global__ void __launch_bounds__(kThreads, 1) k_taylor_moments_tc(TcArgs a, unsigned* fault) {
   extern __shared__ unsigned char smraw[];
   unsigned char* sm = smraw + ((1024u - (smem_u32(smraw) & 1023u)) & 1023u);
-  const int Npad = a.Npad, S = a.stages;
-  const uint32_t bB = b_bytes(Npad), stB = stage_bytes(Npad);
+  const int Nc = a.Nc, S = a.stages;
+  const uint32_t bB = b_bytes(Nc), stB = stage_bytes(Nc);
   double* cen = reinterpret_cast<double*>(sm + (size_t)S * stB);  // [kBT][3]
   int* al = reinterpret_cast<int*>(cen + kBT * 3);                  // [kLmax]
-  uint64_t* full = reinterpret_cast<uint64_t*>(al + kLmax);         // [2]: stage written
+  float2* tab = reinterpret_cast<float2*>(al + kLmax);              // [2][kMaxAxis][kKC]
+  double* axv = reinterpret_cast<double*>(tab + 2 * kMaxAxis * kKC);  // [kMaxAxis]
+  uint64_t* full = reinterpret_cast<uint64_t*>(axv + kMaxAxis);     // [2]: stage written
   uint64_t* empty = full + 2;                                       // [2]: stage read by the MMAs
   uint64_t* done = full + 4;                                        // every MMA complete
   uint32_t* slot = reinterpret_cast<uint32_t*>(full + 5);
@@ -78,13 +101,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_taylor_moments_tc(TcArgs a, uns
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const long long z = blockIdx.x;
   const int bt = blockIdx.y;
+  const int c0 = blockIdx.z * Nc;  // first monomial column of this CTA
   const long long j0 = z * a.Kc, j1 = j0 + a.Kc < a.NF ? j0 + a.Kc : a.NF;
   const int nch = (int)((j1 - j0 + kKC - 1) / kKC);
   const int nbl = a.nB - bt * kBT < kBT ? a.nB - bt * kBT : kBT;
-  const uint32_t ncols = Npad <= 32 ? 32u : Npad <= 64 ? 64u : Npad <= 128 ? 128u : Npad <= 256 ? 256u : 512u;
+  const bool factored = a.ax != nullptr;
+  const int nax = factored ? a.m1 + a.m2 + a.m3 : 0;
+  const uint32_t need = 2u * (uint32_t)Nc;
+  const uint32_t ncols = need <= 32 ? 32u : need <= 64 ? 64u : need <= 128 ? 128u : need <= 256 ? 256u : 512u;
 
   for (int t = tid; t < a.L; t += kThreads) al[t] = a.alist[t];
   for (int t = tid; t < kBT * 3; t += kThreads) cen[t] = t / 3 < nbl ? a.centers[(long long)bt * kBT * 3 + t] : 0.0;
+  for (int t = tid; t < nax; t += kThreads) axv[t] = a.ax[t];
   if (tid == 0) {
     for (int s = 0; s < 2; ++s) {
       mbar_init(&full[s], kGenThreads);
@@ -104,28 +132,35 @@ __global__ void __launch_bounds__(kThreads, 1) k_taylor_moments_tc(TcArgs a, uns
   const uint32_t tmem = *slot;
 
   if (warp < kGenWarps) {
-    // block centers bl = warp + u * kGenWarps are this warp's; monomial rows [r0, r1) too,
-    // sized so that every warp gets the same share of (kBlockCost * blocks + rows)
+    // block centers bl = warp + u * kGenWarps are this warp's; monomial rows [r0, r1) of the
+    // CTA's Nc columns too, sized so that every warp gets the same share of
+    // (kBlockCost * blocks + rows)
     auto row_start = [&](int w) {
-      const int total = kBlockCost * kBT + Npad;
+      const int total = kBlockCost * kBT + Nc;
       int rs = 0;
       for (int v = 1; v <= w; ++v) {
         const int blocksBefore = v < kBT % kGenWarps ? v * kBPW : (kBT % kGenWarps) * kBPW + (v - kBT % kGenWarps) * (kBPW - 1);
         int t = (v * total + kGenWarps / 2) / kGenWarps - kBlockCost * blocksBefore;
         t = t < rs ? rs : t;
-        rs = t < Npad ? t : Npad;
+        rs = t < Nc ? t : Nc;
       }
-      return w >= kGenWarps ? Npad : rs;
+      return w >= kGenWarps ? Nc : rs;
     };
     const int r0 = row_start(warp), r1 = row_start(warp + 1);
-    const int e0 = r0 < a.L ? al[r0] : 0;
+    const int e0 = c0 + r0 < a.L ? al[c0 + r0] : 0;
     double cx[kBPW], cy[kBPW], cz[kBPW];
+    int tx[kBPW], ty[kBPW], tz[kBPW];  // axis-table rows of the centers (factorised phases)
 #pragma unroll
     for (int u = 0; u < kBPW; ++u) {
       const int bl = warp + u * kGenWarps;
       cx[u] = bl < kBT ? cen[3 * bl] : 0.0;
       cy[u] = bl < kBT ? cen[3 * bl + 1] : 0.0;
       cz[u] = bl < kBT ? cen[3 * bl + 2] : 0.0;
+      const int b = bt * kBT + bl;
+      tx[u] = factored ? b % a.m1 : 0;
+      ty[u] = factored ? a.m1 + (b / a.m1) % a.m2 : 0;
+      tz[u] = factored ? a.m1 + a.m2 + b / (a.m1 * a.m2) : 0;
+      if (!(bl < nbl)) tx[u] = ty[u] = tz[u] = 0;
     }
     // this lane's mode of the next stage, loaded one stage ahead
     double nqx = 0.0, nqy = 0.0, nqz = 0.0;
@@ -153,37 +188,47 @@ __global__ void __launch_bounds__(kThreads, 1) k_taylor_moments_tc(TcArgs a, uns
       bool ok = !*abortf;
       if (ok && i >= S) ok = mbar_wait(&empty[s], (unsigned)((i / S - 1) & 1));
       if (!ok) *abortf = 1;
+      float2* tb = tab + (i & 1) * kMaxAxis * kKC;
+      if (factored) {
+        // axis phases of this stage's modes: entry e (x values, then y, then z) for lane's mode;
+        // thread (warp, lane) fills entries warp, warp + 15, ... (every generator warp takes part
+        // in the barrier below on every stage, so the tables of stage i are complete before use
+        // and the other buffer's readers of stage i - 1 are done before stage i + 1 writes it)
+        for (int e = warp; e < nax; e += kGenWarps) {
+          const double qc = e < a.m1 ? qx : e < a.m1 + a.m2 ? qy : qz;
+          tb[e * kKC + lane] = cis(qc * axv[e]);
+        }
+        asm volatile("bar.sync 1, %0;" ::"n"(kGenThreads) : "memory");
+      }
       if (ok) {
         // A: rows 2 bl, 2 bl + 1 = Re, Im of c_j exp(i q_j . r_bl)
         unsigned char* Ahi = stg;
         unsigned char* Alo = stg + kABytes;
-        // c_j e^{i theta} in FP32: the phase reduced to [-pi, pi] in FP64, then sincosf; the
-        // products carry an absolute error ~2^-23 |c_j|, below the 2^-22 of the TF32 split
-        const float cr = (float)cj.x, ci = (float)cj.y;
+        // c_j e^{i theta} in FP32: the products carry an absolute error ~2^-23 |c_j|, below
+        // the 2^-22 of the TF32 split
+        const float2 cf = make_float2((float)cj.x, (float)cj.y);
 #pragma unroll
         for (int u = 0; u < kBPW; ++u) {
           const int bl = warp + u * kGenWarps;
           if (bl < kBT) {
-            float wr = 0.0f, wi = 0.0f;
+            float2 w = make_float2(0.0f, 0.0f);
             if (in && bl < nbl) {
-              const double th = qx * cx[u] + qy * cy[u] + qz * cz[u];
-              const double tr = fma(-rint(th * 0.15915494309189535), 6.283185307179586, th);
-              float sf, cf;
-              sincosf((float)tr, &sf, &cf);
-              wr = fmaf(cr, cf, -ci * sf);
-              wi = fmaf(cr, sf, ci * cf);
+              const float2 ph = factored ? cmulf(cmulf(tb[tx[u] * kKC + lane], tb[ty[u] * kKC + lane]),
+                                                 tb[tz[u] * kKC + lane])
+                                         : cis(qx * cx[u] + qy * cy[u] + qz * cz[u]);
+              w = cmulf(cf, ph);
             }
             float h, l;
-            umma::tf32_split_f32(wr, h, l);
+            umma::tf32_split_f32(w.x, h, l);
             put(Ahi, 2 * bl, lane, h);
             put(Alo, 2 * bl, lane, l);
-            umma::tf32_split_f32(wi, h, l);
+            umma::tf32_split_f32(w.y, h, l);
             put(Ahi, 2 * bl + 1, lane, h);
             put(Alo, 2 * bl + 1, lane, l);
           }
         }
-        // B: row r = qx^a1 qy^a2 qz^a3 for the r-th multi-index (a1 outer, a3 inner), one
-        // multiplication per row; zero rows past L and for modes past the slice
+        // B: local row r = column c0 + r: qx^a1 qy^a2 qz^a3 for that multi-index (a1 outer,
+        // a3 inner), one multiplication per row; zero rows past L and for modes past the slice
         unsigned char* Bhi = stg + 2 * kABytes;
         unsigned char* Blo = Bhi + bB;
         const int a1 = e0 & 255, a2 = (e0 >> 8) & 255, a3 = e0 >> 16;
@@ -194,7 +239,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_taylor_moments_tc(TcArgs a, uns
         double m = t12;
         for (int k = 0; k < a3; ++k) m *= qz;
         int left1 = a.p - a1, left2 = left1 - a2, left3 = left2 - a3;  // steps left on each axis
-        const int rL = r1 < a.L ? r1 : a.L;
+        const int rL = r1 < a.L - c0 ? r1 : a.L - c0;
         for (int r = r0; r < rL; ++r) {
           float h, l;
           umma::tf32_split_f32((float)m, h, l);
@@ -224,8 +269,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_taylor_moments_tc(TcArgs a, uns
     }
   } else {
     // MMA warp: wait for each stage, issue its 3xTF32 products, release it on completion
-    const int N0 = Npad < 256 ? Npad : 256, N1 = Npad - N0;
-    const uint32_t id0 = umma::idesc_tf32(128, N0), id1 = umma::idesc_tf32(128, N1 > 0 ? N1 : 16);
+    const uint32_t id = umma::idesc_tf32(128, Nc);
     for (int i = 0; i < nch; ++i) {
       const int s = i % S;
       const bool ok = !*abortf && mbar_wait(&full[s], (unsigned)((i / S) & 1));
@@ -236,14 +280,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_taylor_moments_tc(TcArgs a, uns
       umma::fence_after_sync();
       if (lane == 0) {
         const uint32_t sa = smem_u32(sm + (size_t)s * stB);
-        for (int kk = 0; kk < kKC / 8; ++kk)
-          for (int pr = 0; pr < 3; ++pr) {  // hi*hi, hi*lo, lo*hi
-            const uint64_t ad = umma::desc_kmajor_sw128(sa + (pr == 2 ? kABytes : 0u) + kk * 32u);
-            const uint32_t bo = sa + 2u * kABytes + (pr == 1 ? bB : 0u) + kk * 32u;
-            const uint32_t acc = (i | kk | pr) != 0 ? 1u : 0u;
-            umma::mma_tf32(tmem, ad, umma::desc_kmajor_sw128(bo), id0, acc);
-            if (N1 > 0) umma::mma_tf32(tmem + 256u, ad, umma::desc_kmajor_sw128(bo + 256u * 128u), id1, acc);
-          }
+        for (int kk = 0; kk < kKC / 8; ++kk) {
+          const uint64_t ahi = umma::desc_kmajor_sw128(sa + kk * 32u);
+          const uint64_t alo = umma::desc_kmajor_sw128(sa + kABytes + kk * 32u);
+          const uint64_t bhi = umma::desc_kmajor_sw128(sa + 2u * kABytes + kk * 32u);
+          const uint64_t blo = umma::desc_kmajor_sw128(sa + 2u * kABytes + bB + kk * 32u);
+          const uint32_t acc = (i | kk) != 0 ? 1u : 0u;
+          umma::mma_tf32(tmem, ahi, bhi, id, acc);                    // head * head
+          umma::mma_tf32(tmem + (uint32_t)Nc, ahi, blo, id, acc);     // cross products
+          umma::mma_tf32(tmem + (uint32_t)Nc, alo, bhi, id, 1u);
+        }
         umma::commit(&empty[s]);
       }
       __syncwarp();
@@ -251,22 +297,25 @@ __global__ void __launch_bounds__(kThreads, 1) k_taylor_moments_tc(TcArgs a, uns
     if (lane == 0) umma::commit(done);  // arrives once every MMA issued above has completed
     __syncwarp();
   }
-  // every thread: the accumulator is final (or the pipeline gave up)
+  // every thread: the accumulators are final (or the pipeline gave up)
   const bool fin = mbar_wait(done, 0u);
   const bool ok = __syncthreads_and(fin && !*abortf);
-  if (ok) {  // all 16 warps: warp w reads lanes 32 (w % 4), column blocks w / 4 + 4 t
+  if (ok) {  // all 16 warps: warp w reads lanes 32 (w % 4), 16-column blocks w / 4 + 4 t
     umma::fence_after_sync();
-    const int q = warp & 3;  // a warp reads TMEM lanes 32 (warp % 4) ...
-    float* orow = a.out + (((long long)z * gridDim.y + bt) * 128 + q * 32 + lane) * (long long)Npad;
-    for (int cc = warp >> 2; cc < Npad / 32; cc += (kGenWarps + 1) / 4) {
-      uint32_t r[32];
-      umma::ld_32x32b_x32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(cc * 32), r);
-      umma::wait_ld(r);
-      float4* o = reinterpret_cast<float4*>(orow + cc * 32);
+    const int q = warp & 3;
+    const uint32_t lane_base = (uint32_t)(q * 32) << 16;
+    float* orow = a.out + (((long long)z * gridDim.y + bt) * 128 + q * 32 + lane) * (long long)a.Npad + c0;
+    for (int cb = warp >> 2; cb < Nc / 16; cb += (kGenWarps + 1) / 4) {
+      uint32_t hh[16], cr[16];
+      umma::ld_32x32b_x16_wait(tmem + lane_base + (uint32_t)(cb * 16), hh);
+      umma::ld_32x32b_x16_wait(tmem + lane_base + (uint32_t)(Nc + cb * 16), cr);
+      float4* o = reinterpret_cast<float4*>(orow + cb * 16);
 #pragma unroll
-      for (int u = 0; u < 8; ++u)
-        o[u] = make_float4(__uint_as_float(r[4 * u]), __uint_as_float(r[4 * u + 1]), __uint_as_float(r[4 * u + 2]),
-                           __uint_as_float(r[4 * u + 3]));
+      for (int u = 0; u < 4; ++u)
+        o[u] = make_float4(__uint_as_float(hh[4 * u]) + __uint_as_float(cr[4 * u]),
+                           __uint_as_float(hh[4 * u + 1]) + __uint_as_float(cr[4 * u + 1]),
+                           __uint_as_float(hh[4 * u + 2]) + __uint_as_float(cr[4 * u + 2]),
+                           __uint_as_float(hh[4 * u + 3]) + __uint_as_float(cr[4 * u + 3]));
     }
   } else if (!ok && tid == 0 && fault) {
     atomicOr(fault, 1u);
@@ -312,12 +361,15 @@ __global__ void k_taylor_tc_finish(const double* __restrict__ part, int groups, 
 TaylorTcPlan taylor_tc_plan(long long NF, int nB, int L) {
   TaylorTcPlan pl{};
   pl.Npad = std::max(32, (L + 31) / 32 * 32);
-  pl.stages = tc_smem(pl.Npad, 2) <= 227 * 1024 ? 2 : 1;
-  pl.smem = tc_smem(pl.Npad, pl.stages);
+  pl.nsplit = 2 * pl.Npad > 512 ? 2 : 1;  // head*head and cross accumulators: 2 Nc <= 512 TMEM columns
+  pl.Nc = pl.Npad / pl.nsplit;             // a multiple of 16
+  pl.stages = tc_smem(pl.Nc, 2) <= 227 * 1024 ? 2 : 1;
+  pl.smem = tc_smem(pl.Nc, pl.stages);
   pl.ntiles = (nB + kBT - 1) / kBT;
   const long long sms = num_sms() > 0 ? num_sms() : 148;
-  const long long waves = std::max<long long>(1, (NF * pl.ntiles + sms * kKcMax - 1) / (sms * kKcMax));
-  const long long want = std::max<long long>(1, (waves * sms + pl.ntiles - 1) / pl.ntiles);
+  const long long per_slice = (long long)pl.ntiles * pl.nsplit;  // CTAs per mode slice
+  const long long waves = std::max<long long>(1, (NF * per_slice + sms * kKcMax - 1) / (sms * kKcMax));
+  const long long want = std::max<long long>(1, (waves * sms + per_slice - 1) / per_slice);
   pl.Kc = std::max<long long>(kKC, ((NF + want - 1) / want + kKC - 1) / kKC * kKC);
   pl.nslices = (NF + pl.Kc - 1) / pl.Kc;
   const size_t per = (size_t)pl.ntiles * 128 * pl.Npad;
@@ -328,9 +380,12 @@ TaylorTcPlan taylor_tc_plan(long long NF, int nB, int L) {
 
 int taylor_moments_tc(const TaylorTcPlan& pl, cudaStream_t s, const double2* c, const double* Q, long long NF,
                       const double* centers, int nB, const int* alistPacked, int L, int p, const double2* coef,
-                      float* out, double2* gamma) {
-  if (L > kLmax || L > pl.Npad || p > kPmax || pl.Npad > 512 || pl.smem > 227 * 1024)
+                      float* out, double2* gamma, const TaylorTcGrid& grid) {
+  if (L > kLmax || L > pl.Npad || p > kPmax || pl.Nc > 256 || pl.Nc % 16 != 0 || pl.smem > 227 * 1024)
     return fail(FAME_ERR_UNSUPPORTED, "tensor-core Taylor moments: order too high");
+  if (grid.ax && (grid.m1 < 1 || grid.m2 < 1 || grid.m3 < 1 || grid.m1 * grid.m2 * grid.m3 != nB ||
+                  grid.m1 + grid.m2 + grid.m3 > kMaxAxis))
+    return fail(FAME_ERR_INVALID, "tensor-core Taylor moments: bad center grid");
   static int attr = [] {
     return cudaFuncSetAttribute(k_taylor_moments_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) ==
                    cudaSuccess
@@ -338,9 +393,10 @@ int taylor_moments_tc(const TaylorTcPlan& pl, cudaStream_t s, const double2* c, 
                : FAME_ERR_CUDA;
   }();
   if (attr != FAME_OK) return fail(attr, "tensor-core Taylor moments: shared-memory limit");
-  TcArgs a{Q, c, NF, centers, nB, alistPacked, L, p, pl.Npad, pl.stages, pl.Kc, out};
-  dim3 grid((unsigned)pl.nslices, (unsigned)pl.ntiles);
-  k_taylor_moments_tc<<<grid, kThreads, pl.smem, s>>>(a, fault_word());
+  TcArgs a{Q, c, NF, centers, nB, alistPacked, L, p, pl.Npad, pl.Nc, pl.stages, pl.Kc, out,
+           grid.ax, grid.m1, grid.m2, grid.m3};
+  dim3 g3((unsigned)pl.nslices, (unsigned)pl.ntiles, (unsigned)pl.nsplit);
+  k_taylor_moments_tc<<<g3, kThreads, pl.smem, s>>>(a, fault_word());
   ::fame::count_launch();
   const long long per = (long long)pl.ntiles * 128 * pl.Npad;
   double* part = reinterpret_cast<double*>(out + pl.nslices * per);

@@ -19,7 +19,7 @@ from ._lib import call
 from .core import MassBackend, build_q_system, make_explicit_krinv_compact, start_vector, Lanczos, _ptr
 from .recon import recover_original_eigenvectors
 
-__all__ = ["mass_adjoint", "eigenpairs", "EigenvalueFunction", "eigenvalue_gradients"]
+__all__ = ["mass_adjoint", "eigenpairs", "EigenvalueFunction", "eigenvalue_gradients", "modes_per_chunk"]
 
 
 def mass_adjoint(mass: MassBackend, X, dEps):
@@ -50,24 +50,65 @@ def eigenpairs(N, theta, P=None, q=None, nev=10, p=40, tol=1e-8, tolCG=1e-10, pr
     return lam[order], Y[:, order.tolist()], sysq, mass, grads, info
 
 
-def eigenvalue_gradients(N, theta, **kw):
-    """(lambda, d lambda / d theta) for the 10 smallest eigenvalues (theta = (delta, a_1..a_6))."""
+def modes_per_chunk(NF, nev, device_bytes=None, device=None):
+    """Eigenvectors recovered (and their adjoint terms evaluated) together: each mode holds
+    X and M X (3 NF complex128 each) plus the recovery's PCG vectors (~6 NF complex128);
+    with ``device_bytes`` (default: half of the device's free memory) fewer modes than
+    ``nev`` are recovered at a time when they do not fit, the rest recomputed chunk by chunk."""
+    per_mode = 12 * NF * 16
+    if device_bytes is None:
+        free, _ = torch.cuda.mem_get_info(device)
+        device_bytes = free // 2
+    return int(max(1, min(nev, device_bytes // per_mode)))
+
+
+def eigenvalue_gradients(N, theta, chunk=None, device_bytes=None, **kw):
+    """(lambda, d lambda / d theta) for the smallest eigenvalues (theta = (delta, a_1..a_6)).
+
+    Only the Ritz vectors Y (2NF x nev) are kept from the solve (the Krylov basis is
+    released); the original eigenvectors x_j = M^{-1} V y_j are recovered ``chunk`` modes
+    at a time (default: as many as fit in ``device_bytes``, see modes_per_chunk) and
+    discarded after their adjoint terms are taken, so the gradient's memory does not grow
+    with nev."""
     lam, Y, sysq, mass, grads, _ = eigenpairs(N, theta, **kw)
-    X, MX, _ = recover_original_eigenvectors(Y, sysq, 1e-12, 3000)
-    quad = mass_adjoint(mass, X, grads)
+    nev = Y.shape[1]
+    chunk = chunk or modes_per_chunk(sysq.NF, nev, device_bytes)
+    quad = np.zeros((nev, len(grads)))
+    for j0 in range(0, nev, chunk):
+        cols = list(range(j0, min(nev, j0 + chunk)))
+        X, MX, _ = recover_original_eigenvectors(Y[:, cols].contiguous(), sysq, 1e-12, 3000)
+        quad[cols] = mass_adjoint(mass, X, grads)
+        del X, MX
     return lam, -lam[:, None] * quad
 
 
 class EigenvalueFunction(torch.autograd.Function):
-    """lambda(theta) with a Hellmann-Feynman backward pass (theta: float64 CPU tensor of 7)."""
+    """lambda(theta) with a Hellmann-Feynman backward pass (theta: float64 CPU tensor of 7).
+
+    ``kw`` are eigenvalue_gradients' keywords; with ``recompute=True`` in it, forward keeps
+    only theta and lambda and backward repeats the solve (deterministic: the same start
+    vector gives the same eigenvectors) to rebuild the eigenvectors, instead of holding
+    any solver state between the two passes."""
 
     @staticmethod
     def forward(ctx, theta, N, kw):
-        lam, dlam = eigenvalue_gradients(N, theta.detach().cpu().numpy(), **(kw or {}))
-        ctx.save_for_backward(torch.as_tensor(dlam))
+        kw = dict(kw or {})
+        recompute = kw.pop("recompute", False)
+        th = theta.detach().cpu().numpy()
+        if recompute:
+            lam = eigenpairs(N, th, **{k: v for k, v in kw.items() if k not in ("chunk", "device_bytes")})[0]
+            ctx.N, ctx.kw = N, kw
+            ctx.save_for_backward(theta.detach().clone())
+            ctx.dlam = None
+        else:
+            lam, dlam = eigenvalue_gradients(N, th, **kw)
+            ctx.dlam = torch.as_tensor(dlam)
         return torch.as_tensor(lam, dtype=torch.float64)
 
     @staticmethod
     def backward(ctx, grad_lam):
-        (dlam,) = ctx.saved_tensors
+        dlam = ctx.dlam
+        if dlam is None:
+            (theta,) = ctx.saved_tensors
+            dlam = torch.as_tensor(eigenvalue_gradients(ctx.N, theta.cpu().numpy(), **ctx.kw)[1])
         return grad_lam.to(dlam.dtype) @ dlam, None, None

@@ -127,6 +127,14 @@ def test_eigenvalue_gradients_fd_and_autograd(cuda_device):
     lam_t = F.grad.EigenvalueFunction.apply(th, N, kw)
     lam_t.sum().backward()
     np.testing.assert_allclose(th.grad.numpy(), dl.sum(0), rtol=1e-12)
+    # eigenvectors recovered one mode at a time (as under a small memory budget) and the
+    # recompute form (backward repeats the solve) give the same gradients
+    _, dl1 = F.grad.eigenvalue_gradients(N, theta, chunk=1, **kw)
+    np.testing.assert_allclose(dl1, dl, rtol=1e-12, atol=1e-15)
+    assert F.grad.modes_per_chunk((2 * N) ** 6, 4, device_bytes=12 * 16 * (2 * N) ** 6 * 2) == 2
+    th2 = torch.tensor(theta, dtype=torch.float64, requires_grad=True)
+    F.grad.EigenvalueFunction.apply(th2, N, dict(kw, recompute=True)).sum().backward()
+    np.testing.assert_allclose(th2.grad.numpy(), dl.sum(0), rtol=1e-12)
 
 
 def test_batched_bloch_path_matches_single_solves(cuda_device):
@@ -162,3 +170,27 @@ def test_taylor_3xtf32_tensor_cores_vs_fp64(cuda_device, N, p, nb):
     assert rel(utc, u64) < 4e-6, rel(utc, u64)
     utc2 = F.taylor_on_blocks(c, Q, pts[1], p, blocks, tensor_cores=True).cpu().numpy()
     assert np.array_equal(utc, utc2)  # deterministic
+
+
+def test_taylor_3xtf32_general_centers(cuda_device):
+    """Blocks in a permuted order: the centers are no longer a tensor grid in block order, so
+    the tensor-core moments take each center's phase by sincosf instead of the per-axis
+    factorisation; both give the FP64 form's field (and each other's) to the same bound."""
+    F, S, sg, m = _sys(2, cuda_device)
+    Q = F.build_projected_q_modes(sg)
+    c = torch.as_tensor(O.start_vector(14, S.NF), device=cuda_device)
+    pts, axes, sz = F.build_yee_points(6, 0.0125)
+    ptr, ids = F.build_yee_block_partition(sz, 3)
+    hp, hi = ptr.cpu().numpy(), ids.cpu().numpy()
+    perm = np.random.default_rng(3).permutation(len(hp) - 1)
+    nptr, nids = [0], []
+    for b in perm:
+        nids.append(hi[hp[b]:hp[b + 1]])
+        nptr.append(nptr[-1] + hp[b + 1] - hp[b])
+    pblocks = (torch.as_tensor(np.asarray(nptr, dtype=np.int64), device=cuda_device),
+               torch.as_tensor(np.concatenate(nids).astype(np.int64), device=cuda_device))
+    for p in (6, 10):
+        u64 = F.taylor_on_blocks(c, Q, pts[1], p, pblocks).cpu().numpy()
+        ugen = F.taylor_on_blocks(c, Q, pts[1], p, pblocks, tensor_cores=True).cpu().numpy()
+        ugrid = F.taylor_on_blocks(c, Q, pts[1], p, (ptr, ids), tensor_cores=True).cpu().numpy()
+        assert rel(ugen, u64) < 4e-6 and rel(ugrid, u64) < 4e-6, (rel(ugen, u64), rel(ugrid, u64))
