@@ -261,6 +261,15 @@ FAME_API int fame_reconstruct_direct_grid(fame_basis* b, const void* coeff, cons
 FAME_API int fame_reconstruct_direct_grid_3xtf32(fame_basis* b, const void* coeff, const double* xs, int nx,
                                                  const double* ys, int ny, const double* zs, int nz,
                                                  void* u);
+/* The factorised direct sum for ncomp (1..3) field components at once: coeff component-
+ * stacked (ncomp x NF), xs/ys/zs the components' axes stacked (ncomp x nx, ...; equal sizes,
+ * as the three staggered Yee plus-grids have), u component-stacked (ncomp x nx ny nz).  The
+ * three GEMMs run as single launches batched over the components (the reference
+ * reconstructs the components one after another, exp2/reconstruct_three_components_exp3.m);
+ * tensor_cores != 0 runs them as split-FP32 (3xTF32) tcgen05 products. */
+FAME_API int fame_reconstruct_direct_grid_fields(fame_basis* b, const void* coeff, int ncomp, const double* xs,
+                                                 int nx, const double* ys, int ny, const double* zs, int nz,
+                                                 int tensor_cores, void* u);
 /* exp2/taylor_on_blocks_exp3.m:8-79 (multi-center Taylor, order p <= 12).  Blocks in
  * CSR form: point indices blockIds[blockPtr[b] .. blockPtr[b+1]) (0-based, device);
  * fixedCenter: host 3-vector or NULL (then each block's bounding-box midpoint). */

@@ -95,7 +95,7 @@ int taylor_moments_tc(const TaylorTcPlan& plan, cudaStream_t s, const double2* c
 // (3xTF32) tcgen05 products (zgemm_tc.cu).
 int zgemm_3xtf32(const double2* A, const double2* B, double2* C, int M, int N, int K, long long sam, long long sak,
                  long long sbk, long long sbn, long long scm, long long scn, long long bA, long long bB, long long bC,
-                 int batch, cudaStream_t s);
+                 int batch, cudaStream_t s, int bdivB = 1);
 // A Hermitian operator on n-vectors of complex128 for the restarted Lanczos
 // (lanczos.cu): y = A x on ctx's stream; *ws holds the reusable basis workspace.
 struct LanczosOperator {

@@ -97,13 +97,14 @@ struct GemmArgs {
   int M, N, K;
   long long sam, sak, sbk, sbn, scm, scn;
   long long bA, bB, bC;  // batch strides (blockIdx.z)
+  int bdivB = 1;         // B advances by bB every bdivB batch entries
 };
 constexpr int kGT = 32, kGK = 16;
 __global__ void __launch_bounds__(256) k_zgemm(GemmArgs g) {
   __shared__ double2 As[kGK][kGT + 1];
   __shared__ double2 Bs[kGK][kGT + 1];
   const double2* A = g.A + g.bA * blockIdx.z;
-  const double2* B = g.B + g.bB * blockIdx.z;
+  const double2* B = g.B + g.bB * (blockIdx.z / g.bdivB);
   double2* Cm = g.C + g.bC * blockIdx.z;
   const int m0 = blockIdx.x * kGT, n0 = blockIdx.y * kGT;
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;  // 16 x 16 threads, 2 x 2 outputs each
@@ -300,9 +301,13 @@ int fame_reconstruct_direct(fame_ctx* ctx, const void* coeff, const double* qMod
   return FAME_OK;
 }
 
-static int direct_grid_impl(fame_basis* bs, const void* coeff, const double* xs, int nx, const double* ys, int ny,
-                            const double* zs, int nz, void* u, bool tc) {
-  if (!bs || !coeff || !xs || !ys || !zs || !u || nx <= 0 || ny <= 0 || nz <= 0)
+// The factorised direct sum for ncomp components at once (component-stacked coeff, axes
+// and u; equal grid sizes): each of the three GEMMs is one launch batched over the
+// components (and, for the second, over its contraction slices), so the launches are
+// ncomp times larger.  No host synchronisation: the results are ordered on the stream.
+static int direct_grid_impl(fame_basis* bs, const void* coeff, int ncomp, const double* xs, int nx, const double* ys,
+                            int ny, const double* zs, int nz, void* u, bool tc) {
+  if (!bs || !coeff || !xs || !ys || !zs || !u || nx <= 0 || ny <= 0 || nz <= 0 || ncomp < 1 || ncomp > 3)
     return fail(FAME_ERR_INVALID, "reconstruct_direct_grid arguments");
   const double* P = bs->P;  // column-major 6 x 3
   for (int l = 0; l < 6; ++l)
@@ -311,15 +316,17 @@ static int direct_grid_impl(fame_basis* bs, const void* coeff, const double* xs,
         return fail(FAME_ERR_UNSUPPORTED, "factorised reconstruction needs an axis-block cut matrix [diag; diag]");
   const int N = bs->N, n = 2 * N;
   const long long n2 = (long long)n * n, NF = bs->NF;
+  if ((long long)ncomp * n2 > 65535) return fail(FAME_ERR_UNSUPPORTED, "reconstruct_direct_grid: too many slices");
   cudaStream_t s = bs->ctx->stream;
-  // workspace pieces: phase tables, permuted coefficients, two GEMM intermediates
+  // workspace pieces (per component, consecutive): phase tables, permuted coefficients,
+  // two GEMM intermediates
   auto carve = [&](Carve& cv, double2** Tx, double2** Ty, double2** Tz, double2** Cp, double2** T1, double2** T2) {
-    *Tx = cv.take<double2>((size_t)nx * n2);
-    *Ty = cv.take<double2>((size_t)ny * n2);
-    *Tz = cv.take<double2>((size_t)nz * n2);
-    *Cp = cv.take<double2>((size_t)NF);
-    *T1 = cv.take<double2>((size_t)nx * n2 * n2);
-    *T2 = cv.take<double2>((size_t)nx * ny * n2);
+    *Tx = cv.take<double2>((size_t)ncomp * nx * n2);
+    *Ty = cv.take<double2>((size_t)ncomp * ny * n2);
+    *Tz = cv.take<double2>((size_t)ncomp * nz * n2);
+    *Cp = cv.take<double2>((size_t)ncomp * NF);
+    *T1 = cv.take<double2>((size_t)ncomp * nx * n2 * n2);
+    *T2 = cv.take<double2>((size_t)ncomp * nx * ny * n2);
   };
   double2 *Tx, *Ty, *Tz, *Cp, *T1, *T2;
   Carve size_only;
@@ -331,41 +338,51 @@ static int direct_grid_impl(fame_basis* bs, const void* coeff, const double* xs,
   carve(cv, &Tx, &Ty, &Tz, &Cp, &T1, &T2);
   const double* k = bs->info.kLift;
   if (st == FAME_OK) {
-    k_phase_table<<<rblocks((long long)nx * n2), 256, 0, s>>>(xs, nx, N, P[0], k[0], P[3], k[3], Tx);
-    ::fame::count_launch();
-    k_phase_table<<<rblocks((long long)ny * n2), 256, 0, s>>>(ys, ny, N, P[6 + 1], k[1], P[6 + 4], k[4], Ty);
-    ::fame::count_launch();
-    k_phase_table<<<rblocks((long long)nz * n2), 256, 0, s>>>(zs, nz, N, P[12 + 2], k[2], P[12 + 5], k[5], Tz);
-    ::fame::count_launch();
-    k_pair_permute<<<rblocks(NF), 256, 0, s>>>((const double2*)coeff, n, Cp);
-    ::fame::count_launch();
-    // T1[x, (b,c)] = sum_a Tx[x, a] Cp[a, (b,c)]
-    GemmArgs g1{Tx, Cp, T1, nx, (int)(n2 * n2), (int)n2, 1, nx, 1, n2, 1, nx, 0, 0, 0};
-    // T2[x, y, c] = sum_b T1[x, b, c] Ty[y, b]   (batched over c)
-    GemmArgs g2{T1, Ty, T2, nx, ny, (int)n2, 1, nx, ny, 1, 1, nx, (long long)nx * n2, 0, (long long)nx * ny};
-    // u[(x,y), z] = sum_c T2[(x,y), c] Tz[z, c]
-    GemmArgs g3{T2, Tz, (double2*)u, nx * ny, nz, (int)n2, 1, (long long)nx * ny, nz, 1, 1, (long long)nx * ny, 0, 0, 0};
+    for (int c = 0; c < ncomp; ++c) {
+      k_phase_table<<<rblocks((long long)nx * n2), 256, 0, s>>>(xs + (long long)c * nx, nx, N, P[0], k[0], P[3], k[3],
+                                                                Tx + (long long)c * nx * n2);
+      k_phase_table<<<rblocks((long long)ny * n2), 256, 0, s>>>(ys + (long long)c * ny, ny, N, P[6 + 1], k[1], P[6 + 4],
+                                                                k[4], Ty + (long long)c * ny * n2);
+      k_phase_table<<<rblocks((long long)nz * n2), 256, 0, s>>>(zs + (long long)c * nz, nz, N, P[12 + 2], k[2],
+                                                                P[12 + 5], k[5], Tz + (long long)c * nz * n2);
+      k_pair_permute<<<rblocks(NF), 256, 0, s>>>((const double2*)coeff + (long long)c * NF, n, Cp + (long long)c * NF);
+      ::fame::count_launch(4);
+    }
+    // T1[x, (b,c)] = sum_a Tx[x, a] Cp[a, (b,c)]                   (batched over components)
+    GemmArgs g1{Tx, Cp, T1, nx, (int)(n2 * n2), (int)n2, 1, nx, 1, n2, 1, nx,
+                (long long)nx * n2, NF, (long long)nx * n2 * n2};
+    // T2[x, y, c] = sum_b T1[x, b, c] Ty[y, b]   (batched over components x c; Ty per component)
+    GemmArgs g2{T1, Ty, T2, nx, ny, (int)n2, 1, nx, ny, 1, 1, nx, (long long)nx * n2, (long long)ny * n2,
+                (long long)nx * ny, (int)n2};
+    // u[(x,y), z] = sum_c T2[(x,y), c] Tz[z, c]                    (batched over components)
+    GemmArgs g3{T2, Tz, (double2*)u, nx * ny, nz, (int)n2, 1, (long long)nx * ny, nz, 1, 1, (long long)nx * ny,
+                (long long)nx * ny * n2, (long long)nz * n2, (long long)nx * ny * nz};
     const GemmArgs* gs[3] = {&g1, &g2, &g3};
-    const int batches[3] = {1, (int)n2, 1};
+    const int batches[3] = {ncomp, (int)(ncomp * n2), ncomp};
     for (int t = 0; t < 3 && st == FAME_OK; ++t) {
       const GemmArgs& g = *gs[t];
       st = tc ? zgemm_3xtf32(g.A, g.B, g.C, g.M, g.N, g.K, g.sam, g.sak, g.sbk, g.sbn, g.scm, g.scn, g.bA, g.bB, g.bC,
-                             batches[t], s)
+                             batches[t], s, g.bdivB)
               : zgemm(g, batches[t], s);
     }
-    if (st == FAME_OK) st = cudaStreamSynchronize(s) == cudaSuccess ? FAME_OK : fail(FAME_ERR_CUDA, "sync");
   }
   return st;
 }
 
 int fame_reconstruct_direct_grid(fame_basis* bs, const void* coeff, const double* xs, int nx, const double* ys, int ny,
                                  const double* zs, int nz, void* u) {
-  return direct_grid_impl(bs, coeff, xs, nx, ys, ny, zs, nz, u, false);
+  return direct_grid_impl(bs, coeff, 1, xs, nx, ys, ny, zs, nz, u, false);
 }
 
 int fame_reconstruct_direct_grid_3xtf32(fame_basis* bs, const void* coeff, const double* xs, int nx, const double* ys,
                                         int ny, const double* zs, int nz, void* u) {
-  return direct_grid_impl(bs, coeff, xs, nx, ys, ny, zs, nz, u, true);
+  return direct_grid_impl(bs, coeff, 1, xs, nx, ys, ny, zs, nz, u, true);
+}
+
+int fame_reconstruct_direct_grid_fields(fame_basis* bs, const void* coeff, int ncomp, const double* xs, int nx,
+                                        const double* ys, int ny, const double* zs, int nz, int tensor_cores,
+                                        void* u) {
+  return direct_grid_impl(bs, coeff, ncomp, xs, nx, ys, ny, zs, nz, u, tensor_cores != 0);
 }
 
 }  // extern "C"

@@ -39,6 +39,7 @@ struct ZgArgs {
   int M, N, K, Nt;
   long long sam, sak, sbk, sbn, scm, scn;
   long long bA, bB, bC;
+  int bdivB;  // B advances by bB every bdivB batch entries
 };
 
 __device__ __forceinline__ void put2(unsigned char* base, int row, int k, float x, float y) {
@@ -59,7 +60,7 @@ __global__ void __launch_bounds__(kZThreads, 1) k_zgemm_3xtf32(ZgArgs g, unsigne
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * kZM, n0 = blockIdx.y * Nt;
   const double2* A = g.A + g.bA * blockIdx.z;
-  const double2* B = g.B + g.bB * blockIdx.z;
+  const double2* B = g.B + g.bB * (blockIdx.z / g.bdivB);
   double2* Cm = g.C + g.bC * blockIdx.z;
   const int nch = (g.K + kZKC - 1) / kZKC;
   const uint32_t ncols = 2 * Nt <= 32 ? 32u : 2 * Nt <= 64 ? 64u : 2 * Nt <= 128 ? 128u : 2 * Nt <= 256 ? 256u : 512u;
@@ -191,7 +192,7 @@ __global__ void __launch_bounds__(kZThreads, 1) k_zgemm_3xtf32(ZgArgs g, unsigne
 
 int zgemm_3xtf32(const double2* A, const double2* B, double2* C, int M, int N, int K, long long sam, long long sak,
                  long long sbk, long long sbn, long long scm, long long scn, long long bA, long long bB, long long bC,
-                 int batch, cudaStream_t s) {
+                 int batch, cudaStream_t s, int bdivB) {
   if (M <= 0 || N <= 0 || K <= 0 || batch <= 0) return fail(FAME_ERR_INVALID, "zgemm_3xtf32: empty shape");
   const int Nt = std::min(256, (N + 31) / 32 * 32);
   const size_t smem = zsmem(Nt);
@@ -204,7 +205,8 @@ int zgemm_3xtf32(const double2* A, const double2* B, double2* C, int M, int N, i
   if (attr != FAME_OK) return fail(attr, "zgemm_3xtf32: shared-memory limit");
   const long long gy = (N + Nt - 1) / Nt;
   if (gy > 65535 || batch > 65535) return fail(FAME_ERR_UNSUPPORTED, "zgemm_3xtf32: grid too large");
-  ZgArgs g{A, B, C, M, N, K, Nt, sam, sak, sbk, sbn, scm, scn, bA, bB, bC};
+  if (bdivB < 1) return fail(FAME_ERR_INVALID, "zgemm_3xtf32: batch divisor");
+  ZgArgs g{A, B, C, M, N, K, Nt, sam, sak, sbk, sbn, scm, scn, bA, bB, bC, bdivB};
   dim3 grid((unsigned)((M + kZM - 1) / kZM), (unsigned)gy, (unsigned)batch);
   k_zgemm_3xtf32<<<grid, kZThreads, smem, s>>>(g, fault_word());
   ::fame::count_launch();

@@ -111,6 +111,7 @@ SIGNATURES = {
     "fame_reconstruct_direct": [P, P, P, LL, P, LL, P],
     "fame_reconstruct_direct_grid": [P, P, P, I, P, I, P, I, P],
     "fame_reconstruct_direct_grid_3xtf32": [P, P, P, I, P, I, P, I, P],
+    "fame_reconstruct_direct_grid_fields": [P, P, I, P, I, P, I, P, I, I, P],
     "fame_taylor_on_blocks": [P, P, P, LL, P, LL, I, P, P, I, C.POINTER(D), P],
     "fame_taylor_on_blocks_3xtf32": [P, P, P, LL, P, LL, I, P, P, I, C.POINTER(D), P],
     "fame_mass_adjoint": [P, P, I, P, I, C.POINTER(D)],

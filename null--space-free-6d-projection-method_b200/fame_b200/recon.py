@@ -11,7 +11,7 @@ from . import _lib as L
 from ._lib import FameError, call
 from .core import QSystem, _ptr, default_context
 
-__all__ = ["compute_yee_lwrq_metrics", "recover_original_eigenvectors", "compute_fourier_diagnostics", "build_projected_q_modes",
+__all__ = ["compute_yee_lwrq_metrics", "reconstruct_fields_direct_grid", "recover_original_eigenvectors", "compute_fourier_diagnostics", "build_projected_q_modes",
            "build_yee_points", "build_yee_block_partition", "reconstruct_field_direct_blocked",
            "reconstruct_field_direct_grid", "taylor_on_blocks", "reconstruct_field_taylor_multi",
            "reconstruct_field_taylor_single", "reconstruct_three_components"]
@@ -142,6 +142,28 @@ def reconstruct_field_direct_grid(coeff, sys: QSystem, axes, tensor_cores=False)
     call("fame_reconstruct_direct_grid_3xtf32" if tensor_cores else "fame_reconstruct_direct_grid", sys.h, _ptr(c),
          _ptr(xs), xs.numel(), _ptr(ys), ys.numel(), _ptr(zs), zs.numel(), _ptr(u))
     return u
+
+
+def reconstruct_fields_direct_grid(coeff, sys: QSystem, axes_list, tensor_cores=False):
+    """The factorised direct sum for several field components in one call (each GEMM one
+    launch over all components; exp2/reconstruct_three_components_exp3.m reconstructs them
+    one after another).  ``coeff``: the component-stacked coefficients (ncomp x NF, e.g. a
+    recovered 3NF eigenvector); ``axes_list``: per component (xs, ys, zs) of equal sizes.
+    Returns one field per component (views of one buffer)."""
+    nc = len(axes_list)
+    xs = torch.cat([a[0] for a in axes_list]).contiguous()
+    ys = torch.cat([a[1] for a in axes_list]).contiguous()
+    zs = torch.cat([a[2] for a in axes_list]).contiguous()
+    nx, ny, nz = (axes_list[0][d].numel() for d in range(3))
+    c = coeff.reshape(-1).contiguous()
+    if c.numel() != nc * sys.NF:
+        raise ValueError("coeff must hold ncomp x NF coefficients")
+    M = nx * ny * nz
+    u = torch.empty(nc * M, dtype=torch.complex128, device=c.device)
+    sys.ctx.bind()
+    call("fame_reconstruct_direct_grid_fields", sys.h, _ptr(c), nc, _ptr(xs), nx, _ptr(ys), ny, _ptr(zs), nz,
+         int(bool(tensor_cores)), _ptr(u))
+    return [u[i * M:(i + 1) * M] for i in range(nc)]
 
 
 def taylor_on_blocks(coeff, qModes, rPoints, p, blocks, fixedCenter=None, ctx=None, tensor_cores=False):
