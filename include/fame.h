@@ -206,6 +206,9 @@ typedef struct {
                              material 1/eps, C^{-1} B^H (I3 (x) M^{-1}) B C^{-1}; the stopping
                              test stays ||b - Mhat u|| <= tolCG ||b|| (1).  0: plain CG as the
                              reference's pcg(Mhat, ...) in exp1/make_explicit_krinv_compact.m:43 */
+  int passColumns; /* columns per CTA of the inner solves' pass A/C kernels: 0 = built-in default;
+                      alternatives 1, 4 (2N = 10), 2, 4 (2N = 8), 4, 6 (2N = 6); other values
+                      fall back to the default (fame_b200.autotune picks it per problem) */
 } fame_krinv_opts;
 FAME_API int fame_krinv_default_opts(fame_krinv_opts* o);
 FAME_API int fame_krinv_create(fame_basis* b, fame_mass* m, const fame_krinv_opts* o, fame_krinv** out);

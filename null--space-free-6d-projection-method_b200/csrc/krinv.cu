@@ -265,6 +265,7 @@ int fame_krinv_default_opts(fame_krinv_opts* o) {
   o->verifyTrueResidual = 1;
   o->useGraphs = 1;
   o->mhatPreconditioner = 1;
+  o->passColumns = 0;
   return FAME_OK;
 }
 

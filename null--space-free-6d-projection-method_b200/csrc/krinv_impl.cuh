@@ -73,12 +73,12 @@ template <typename T> struct OpMhat {
   int matvec(fame_krinv* K, PcgBuf<T>& B, PcgState* st, cudaStream_t s) const {
     ProPcgMhat<T> pro{c, B.x, B.r, B.p, B.Ap, st};
     EpiPcgMhat<T> epi{c, B.Ap, B.p, B.r, st, K->partials, K->counter};
-    return run_chain_lin<T, 3>(K->n, pro, epi, B.work, Es, K->NF, s, Gate{&st->active});
+    return run_chain_lin<T, 3>(K->n, pro, epi, B.work, Es, K->NF, s, Gate{&st->active}, K->o.passColumns);
   }
   int resid(fame_krinv* K, PcgBuf<T>& B, const C<T>* b, double* out, cudaStream_t s) const {
     ProResidMhat<T, T, false> pro{c, B.x, nullptr};
     EpiResidMhat<T> epi{c, b, B.r, out, reinterpret_cast<T*>(K->partials), K->counter};
-    return run_chain_lin<T, 3>(K->n, pro, epi, B.work, Es, K->NF, s);
+    return run_chain_lin<T, 3>(K->n, pro, epi, B.work, Es, K->NF, s, Gate{nullptr}, K->o.passColumns);
   }
 };
 
@@ -115,10 +115,10 @@ template <typename T> struct OpMhatPre {
   int matvec(fame_krinv* K, PcgBuf<T>& B, PcgState* st, cudaStream_t s) const {
     ProPcgPre<T> pp{c, B.x, B.r, B.p, B.Ap, st};
     EpiPcgPre<T> ep{c, B.z, B.r, st, K->partials, K->counter};
-    FAME_TRY((run_chain_lin<T, 3>(K->n, pp, ep, B.work, EsInv, K->NF, s, Gate{&st->active})));
+    FAME_TRY((run_chain_lin<T, 3>(K->n, pp, ep, B.work, EsInv, K->NF, s, Gate{&st->active}, K->o.passColumns)));
     ProPcgDir<T> pd{c, B.p, B.z, st};
     EpiPcgMhat<T, true> ea{c, B.Ap, B.p, B.r, st, K->partials, K->counter};
-    return run_chain_lin<T, 3>(K->n, pd, ea, B.work, Es, K->NF, s, Gate{&st->active});
+    return run_chain_lin<T, 3>(K->n, pd, ea, B.work, Es, K->NF, s, Gate{&st->active}, K->o.passColumns);
   }
   int resid(fame_krinv* K, PcgBuf<T>& B, const C<T>* b, double* out, cudaStream_t s) const {
     return OpMhat<T>{c, Es}.resid(K, B, b, out, s);

@@ -124,11 +124,10 @@ template <int n, typename T> struct LinCols {
   static_assert((n * n * n) % value == 0 && value * n * n <= 512, "linear chain tiling");
 };
 
-template <int n, typename T, int F, class Pro, class Epi, typename TE>
-int chain_lin_n(const Pro& pro, const Epi& epi, C<T>* work, const TE* Et, long long NF,
+template <int n, typename T, int F, int G, class Pro, class Epi, typename TE>
+int chain_lin_g(const Pro& pro, const Epi& epi, C<T>* work, const TE* Et, long long NF,
                 cudaStream_t st, Gate gate) {
   if constexpr (std::is_same<T, float>::value) {  // packed passes on pair-split cubes
-    constexpr int G = LinCols<n, T>::value;
     const size_t smem = (size_t)G * CubePk<n>::S * sizeof(float4);
     const int threads = round32(G * n * n);
     static int attrA = ensure_smem(k_passA_lin_pk<n, F, G, Pro>, smem);
@@ -144,7 +143,6 @@ int chain_lin_n(const Pro& pro, const Epi& epi, C<T>* work, const TE* Et, long l
     return FAME_OK;
   }
   using Q = Cube<n, T>;
-  constexpr int G = LinCols<n, T>::value;
   const size_t smem = (size_t)G * Q::size * sizeof(C<T>);
   const int threads = round32(G * Q::n2);
   static int attrA = ensure_smem(k_passA_lin<n, T, F, G, Pro>, smem);
@@ -160,17 +158,38 @@ int chain_lin_n(const Pro& pro, const Epi& epi, C<T>* work, const TE* Et, long l
   return FAME_OK;
 }
 
+// Columns per CTA of the linear passes: LinCols by default; `cols` selects one of the
+// alternatives compiled for the Bloch-path sizes (n = 6, 8, 10), any other value the default.
+// The choice changes the CTA grouping (and so the order of the grid reductions), not the
+// arithmetic of a mode.
+template <int n, typename T, int F, class Pro, class Epi, typename TE>
+int chain_lin_n(const Pro& pro, const Epi& epi, C<T>* work, const TE* Et, long long NF, cudaStream_t st, Gate gate,
+                int cols) {
+  if constexpr (n == 10) {
+    if (cols == 1) return chain_lin_g<n, T, F, 1>(pro, epi, work, Et, NF, st, gate);
+    if (cols == 4) return chain_lin_g<n, T, F, 4>(pro, epi, work, Et, NF, st, gate);
+  } else if constexpr (n == 8) {
+    if (cols == 2) return chain_lin_g<n, T, F, 2>(pro, epi, work, Et, NF, st, gate);
+    if (cols == 4) return chain_lin_g<n, T, F, 4>(pro, epi, work, Et, NF, st, gate);
+  } else if constexpr (n == 6) {
+    if (cols == 4) return chain_lin_g<n, T, F, 4>(pro, epi, work, Et, NF, st, gate);
+    if (cols == 6) return chain_lin_g<n, T, F, 6>(pro, epi, work, Et, NF, st, gate);
+  }
+  return chain_lin_g<n, T, F, LinCols<n, T>::value>(pro, epi, work, Et, NF, st, gate);
+}
+
 // Linear-field chain (see k_passA_lin) for axis length n in {2,4,...,14}.
 template <typename T, int F, class Pro, class Epi, typename TE>
-int run_chain_lin(int n, const Pro& pro, const Epi& epi, C<T>* work, const TE* Et, long long NF, cudaStream_t st, Gate gate = Gate{nullptr}) {
+int run_chain_lin(int n, const Pro& pro, const Epi& epi, C<T>* work, const TE* Et, long long NF, cudaStream_t st,
+                  Gate gate = Gate{nullptr}, int cols = 0) {
   switch (n) {
-    case 2: return chain_lin_n<2, T, F>(pro, epi, work, Et, NF, st, gate);
-    case 4: return chain_lin_n<4, T, F>(pro, epi, work, Et, NF, st, gate);
-    case 6: return chain_lin_n<6, T, F>(pro, epi, work, Et, NF, st, gate);
-    case 8: return chain_lin_n<8, T, F>(pro, epi, work, Et, NF, st, gate);
-    case 10: return chain_lin_n<10, T, F>(pro, epi, work, Et, NF, st, gate);
-    case 12: return chain_lin_n<12, T, F>(pro, epi, work, Et, NF, st, gate);
-    case 14: return chain_lin_n<14, T, F>(pro, epi, work, Et, NF, st, gate);
+    case 2: return chain_lin_n<2, T, F>(pro, epi, work, Et, NF, st, gate, cols);
+    case 4: return chain_lin_n<4, T, F>(pro, epi, work, Et, NF, st, gate, cols);
+    case 6: return chain_lin_n<6, T, F>(pro, epi, work, Et, NF, st, gate, cols);
+    case 8: return chain_lin_n<8, T, F>(pro, epi, work, Et, NF, st, gate, cols);
+    case 10: return chain_lin_n<10, T, F>(pro, epi, work, Et, NF, st, gate, cols);
+    case 12: return chain_lin_n<12, T, F>(pro, epi, work, Et, NF, st, gate, cols);
+    case 14: return chain_lin_n<14, T, F>(pro, epi, work, Et, NF, st, gate, cols);
     default: return fail(FAME_ERR_UNSUPPORTED, "mass operator supports 2N in {2,4,...,14}");
   }
 }

@@ -67,13 +67,33 @@ def test_method_a_entry_points_reject_bad_arguments_without_gpu():
     assert L.fame_osi_destroy(None) == 0
 
 
-def test_struct_layouts_match_header():
+def test_struct_layouts_match_header(tmp_path):
+    """Every ABI struct of include/fame.h, compiled by the C compiler, has the size and field
+    offsets of its ctypes mirror."""
+    import shutil
+    import subprocess
     from fame_b200 import _lib
-    # field counts mirror include/fame.h
-    assert len(_lib.fame_krinv_opts._fields_) == 16
-    assert len(_lib.fame_krinv_stats._fields_) == 10
-    assert C.sizeof(_lib.fame_basis_info) == 8 + 4 + 4 + 8 + 8 + 48 + 8
-    assert C.sizeof(_lib.fame_osi_stats) == 3 * 8 + 8 + 4 + 4
+    structs = [_lib.fame_krinv_opts, _lib.fame_krinv_stats, _lib.fame_basis_info, _lib.fame_osi_stats,
+               _lib.fame_lanczos_info]
+    cc = shutil.which("gcc") or shutil.which("cc")
+    assert cc, "a C compiler is needed for the layout check"
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "fame.h"', "int main(void) {"]
+    for st in structs:
+        lines.append('printf("%%s %%zu\\n", "%s", sizeof(%s));' % (st.__name__, st.__name__))
+        for f in st._fields_:
+            lines.append('printf("%%s.%%s %%zu\\n", "%s", "%s", offsetof(%s, %s));'
+                         % (st.__name__, f[0], st.__name__, f[0]))
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(l.rsplit(" ", 1) for l in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                           check=True).stdout.splitlines())
+    for st in structs:
+        assert int(got[st.__name__]) == C.sizeof(st), st.__name__
+        for f in st._fields_:
+            assert int(got["%s.%s" % (st.__name__, f[0])]) == getattr(st, f[0]).offset, (st.__name__, f[0])
 
 
 def test_twiddle_header_is_generated_and_exact():

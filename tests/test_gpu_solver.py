@@ -181,14 +181,16 @@ def test_pivoted_split_when_v1_is_singular(cuda_device):
 @pytest.mark.parametrize("N", [2, 3])
 def test_launch_schedule_autotuner(cuda_device, N):
     """The launch-schedule candidates (host-check cadence, graph replay) give bitwise-
-    identical K_r^{-1} actions (the tuner raises otherwise) and the tuner returns the
-    fastest as make_explicit_krinv_compact options."""
+    identical K_r^{-1} actions, the pass tile shapes (columns per CTA, alternatives at
+    2N = 6) agree to 1e-7 (the tuner raises otherwise), and the tuner returns the fastest
+    as make_explicit_krinv_compact options."""
     import fame_b200 as F
     E = torch.as_tensor(O.material_smooth_exp(N), device=cuda_device)
     s = F.build_q_system(F.MassBackend(E, N), F.configs.P_REFERENCE, F.configs.Q_TRACKING)
     best, table = F.autotune.tune_krinv_schedule(s, precision="mixed", reps=2)
-    assert len(table) == len(F.autotune.DEFAULT_CANDIDATES)
+    ncols = len(F.autotune.COLUMN_CANDIDATES.get(2 * N, (0,)))
+    assert len(table) == len(F.autotune.DEFAULT_CANDIDATES) * ncols
     fastest = min(table, key=lambda r: r["seconds"])
-    assert best == {"checkEvery": fastest["checkEvery"], "useGraphs": fastest["useGraphs"]}
+    assert best == {k: fastest[k] for k in ("checkEvery", "useGraphs", "passColumns")}
     op, _ = F.make_explicit_krinv_compact(s, 1e-10, 3000, precision="mixed", **best)
     assert op(F.start_vector(7, s.nr).reshape(-1, 1)).isfinite().all()
