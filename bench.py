@@ -43,7 +43,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["fame", "reference"], default="fame")
     ap.add_argument("--N", type=int, default=N_BENCH)
-    ap.add_argument("--case", choices=["chain", "pcg", "solve", "yee", "grad", "osi"], default=None,
+    ap.add_argument("--case", choices=["chain", "pcg", "solve", "yee", "recon", "grad", "osi"], default=None,
                     help="run one piece of the step alone (for profiling), print its device time")
     ap.add_argument("--precision", choices=["fp32", "fp64", "mixed"], default="mixed")
     ap.add_argument("--reps", type=int, default=3)
@@ -581,6 +581,8 @@ def run_case(args):
     prec = "fp64" if args.precision == "fp64" else "mixed"
     if args.case == "yee":
         return yee_sweep(F, cfg, sysq, v0, args)
+    if args.case == "recon":
+        return recon_case(F, cfg, sysq, v0, args)
     if args.case == "chain":
         x = torch.randn(NF, dtype=torch.complex128 if prec == "fp64" else torch.complex64, device=dev)
         body = lambda: F.apply_Mhat_C_scalar_compact(x, sysq)  # noqa: E731
@@ -677,6 +679,39 @@ def osi_case(F, args):
                           "speedup_C_mixed_over_A": round(tA / out["mixed"][0], 2),
                           "lambda_rel_diff_A_vs_C": float(np.max(np.abs(lamA - lamC) / lamC)),
                           "lambda": lamC.tolist()}), flush=True)
+
+
+def recon_case(F, cfg, sysq, v0, args):
+    """Eigenmode 10 at N=5 on the n = 40 window (h = 0.0125): ``--reps`` times the three
+    components by the batched 3xTF32 direct grid and by 3xTF32 Taylor (p = 10, 4^3 centers),
+    timed per repetition (for profiling the reconstruction kernels)."""
+    import numpy as np
+    import torch
+    S = cfg.SOLVE
+    op = F.make_explicit_krinv_compact(sysq, S["tolCG"], S["maxitCG"], precision="fp64")[0]
+    Y, theta = F.Lanczos(op, None, None, sysq.nr, S["nev"], S["tol"], S["maxRestart"], S["p"], v0)[:2]
+    F.rayleigh_ritz(sysq, Y)
+    X, _, _ = F.recover_original_eigenvectors(Y[:, 9].reshape(-1, 1).contiguous(), sysq, 1e-12, 3000)
+    x3 = X[:, 0].contiguous()
+    NF = sysq.NF
+    pts, axes, sz = F.build_yee_points(40, 0.0125)
+    Qm = F.build_projected_q_modes(sysq)
+    blocks = F.build_yee_block_partition(sz, 4)
+    out = {}
+    for name, fn in (("direct_3xtf32", lambda: F.reconstruct_fields_direct_grid(x3, sysq, axes, tensor_cores=True)),
+                     ("taylor_3xtf32", lambda: [F.taylor_on_blocks(x3[c * NF:(c + 1) * NF], Qm, pts[c], 10, blocks,
+                                                                   tensor_cores=True) for c in range(3)])):
+        ts = []
+        for _ in range(max(1, args.reps)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        out[name] = sorted(ts)[len(ts) // 2]
+    M3 = sum(int(p.shape[0]) for p in pts)
+    print(json.dumps({"case": "recon", "n": 40, "points": M3,
+                      **{k + "_pts_per_s": M3 / v for k, v in out.items()}}), flush=True)
 
 
 def yee_sweep(F, cfg, sysq, v0, args):
