@@ -26,6 +26,14 @@
 #include "bulk.cuh"
 #include "fft6d.cuh"
 
+// Register caps of the pass-B kernels at 2N = 10 (tuning constants).
+#ifndef FAME_PASSB64_REGS
+#define FAME_PASSB64_REGS 96
+#endif
+#ifndef FAME_PASSB32_REGS
+#define FAME_PASSB32_REGS 96
+#endif
+
 namespace fame {
 
 template <int n, typename T> struct PassBGeom {
@@ -39,7 +47,7 @@ template <int n, typename T> struct PassBGeom {
   static constexpr unsigned plane_bytes = (unsigned)(TT * n2 * sizeof(C<T>));
   static constexpr int threads = (L + 31) / 32 * 32;
   // registers per thread: three CTAs of 7 warps per SM at n = 10 (21 x 32 x 96 <= 65536)
-  static constexpr int max_regs = n == 10 ? 96 : 255;
+  static constexpr int max_regs = n == 10 ? FAME_PASSB64_REGS : 255;
   static_assert((P6 * sizeof(C<T>)) % 16 == 0 && (stage * sizeof(C<T>)) % 16 == 0, "bulk-copy alignment");
   static_assert(plane_bytes % 16 == 0, "bulk-copy size");
   template <typename TE> static constexpr size_t smem_bytes() {
@@ -173,7 +181,7 @@ template <int n> struct PassBPkGeom {
   static constexpr int threads = (L + 31) / 32 * 32;
   static constexpr size_t smem_bytes = 2 * (size_t)stage * sizeof(float4) + 2 * sizeof(uint64_t);
   // registers per thread: three CTAs per SM for n <= 10 (7 warps each: 21 x 32 x 96 <= 65536)
-  static constexpr int max_regs = n <= 10 ? 96 : 255;
+  static constexpr int max_regs = n <= 10 ? FAME_PASSB32_REGS : 255;
 };
 
 // poll_limit / arm_only: fault-path self-test (fame_selftest_bounded_wait); arm_only
