@@ -4,6 +4,7 @@
 //   for every outer matvec.  Outer scalars live in an OuterState on the device;
 //   the host reads it once per outer iteration.  In FAME_PREC_MIXED the inner
 //   M3 solves are FP64 iterative refinement around an FP32 PCG.
+#include <cstdio>
 #include <algorithm>
 #include <cmath>
 #include <string>
@@ -215,8 +216,11 @@ static int inner_m3_solve(fame_krinv* K) {
   K->stats.massSolveCalls += 1;
   K->stats.totalMassIterations += its;
   const double rr = bn2 > 0 ? std::sqrt(rn2 / bn2) : 0.0;
-  if (rr > 10 * tolM)
-    return fail(FAME_ERR_NOT_CONVERGED, "Nested M refinement failed: relres=" + std::to_string(rr));
+  if (rr > 10 * tolM) {
+    char msg[96];
+    std::snprintf(msg, sizeof(msg), "Nested M refinement failed: relres=%.3e after %d refinements", rr, refine);
+    return fail(FAME_ERR_NOT_CONVERGED, msg);
+  }
   return FAME_OK;
 }
 

@@ -293,6 +293,13 @@ int small_gep(const std::vector<cd>& G0, const std::vector<cd>& B0, int k, std::
   return FAME_OK;
 }
 
+// Device-to-host copy of a few kilobytes into pageable host memory (stream-ordered, waited on).
+int copy_to_host(fame_ctx* ctx, const void* dsrc, void* hdst, size_t bytes) {
+  FAME_CUDA_TRY(cudaMemcpyAsync(hdst, dsrc, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  FAME_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return FAME_OK;
+}
+
 }  // namespace fame
 
 using namespace fame;
@@ -344,7 +351,7 @@ extern "C" int fame_rayleigh_ritz(fame_basis* b, fame_mass* m, void* Y, int k, d
   count_launch(2);
   FAME_CUDA_TRY(cudaGetLastError());
   std::vector<double2> hg(npair);
-  FAME_TRY(read_back(ctx, gram, hg.data(), npair * sizeof(double2)));
+  FAME_TRY(copy_to_host(ctx, gram, hg.data(), npair * sizeof(double2)));
   FAME_TRY(check_fault(ctx));
   std::vector<cd> G((size_t)k * k), B((size_t)k * k);
   for (int p = 0; p < k * k; ++p) {
@@ -366,7 +373,7 @@ extern "C" int fame_rayleigh_ritz(fame_basis* b, fame_mass* m, void* Y, int k, d
   FAME_CUDA_TRY(cudaGetLastError());
   FAME_CUDA_TRY(cudaMemcpyAsync(Yd, Yr, (size_t)nr * k * sizeof(double2), cudaMemcpyDeviceToDevice, st));
   std::vector<double> hres((size_t)rblk * 2 * k);
-  FAME_TRY(read_back(ctx, resd, hres.data(), hres.size() * sizeof(double)));
+  FAME_TRY(copy_to_host(ctx, resd, hres.data(), hres.size() * sizeof(double)));
   for (int j = 0; j < k; ++j) {
     lambda[j] = lam[j];
     if (relres) {
