@@ -320,6 +320,10 @@ template <int n, typename T> struct WorkIO {
     return w[work_at<n, T>(c123, c456)];
   }
 };
+#ifndef FAME_FP32_PAIRSPLIT
+#define FAME_FP32_PAIRSPLIT 1
+#endif
+#if FAME_FP32_PAIRSPLIT
 template <int n> struct WorkIO<n, float> {
   static_assert(WorkTile<n, float>::TT % 2 == 0, "FP32 rows hold element pairs");
   // float offset of the real part; the imaginary part is 2 floats further
@@ -338,6 +342,7 @@ template <int n> struct WorkIO<n, float> {
     return make_float2(f[o], f[o + 2]);
   }
 };
+#endif
 
 // float4 index of the pair (c123, c123 + 1), c123 even, in a pair-split work field
 template <int n> __device__ __forceinline__ long long work_pair_at(long long c123, long long c456) {
@@ -535,16 +540,8 @@ __global__ void __launch_bounds__(512) k_passC(Epi epi, const C<T>* __restrict__
 //          C<T> coef(f, ia, in)      a_f(i) (a_0 == 1 when unit0)
 // LinEpi:  C<T> coef(f, ia, in)      b_f(i) (b_0 == 1 when unit0)
 //          void store(ia, in, C<T> s, Red<Acc,K>& acc), finalize(tot)
-// Register cap of the scalar linear-field passes (FP64) at 2N = 10 (tuning constant).
-#ifndef FAME_LIN64_REGS
-#define FAME_LIN64_REGS 255
-#endif
-template <int n, typename T> struct LinRegs {
-  static constexpr int value = (sizeof(T) == 8 && n == 10) ? FAME_LIN64_REGS : 255;
-};
-
 template <int n, typename T, int F, int G, class Pro>
-__global__ void __launch_bounds__(512) __maxnreg__((LinRegs<n, T>::value)) k_passA_lin(Pro pro, C<T>* __restrict__ work, long long NF, Gate gate) {
+__global__ void __launch_bounds__(512) k_passA_lin(Pro pro, C<T>* __restrict__ work, long long NF, Gate gate) {
   if (gate.off()) return;
   using Q = Cube<n, T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -602,7 +599,7 @@ __global__ void __launch_bounds__(512) __maxnreg__((LinRegs<n, T>::value)) k_pas
 }
 
 template <int n, typename T, int F, int G, class Epi>
-__global__ void __launch_bounds__(512) __maxnreg__((LinRegs<n, T>::value)) k_passC_lin(Epi epi, const C<T>* __restrict__ work, long long NF, Gate gate) {
+__global__ void __launch_bounds__(512) k_passC_lin(Epi epi, const C<T>* __restrict__ work, long long NF, Gate gate) {
   if (gate.off()) return;
   using Q = Cube<n, T>;
   using A = typename Epi::Acc;

@@ -42,10 +42,12 @@ int launch_passB_pk(float2* work, int nfields, const float* Et, long long NF, cu
 
 template <int n, typename T, typename TE>
 int launch_passB(C<T>* work, int nfields, const TE* Et, long long NF, cudaStream_t st, Gate gate) {
+#if FAME_FP32_PAIRSPLIT
   if constexpr (std::is_same<T, float>::value) {
     static_assert(std::is_same<TE, float>::value, "FP32 chains use the FP32 material tiles");
     return launch_passB_pk<n>(work, nfields, Et, NF, st, gate);
   }
+#endif
   using G = PassBGeom<n, T>;
   constexpr size_t smem = G::template smem_bytes<TE>();
   static int attr = ensure_smem(k_passB<n, T, TE>, smem);
@@ -127,7 +129,10 @@ template <int n, typename T> struct LinCols {
 template <int n, typename T, int F, int G, class Pro, class Epi, typename TE>
 int chain_lin_g(const Pro& pro, const Epi& epi, C<T>* work, const TE* Et, long long NF,
                 cudaStream_t st, Gate gate) {
-  if constexpr (std::is_same<T, float>::value) {  // packed passes on pair-split cubes
+#ifndef FAME_FP32_AC_PACKED
+#define FAME_FP32_AC_PACKED 1
+#endif
+  if constexpr (FAME_FP32_AC_PACKED && FAME_FP32_PAIRSPLIT && std::is_same<T, float>::value) {  // packed passes
     const size_t smem = (size_t)G * CubePk<n>::S * sizeof(float4);
     const int threads = round32(G * n * n);
     static int attrA = ensure_smem(k_passA_lin_pk<n, F, G, Pro>, smem);

@@ -5,11 +5,9 @@
 // Persistent kernel: each CTA owns a contiguous range of units (tile k,
 // field f) and streams them through two shared-memory stages.  One thread
 // pulls a unit with n bulk copies (one per i6-plane, completed on the stage's
-// mbarrier); the copy of unit i+2 is issued as soon as unit i has been read out
-// of its stage, so global latency overlaps the transforms of the next unit.  The
-// material values of a thread's axis-5 line are read from global memory (L2) in
-// that phase, which keeps the shared memory of a CTA to its two stages.  This
-// generic kernel runs the FP64 chains; FP32 uses k_passB_pk below.  In shared memory
+// mbarrier) plus, at the first unit of a tile, the material tile; the copy of
+// unit i+2 is issued as soon as unit i has been read out of its stage, so
+// global latency overlaps the transforms of the next unit.  In shared memory
 // element (t, i4, i5, i6) of a unit sits at t + TT*i4 + P5*i5 + P6*i6 with
 // P5 = TT*n and P6 = TT*n^2 + TT (one padding row per plane); each phase
 // transforms one line per thread in place:
@@ -26,12 +24,9 @@
 #include "bulk.cuh"
 #include "fft6d.cuh"
 
-// Register caps of the pass-B kernels at 2N = 10 (tuning constants).
-#ifndef FAME_PASSB64_REGS
-#define FAME_PASSB64_REGS 96
-#endif
+// Register cap of the packed FP32 pass B at 2N <= 10 (tuning constant; 255 = none).
 #ifndef FAME_PASSB32_REGS
-#define FAME_PASSB32_REGS 96
+#define FAME_PASSB32_REGS 255
 #endif
 
 namespace fame {
@@ -46,38 +41,40 @@ template <int n, typename T> struct PassBGeom {
   static constexpr int tile = TT * n3;     // elements per tile (global)
   static constexpr unsigned plane_bytes = (unsigned)(TT * n2 * sizeof(C<T>));
   static constexpr int threads = (L + 31) / 32 * 32;
-  // registers per thread: three CTAs of 7 warps per SM at n = 10 (21 x 32 x 96 <= 65536)
-  static constexpr int max_regs = n == 10 ? FAME_PASSB64_REGS : 255;
   static_assert((P6 * sizeof(C<T>)) % 16 == 0 && (stage * sizeof(C<T>)) % 16 == 0, "bulk-copy alignment");
   static_assert(plane_bytes % 16 == 0, "bulk-copy size");
   template <typename TE> static constexpr size_t smem_bytes() {
-    return 2 * stage * sizeof(C<T>) + 2 * sizeof(uint64_t);
+    return 2 * stage * sizeof(C<T>) + 2 * (size_t)tile * sizeof(TE) + 2 * sizeof(uint64_t);
   }
 };
 
 template <int n, typename T, typename TE>
-__global__ void __launch_bounds__(512) __maxnreg__((PassBGeom<n, T>::max_regs))
-    k_passB(C<T>* __restrict__ work, const TE* __restrict__ Et, int nfields,
+__global__ void __launch_bounds__(512) k_passB(C<T>* __restrict__ work, const TE* __restrict__ Et, int nfields,
                                               long long NF, Gate gate, unsigned* fault) {
   if (gate.off()) return;
   using G = PassBGeom<n, T>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   C<T>* stg = reinterpret_cast<C<T>*>(smem_raw);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * G::stage * sizeof(C<T>));
+  TE* es = reinterpret_cast<TE*>(smem_raw + 2 * G::stage * sizeof(C<T>));
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * G::stage * sizeof(C<T>) + 2 * G::tile * sizeof(TE));
   constexpr int tiles = G::n3 / G::TT;
   const int U = tiles * nfields;
   const int u0 = (int)((long long)blockIdx.x * U / gridDim.x);
   const int u1 = (int)((long long)(blockIdx.x + 1) * U / gridDim.x);
   if (u0 >= u1) return;
+  const int k0 = u0 / nfields;
   const int tid = threadIdx.x;
 
   auto issue = [&](int u, int s) {
     const int k = u / nfields, f = u - k * nfields;
-    mbar_arrive_expect_tx(&bar[s], n * G::plane_bytes);
+    const bool needE = (u == u0) || (f == 0);
+    mbar_arrive_expect_tx(&bar[s], n * G::plane_bytes + (needE ? (unsigned)(G::tile * sizeof(TE)) : 0u));
     const C<T>* src = work + (long long)f * NF + (long long)k * G::tile;
     C<T>* dst = stg + s * G::stage;
 #pragma unroll 1
     for (int p = 0; p < n; ++p) bulk_g2s(dst + p * G::P6, src + p * G::TT * G::n2, G::plane_bytes, &bar[s]);
+    if (needE)
+      bulk_g2s(es + ((k - k0) & 1) * G::tile, Et + (long long)k * G::tile, (unsigned)(G::tile * sizeof(TE)), &bar[s]);
   };
 
   if (tid == 0) {
@@ -106,7 +103,7 @@ __global__ void __launch_bounds__(512) __maxnreg__((PassBGeom<n, T>::max_regs))
     }
     C<T>* S = stg + s * G::stage;
     const int k = u / nfields, f = u - k * nfields;
-    const TE* E = Et + (long long)k * G::tile;  // material tile, read from L2 in the axis-5 phase
+    const TE* E = es + ((k - k0) & 1) * G::tile;
     if (act) line_dft<n, +1, T>(S + b1, G::TT);
     __syncthreads();
     if (act) line_dft<n, +1, T>(S + b2, G::P6);
@@ -123,7 +120,7 @@ __global__ void __launch_bounds__(512) __maxnreg__((PassBGeom<n, T>::max_regs))
       Dft<n, +1, T>::run(re, im);
 #pragma unroll
       for (int j = 0; j < n; ++j) {
-        const T e = (T)__ldg(E + j * G::L + tid);
+        const T e = (T)E[j * G::L + tid];
         re[j] *= e;
         im[j] *= e;
       }
@@ -164,9 +161,9 @@ __global__ void __launch_bounds__(512) __maxnreg__((PassBGeom<n, T>::max_regs))
 // (p, i4, i5, i6) is one float4 (re_2p, re_2p+1, im_2p, im_2p+1) at float4 index
 // p + Q4*i4 + Q5*i5 + Q6*i6 (Q4 = TT/2, Q5 = Q4*n, Q6 = Q4*n^2 + pad); the pads were
 // chosen by counting 16-byte shared-memory wavefronts of the three line orders
-// (n = 10: 80 wavefronts per phase set against an ideal 75).  The material pairs of a
-// thread's axis-5 line are read from global memory (L2) in that phase, so a stage
-// holds only the unit and three CTAs fit on an SM.
+// (n = 10: 80 wavefronts per phase set against an ideal 75).  The material tile comes
+// with the first unit of each tile by one more bulk copy (two buffers), and the axis-5
+// phase reads its pairs (E_2p, E_2p+1) from shared memory.
 template <int n> struct PassBPkPad {
   static constexpr int value = n == 8 || n == 10 ? 2 : n >= 12 ? 1 : 4;
 };
@@ -179,8 +176,8 @@ template <int n> struct PassBPkGeom {
   static constexpr int tile = TP * n3;  // float4 per tile of a field (= float2 pairs of the material tile)
   static constexpr unsigned plane_bytes = (unsigned)(TP * n2 * sizeof(float4));
   static constexpr int threads = (L + 31) / 32 * 32;
-  static constexpr size_t smem_bytes = 2 * (size_t)stage * sizeof(float4) + 2 * sizeof(uint64_t);
-  // registers per thread: three CTAs per SM for n <= 10 (7 warps each: 21 x 32 x 96 <= 65536)
+  static constexpr unsigned e_bytes = (unsigned)(tile * sizeof(float2));  // material tile
+  static constexpr size_t smem_bytes = 2 * (size_t)stage * sizeof(float4) + 2 * (size_t)e_bytes + 2 * sizeof(uint64_t);
   static constexpr int max_regs = n <= 10 ? FAME_PASSB32_REGS : 255;
 };
 
@@ -195,22 +192,26 @@ __global__ void __launch_bounds__(PassBPkGeom<n>::threads) __maxnreg__(PassBPkGe
   using G = PassBPkGeom<n>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   float4* stg = reinterpret_cast<float4*>(smem_raw);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * (size_t)G::stage * sizeof(float4));
+  float2* es = reinterpret_cast<float2*>(smem_raw + 2 * (size_t)G::stage * sizeof(float4));
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * (size_t)G::stage * sizeof(float4) + 2 * (size_t)G::e_bytes);
   constexpr int tiles = G::n3 / G::TT;
   const int U = tiles * nfields;
   const int u0 = (int)((long long)blockIdx.x * U / gridDim.x);
   const int u1 = (int)((long long)(blockIdx.x + 1) * U / gridDim.x);
   if (u0 >= u1) return;
+  const int k0 = u0 / nfields;
   const int tid = threadIdx.x;
 
   auto issue = [&](int u, int s) {
     const int k = u / nfields, f = u - k * nfields;
-    mbar_arrive_expect_tx(&bar[s], n * G::plane_bytes);
+    const bool needE = (u == u0) || (f == 0);
+    mbar_arrive_expect_tx(&bar[s], n * G::plane_bytes + (needE ? G::e_bytes : 0u));
     if (arm_only) return;
     const float4* src = work + (long long)f * NF4 + (long long)k * G::tile;
     float4* dst = stg + s * G::stage;
 #pragma unroll 1
     for (int p = 0; p < n; ++p) bulk_g2s(dst + p * G::Q6, src + p * G::TP * G::n2, G::plane_bytes, &bar[s]);
+    if (needE) bulk_g2s(es + ((k - k0) & 1) * G::tile, Et + (long long)k * G::tile, G::e_bytes, &bar[s]);
   };
 
   if (tid == 0) {
@@ -233,7 +234,7 @@ __global__ void __launch_bounds__(PassBPkGeom<n>::threads) __maxnreg__(PassBPkGe
   for (int u = u0, i = 0; u < u1; ++u, ++i) {
     const int s = i & 1;
     const int k = u / nfields, f = u - k * nfields;
-    const float2* Ek = Et + (long long)k * G::tile + tid;
+    const float2* Ek = es + ((k - k0) & 1) * G::tile + tid;
     const bool landed = mbar_wait(&bar[s], (unsigned)((i >> 1) & 1), poll_limit);
     if (!__syncthreads_and(landed)) {  // bounded wait, agreed on by the whole CTA
       if (fault && tid == 0) atomicOr(fault, 1u);
@@ -256,7 +257,7 @@ __global__ void __launch_bounds__(PassBPkGeom<n>::threads) __maxnreg__(PassBPkGe
       Dft<n, +1, F2>::run(re, im);
 #pragma unroll
       for (int j = 0; j < n; ++j) {
-        const F2 e(__ldg(Ek + j * G::L));
+        const F2 e(Ek[j * G::L]);
         re[j] = re[j] * e;
         im[j] = im[j] * e;
       }
