@@ -207,7 +207,7 @@ typedef struct {
                              test stays ||b - Mhat u|| <= tolCG ||b|| (1).  0: plain CG as the
                              reference's pcg(Mhat, ...) in exp1/make_explicit_krinv_compact.m:43 */
   int passColumns; /* columns per CTA of the inner solves' pass A/C kernels: 0 = built-in default;
-                      alternatives 1, 4 (2N = 10), 2, 4 (2N = 8), 4, 6 (2N = 6); other values
+                      alternatives 2, 4 (2N = 10), 2, 4 (2N = 8), 4, 6 (2N = 6); other values
                       fall back to the default (fame_b200.autotune picks it per problem) */
 } fame_krinv_opts;
 FAME_API int fame_krinv_default_opts(fame_krinv_opts* o);

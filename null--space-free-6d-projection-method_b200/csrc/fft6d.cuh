@@ -23,10 +23,13 @@
 // functors receive both indices (ia = line order, in = natural order).
 #pragma once
 #include "fame_common.cuh"
-#include "pk2.cuh"
 #include "twiddles.cuh"
 
 namespace fame {
+
+// a * b + c (written out so that the DFTs below state their fused multiply-adds)
+__host__ __device__ __forceinline__ float fmadd(float a, float b, float c) { return a * b + c; }
+__host__ __device__ __forceinline__ double fmadd(double a, double b, double c) { return a * b + c; }
 
 template <int n> struct SmallestFactor {
   static constexpr int value = (n % 2 == 0) ? 2 : (n % 3 == 0) ? 3 : (n % 5 == 0) ? 5 : (n % 7 == 0) ? 7 : n;
@@ -230,22 +233,6 @@ __device__ __forceinline__ void line_dft(C<T>* p, int stride) {
   for (int j = 0; j < n; ++j) p[j * stride] = mk<T>(re[j], im[j]);
 }
 
-// In-place DFT of two lines held as packed pairs: element j of the pair is the float4
-// (re_a, re_b, im_a, im_b) at p[j * stride].
-template <int n, int SIGN>
-__device__ __forceinline__ void line_pk(float4* p, int stride) {
-  F2 re[n], im[n];
-#pragma unroll
-  for (int j = 0; j < n; ++j) {
-    const float4 v = p[j * stride];
-    re[j] = F2(make_float2(v.x, v.y));
-    im[j] = F2(make_float2(v.z, v.w));
-  }
-  Dft<n, SIGN, F2>::run(re, im);
-#pragma unroll
-  for (int j = 0; j < n; ++j) p[j * stride] = make_float4(re[j].v.x, re[j].v.y, im[j].v.x, im[j].v.y);
-}
-
 // Device-resident status word used to gate queued iterations: kernels return
 // immediately when *gate == 0.
 struct Gate {
@@ -307,11 +294,7 @@ template <int n, typename T> __host__ __device__ __forceinline__ long long work_
   return TT * ((c123 / TT) * n3 + c456) + c123 % TT;
 }
 
-// Element access to field f of the work fields.  FP64 rows hold TT interleaved
-// complex values.  FP32 rows (TT even) are "pair-split": elements 2p and 2p+1 of a
-// row are stored as the four floats (re_2p, re_2p+1, im_2p, im_2p+1), so that pass B
-// loads the real parts and the imaginary parts of two lines (c123 = 2p, 2p+1) as
-// packed pairs with one 16-byte shared-memory load (passb.cuh, k_passB_pk).
+// Element access to field f of the work fields (rows of TT interleaved complex values).
 template <int n, typename T> struct WorkIO {
   static __device__ __forceinline__ void store(C<T>* w, long long c123, long long c456, C<T> v) {
     w[work_at<n, T>(c123, c456)] = v;
@@ -320,34 +303,6 @@ template <int n, typename T> struct WorkIO {
     return w[work_at<n, T>(c123, c456)];
   }
 };
-#ifndef FAME_FP32_PAIRSPLIT
-#define FAME_FP32_PAIRSPLIT 1
-#endif
-#if FAME_FP32_PAIRSPLIT
-template <int n> struct WorkIO<n, float> {
-  static_assert(WorkTile<n, float>::TT % 2 == 0, "FP32 rows hold element pairs");
-  // float offset of the real part; the imaginary part is 2 floats further
-  static __device__ __forceinline__ long long re_at(long long c123, long long c456) {
-    return 2 * work_at<n, float>(c123, c456) - (c123 & 1);
-  }
-  static __device__ __forceinline__ void store(float2* w, long long c123, long long c456, float2 v) {
-    float* f = reinterpret_cast<float*>(w);
-    const long long o = re_at(c123, c456);
-    f[o] = v.x;
-    f[o + 2] = v.y;
-  }
-  static __device__ __forceinline__ float2 load(const float2* w, long long c123, long long c456) {
-    const float* f = reinterpret_cast<const float*>(w);
-    const long long o = re_at(c123, c456);
-    return make_float2(f[o], f[o + 2]);
-  }
-};
-#endif
-
-// float4 index of the pair (c123, c123 + 1), c123 even, in a pair-split work field
-template <int n> __device__ __forceinline__ long long work_pair_at(long long c123, long long c456) {
-  return work_at<n, float>(c123, c456) >> 1;
-}
 
 // ------------------------------------------------------------------ pass A
 // CTA = G consecutive columns c456 x F fields.
@@ -659,162 +614,6 @@ __global__ void __launch_bounds__(512) k_passC_lin(Epi epi, const C<T>* __restri
   if (act) {
 #pragma unroll
     for (int j = 0; j < n; ++j) epi.store(cb + l + Q::n2 * j, cb + j + (long long)n * l, sum[j], acc);
-  }
-  if constexpr (K > 0) {
-    grid_sum_finalize<A, K>(acc, epi.partials, epi.counter, [&](const Red<A, K>& tot) { epi.finalize(tot); });
-  }
-}
-
-// ------------------------------------------- FP32 linear-field chains, packed
-// FP32 passes A and C of the linear-field chains with the n^3 cube of a column
-// stored pair-split along axis 1: pair element (p, i2, i3) is one float4
-// (re(2p), re(2p+1), im(2p), im(2p+1)) at p + R1*i2 + R2*i3 (column stride S; the
-// pitches were chosen by counting 16-byte shared-memory wavefronts of the three
-// access patterns below).  The axis-1 phase runs one line per thread in registers
-// (scalar DFT, as before); the axis-2 and axis-3 phases run two lines (i1 = 2p, 2p+1)
-// per thread on packed pairs (F2), and the axis-3 phase exchanges with the
-// pair-split work rows (WorkIO<n, float>) one float4 per element pair.
-template <int n> struct CubePk;
-template <> struct CubePk<2> { static constexpr int R1 = 1, R2 = 3, S = 6; };
-template <> struct CubePk<4> { static constexpr int R1 = 2, R2 = 9, S = 36; };
-template <> struct CubePk<6> { static constexpr int R1 = 3, R2 = 19, S = 114; };
-template <> struct CubePk<8> { static constexpr int R1 = 5, R2 = 44, S = 352; };
-template <> struct CubePk<10> { static constexpr int R1 = 5, R2 = 53, S = 530; };
-template <> struct CubePk<12> { static constexpr int R1 = 6, R2 = 78, S = 936; };
-template <> struct CubePk<14> { static constexpr int R1 = 7, R2 = 103, S = 1442; };
-
-template <int n, int F, int G, class Pro>
-__global__ void __launch_bounds__(512) k_passA_lin_pk(Pro pro, float2* __restrict__ work, long long NF, Gate gate) {
-  if (gate.off()) return;
-  using Q = CubePk<n>;
-  constexpr int n2 = n * n, n3 = n2 * n, h = n / 2;
-  static_assert(Q::R1 >= h && Q::R2 >= Q::R1 * n && Q::S >= Q::R2 * n, "pair-split cube pitches");
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  float4* s = reinterpret_cast<float4*>(smem_raw);
-  const long long col0 = (long long)blockIdx.x * G;
-  const int it = threadIdx.x;
-  const bool act = it < G * n2;  // axis-1 phase: one line (i2, i3) per thread
-  const int cc = act ? it / n2 : 0, l = act ? it % n2 : 0;
-  const int i2 = l % n, i3 = l / n;
-  const long long cb = (col0 + cc) * n3;
-  const bool act2 = it < G * n2 / 2;  // packed phases: one line pair (p, x) per thread
-  const int cc2 = act2 ? it / (n2 / 2) : 0, q2 = act2 ? it % (n2 / 2) : 0;
-  const int p2 = q2 % h, x2 = q2 / h;
-  C<float> u[n];
-  if (act) {  // each thread owns the modes of its line: stores may follow each load
-#pragma unroll
-    for (int j = 0; j < n; ++j) {
-      typename Pro::Ext e;
-      u[j] = pro.load(cb + l + n2 * j, cb + j + (long long)n * l, e);
-      pro.commit(cb + l + n2 * j, cb + j + (long long)n * l, e);
-    }
-  }
-#pragma unroll 1
-  for (int f = 0; f < F; ++f) {
-    if (act) {  // axis 1 in registers -> pair-split cube
-      float re[n], im[n];
-#pragma unroll
-      for (int j = 0; j < n; ++j) {
-        C<float> v = u[j];
-        if (!(Pro::unit0 && f == 0)) v = cmul<float>(pro.coef(f, cb + l + n2 * j, cb + j + (long long)n * l), v);
-        re[j] = v.x;
-        im[j] = v.y;
-      }
-      Dft<n, +1, float>::run(re, im);
-      float4* sc = s + cc * Q::S + Q::R1 * i2 + Q::R2 * i3;
-#pragma unroll
-      for (int p = 0; p < h; ++p) sc[p] = make_float4(re[2 * p], re[2 * p + 1], im[2 * p], im[2 * p + 1]);
-    }
-    __syncthreads();
-    if (act2) line_pk<n, +1>(s + cc2 * Q::S + p2 + Q::R2 * x2, Q::R1);  // axis 2, pair (p, i3 = x2)
-    __syncthreads();
-    if (act2) {  // axis 3, pair (p, i2 = x2) -> work
-      const float4* sc = s + cc2 * Q::S + p2 + Q::R1 * x2;
-      F2 re[n], im[n];
-#pragma unroll
-      for (int j = 0; j < n; ++j) {
-        const float4 v = sc[Q::R2 * j];
-        re[j] = F2(make_float2(v.x, v.y));
-        im[j] = F2(make_float2(v.z, v.w));
-      }
-      Dft<n, +1, F2>::run(re, im);
-      float4* wf = reinterpret_cast<float4*>(work + f * NF);
-#pragma unroll
-      for (int j = 0; j < n; ++j)
-        wf[work_pair_at<n>(2 * p2 + n * x2 + n2 * j, col0 + cc2)] =
-            make_float4(re[j].v.x, re[j].v.y, im[j].v.x, im[j].v.y);
-    }
-    __syncthreads();
-  }
-}
-
-template <int n, int F, int G, class Epi>
-__global__ void __launch_bounds__(512) k_passC_lin_pk(Epi epi, const float2* __restrict__ work, long long NF, Gate gate) {
-  if (gate.off()) return;
-  using Q = CubePk<n>;
-  using A = typename Epi::Acc;
-  constexpr int K = Epi::K;
-  constexpr int n2 = n * n, n3 = n2 * n, h = n / 2;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  float4* s = reinterpret_cast<float4*>(smem_raw);
-  const long long col0 = (long long)blockIdx.x * G;
-  const int it = threadIdx.x;
-  const bool act = it < G * n2;
-  const int cc = act ? it / n2 : 0, l = act ? it % n2 : 0;
-  const int i2 = l % n, i3 = l / n;
-  const long long cb = (col0 + cc) * n3;
-  const bool act2 = it < G * n2 / 2;
-  const int cc2 = act2 ? it / (n2 / 2) : 0, q2 = act2 ? it % (n2 / 2) : 0;
-  const int p2 = q2 % h, x2 = q2 / h;
-  C<float> sum[n];
-#pragma unroll
-  for (int j = 0; j < n; ++j) sum[j] = mk<float>(0, 0);
-#pragma unroll 1
-  for (int f = 0; f < F; ++f) {
-    if (act2) {  // axis 3 from work, pair (p, i2 = x2)
-      const float4* wf = reinterpret_cast<const float4*>(work + f * NF);
-      F2 re[n], im[n];
-#pragma unroll
-      for (int j = 0; j < n; ++j) {
-        const float4 v = wf[work_pair_at<n>(2 * p2 + n * x2 + n2 * j, col0 + cc2)];
-        re[j] = F2(make_float2(v.x, v.y));
-        im[j] = F2(make_float2(v.z, v.w));
-      }
-      Dft<n, -1, F2>::run(re, im);
-      float4* sc = s + cc2 * Q::S + p2 + Q::R1 * x2;
-#pragma unroll
-      for (int j = 0; j < n; ++j) sc[Q::R2 * j] = make_float4(re[j].v.x, re[j].v.y, im[j].v.x, im[j].v.y);
-    }
-    __syncthreads();
-    if (act2) line_pk<n, -1>(s + cc2 * Q::S + p2 + Q::R2 * x2, Q::R1);  // axis 2
-    __syncthreads();
-    if (act) {  // axis 1 in registers, accumulate b_f v_f
-      const float4* sc = s + cc * Q::S + Q::R1 * i2 + Q::R2 * i3;
-      float re[n], im[n];
-#pragma unroll
-      for (int p = 0; p < h; ++p) {
-        const float4 v = sc[p];
-        re[2 * p] = v.x;
-        re[2 * p + 1] = v.y;
-        im[2 * p] = v.z;
-        im[2 * p + 1] = v.w;
-      }
-      Dft<n, -1, float>::run(re, im);
-#pragma unroll
-      for (int j = 0; j < n; ++j) {
-        C<float> v = mk<float>(re[j], im[j]);
-        if (!(Epi::unit0 && f == 0)) v = cmul<float>(epi.coef(f, cb + l + n2 * j, cb + j + (long long)n * l), v);
-        sum[j] = cadd<float>(sum[j], v);
-      }
-    }
-    __syncthreads();
-  }
-  Red<A, (K > 0 ? K : 1)> acc;
-#pragma unroll
-  for (int k = 0; k < (K > 0 ? K : 1); ++k) acc.v[k] = 0;
-  if (act) {
-#pragma unroll
-    for (int j = 0; j < n; ++j) epi.store(cb + l + n2 * j, cb + j + (long long)n * l, sum[j], acc);
   }
   if constexpr (K > 0) {
     grid_sum_finalize<A, K>(acc, epi.partials, epi.counter, [&](const Red<A, K>& tot) { epi.finalize(tot); });

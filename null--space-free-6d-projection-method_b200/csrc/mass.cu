@@ -233,13 +233,13 @@ int fame_selftest_bounded_wait(fame_mass* m, unsigned poll_limit) {
   const Gate g{nullptr};
   int s = FAME_OK;
   switch (m->n) {
-    case 2: s = launch_passB_pk<2>(w, 1, m->Et32, m->NF, ctx->stream, g, poll_limit, 1); break;
-    case 4: s = launch_passB_pk<4>(w, 1, m->Et32, m->NF, ctx->stream, g, poll_limit, 1); break;
-    case 6: s = launch_passB_pk<6>(w, 1, m->Et32, m->NF, ctx->stream, g, poll_limit, 1); break;
-    case 8: s = launch_passB_pk<8>(w, 1, m->Et32, m->NF, ctx->stream, g, poll_limit, 1); break;
-    case 10: s = launch_passB_pk<10>(w, 1, m->Et32, m->NF, ctx->stream, g, poll_limit, 1); break;
-    case 12: s = launch_passB_pk<12>(w, 1, m->Et32, m->NF, ctx->stream, g, poll_limit, 1); break;
-    default: s = launch_passB_pk<14>(w, 1, m->Et32, m->NF, ctx->stream, g, poll_limit, 1); break;
+    case 2: s = launch_passB<2, float, float>(w, 1, m->Et32, m->NF, ctx->stream, g, poll_limit, 1); break;
+    case 4: s = launch_passB<4, float, float>(w, 1, m->Et32, m->NF, ctx->stream, g, poll_limit, 1); break;
+    case 6: s = launch_passB<6, float, float>(w, 1, m->Et32, m->NF, ctx->stream, g, poll_limit, 1); break;
+    case 8: s = launch_passB<8, float, float>(w, 1, m->Et32, m->NF, ctx->stream, g, poll_limit, 1); break;
+    case 10: s = launch_passB<10, float, float>(w, 1, m->Et32, m->NF, ctx->stream, g, poll_limit, 1); break;
+    case 12: s = launch_passB<12, float, float>(w, 1, m->Et32, m->NF, ctx->stream, g, poll_limit, 1); break;
+    default: s = launch_passB<14, float, float>(w, 1, m->Et32, m->NF, ctx->stream, g, poll_limit, 1); break;
   }
   FAME_TRY(s);
   FAME_CUDA_TRY(cudaGetLastError());

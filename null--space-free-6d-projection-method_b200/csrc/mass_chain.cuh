@@ -1,7 +1,6 @@
 // Host-side launch of one fused mass-operator chain (pass A -> B -> C) for a
 // runtime axis length n = 2N, dispatching to the compile-time kernels.
 #pragma once
-#include <type_traits>
 #include "passb.cuh"
 
 namespace fame {
@@ -18,36 +17,10 @@ template <typename K> int ensure_smem(K kernel, size_t bytes) {
 // Pass B over nfields tile-major fields with the tiled material Et (E/NF in the
 // layout of k_tile_E for this n and T): a persistent grid of (resident CTAs per
 // SM) x SMs, each CTA owning a contiguous range of (tile, field) units.
-// FP32: the packed kernel on the pair-split rows (two lines per thread).  poll_limit /
-// arm_only are the fault-path self-test (fame_selftest_bounded_wait).
-template <int n>
-int launch_passB_pk(float2* work, int nfields, const float* Et, long long NF, cudaStream_t st, Gate gate,
-                    unsigned poll_limit = kMbarPollLimit, int arm_only = 0) {
-  using G = PassBPkGeom<n>;
-  constexpr size_t smem = G::smem_bytes;
-  static int attr = ensure_smem(k_passB_pk<n>, smem);
-  if (attr != FAME_OK) return attr;
-  static int per_sm = [] {
-    int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_passB_pk<n>, G::threads, smem) != cudaSuccess) b = 1;
-    return b < 1 ? 1 : b;
-  }();
-  const int units = (G::n3 / G::TT) * nfields;
-  const int grid = std::min(units, per_sm * num_sms());
-  k_passB_pk<n><<<grid, G::threads, smem, st>>>(reinterpret_cast<float4*>(work), reinterpret_cast<const float2*>(Et),
-                                               nfields, NF / 2, gate, fault_word(), poll_limit, arm_only);
-  ::fame::count_launch();
-  return FAME_OK;
-}
-
+// poll_limit / arm_only: fault-path self-test (fame_selftest_bounded_wait).
 template <int n, typename T, typename TE>
-int launch_passB(C<T>* work, int nfields, const TE* Et, long long NF, cudaStream_t st, Gate gate) {
-#if FAME_FP32_PAIRSPLIT
-  if constexpr (std::is_same<T, float>::value) {
-    static_assert(std::is_same<TE, float>::value, "FP32 chains use the FP32 material tiles");
-    return launch_passB_pk<n>(work, nfields, Et, NF, st, gate);
-  }
-#endif
+int launch_passB(C<T>* work, int nfields, const TE* Et, long long NF, cudaStream_t st, Gate gate,
+                 unsigned poll_limit = kMbarPollLimit, int arm_only = 0) {
   using G = PassBGeom<n, T>;
   constexpr size_t smem = G::template smem_bytes<TE>();
   static int attr = ensure_smem(k_passB<n, T, TE>, smem);
@@ -59,7 +32,7 @@ int launch_passB(C<T>* work, int nfields, const TE* Et, long long NF, cudaStream
   }();
   const int units = (G::n3 / G::TT) * nfields;
   const int grid = std::min(units, per_sm * num_sms());
-  k_passB<n, T, TE><<<grid, G::threads, smem, st>>>(work, Et, nfields, NF, gate, fault_word());
+  k_passB<n, T, TE><<<grid, G::threads, smem, st>>>(work, Et, nfields, NF, gate, fault_word(), poll_limit, arm_only);
   ::fame::count_launch();
   return FAME_OK;
 }
@@ -119,9 +92,10 @@ int run_chain(int n, const Pro& pro, const Epi& epi, C<T>* work, const TE* Et, l
 }
 
 // Columns per CTA of the linear-field passes (one line per thread).
-// n = 10: two columns (200 lines) per CTA, several CTAs per SM (FP64 lines need twice the registers).
+// n = 10: one column (100 lines) per CTA, several CTAs per SM (measured 1-3 % faster K_r^{-1}
+// actions than two columns, in both precision forms).
 template <int n, typename T> struct LinCols {
-  static constexpr int value = n == 10 ? 2
+  static constexpr int value = n == 10 ? 1
                                : n == 2 ? 8 : n == 4 ? 16 : n == 6 ? 12 : n == 8 ? 8 : n == 12 ? 2 : 2;
   static_assert((n * n * n) % value == 0 && value * n * n <= 512, "linear chain tiling");
 };
@@ -129,24 +103,6 @@ template <int n, typename T> struct LinCols {
 template <int n, typename T, int F, int G, class Pro, class Epi, typename TE>
 int chain_lin_g(const Pro& pro, const Epi& epi, C<T>* work, const TE* Et, long long NF,
                 cudaStream_t st, Gate gate) {
-#ifndef FAME_FP32_AC_PACKED
-#define FAME_FP32_AC_PACKED 1
-#endif
-  if constexpr (FAME_FP32_AC_PACKED && FAME_FP32_PAIRSPLIT && std::is_same<T, float>::value) {  // packed passes
-    const size_t smem = (size_t)G * CubePk<n>::S * sizeof(float4);
-    const int threads = round32(G * n * n);
-    static int attrA = ensure_smem(k_passA_lin_pk<n, F, G, Pro>, smem);
-    static int attrC = ensure_smem(k_passC_lin_pk<n, F, G, Epi>, smem);
-    if (attrA != FAME_OK) return attrA;
-    if (attrC != FAME_OK) return attrC;
-    k_passA_lin_pk<n, F, G, Pro><<<(n * n * n) / G, threads, smem, st>>>(pro, work, NF, gate);
-    ::fame::count_launch();
-    FAME_TRY((launch_passB<n, T, TE>(work, F, Et, NF, st, gate)));
-    k_passC_lin_pk<n, F, G, Epi><<<(n * n * n) / G, threads, smem, st>>>(epi, work, NF, gate);
-    ::fame::count_launch();
-    FAME_CUDA_TRY(cudaGetLastError());
-    return FAME_OK;
-  }
   using Q = Cube<n, T>;
   const size_t smem = (size_t)G * Q::size * sizeof(C<T>);
   const int threads = round32(G * Q::n2);
@@ -171,7 +127,7 @@ template <int n, typename T, int F, class Pro, class Epi, typename TE>
 int chain_lin_n(const Pro& pro, const Epi& epi, C<T>* work, const TE* Et, long long NF, cudaStream_t st, Gate gate,
                 int cols) {
   if constexpr (n == 10) {
-    if (cols == 1) return chain_lin_g<n, T, F, 1>(pro, epi, work, Et, NF, st, gate);
+    if (cols == 2) return chain_lin_g<n, T, F, 2>(pro, epi, work, Et, NF, st, gate);
     if (cols == 4) return chain_lin_g<n, T, F, 4>(pro, epi, work, Et, NF, st, gate);
   } else if constexpr (n == 8) {
     if (cols == 2) return chain_lin_g<n, T, F, 2>(pro, epi, work, Et, NF, st, gate);

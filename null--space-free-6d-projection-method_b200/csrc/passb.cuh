@@ -24,10 +24,6 @@
 #include "bulk.cuh"
 #include "fft6d.cuh"
 
-// Register cap of the packed FP32 pass B at 2N <= 10 (tuning constant; 255 = none).
-#ifndef FAME_PASSB32_REGS
-#define FAME_PASSB32_REGS 255
-#endif
 
 namespace fame {
 
@@ -50,7 +46,8 @@ template <int n, typename T> struct PassBGeom {
 
 template <int n, typename T, typename TE>
 __global__ void __launch_bounds__(512) k_passB(C<T>* __restrict__ work, const TE* __restrict__ Et, int nfields,
-                                              long long NF, Gate gate, unsigned* fault) {
+                                              long long NF, Gate gate, unsigned* fault,
+                                              unsigned poll_limit = kMbarPollLimit, int arm_only = 0) {
   if (gate.off()) return;
   using G = PassBGeom<n, T>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -69,6 +66,7 @@ __global__ void __launch_bounds__(512) k_passB(C<T>* __restrict__ work, const TE
     const int k = u / nfields, f = u - k * nfields;
     const bool needE = (u == u0) || (f == 0);
     mbar_arrive_expect_tx(&bar[s], n * G::plane_bytes + (needE ? (unsigned)(G::tile * sizeof(TE)) : 0u));
+    if (arm_only) return;  // fault-path self-test: the bytes never come, nothing is in flight
     const C<T>* src = work + (long long)f * NF + (long long)k * G::tile;
     C<T>* dst = stg + s * G::stage;
 #pragma unroll 1
@@ -96,7 +94,7 @@ __global__ void __launch_bounds__(512) k_passB(C<T>* __restrict__ work, const TE
 #pragma unroll 1
   for (int u = u0, i = 0; u < u1; ++u, ++i) {
     const int s = i & 1;
-    const bool landed = mbar_wait(&bar[s], (unsigned)((i >> 1) & 1));
+    const bool landed = mbar_wait(&bar[s], (unsigned)((i >> 1) & 1), poll_limit);
     if (!__syncthreads_and(landed)) {  // bounded wait, agreed on by the whole CTA
       if (fault && tid == 0) atomicOr(fault, 1u);
       return;
@@ -150,143 +148,6 @@ __global__ void __launch_bounds__(512) k_passB(C<T>* __restrict__ work, const TE
       C<T>* dst = work + (long long)f * NF + (long long)k * G::tile + gout;
 #pragma unroll
       for (int j = 0; j < n; ++j) dst[j * G::TT] = mk<T>(re[j], im[j]);
-    }
-  }
-}
-
-// ---------------------------------------------------------------- FP32, packed
-// FP32 pass B on the pair-split work rows (WorkIO<n, float>): each thread owns two
-// lines (c123 = 2p, 2p+1 of the tile) through all five phases, and every DFT
-// instruction advances both (F2, pk2.cuh).  In shared memory, pair element
-// (p, i4, i5, i6) is one float4 (re_2p, re_2p+1, im_2p, im_2p+1) at float4 index
-// p + Q4*i4 + Q5*i5 + Q6*i6 (Q4 = TT/2, Q5 = Q4*n, Q6 = Q4*n^2 + pad); the pads were
-// chosen by counting 16-byte shared-memory wavefronts of the three line orders
-// (n = 10: 80 wavefronts per phase set against an ideal 75).  The material tile comes
-// with the first unit of each tile by one more bulk copy (two buffers), and the axis-5
-// phase reads its pairs (E_2p, E_2p+1) from shared memory.
-template <int n> struct PassBPkPad {
-  static constexpr int value = n == 8 || n == 10 ? 2 : n >= 12 ? 1 : 4;
-};
-template <int n> struct PassBPkGeom {
-  static constexpr int TT = WorkTile<n, float>::TT, TP = TT / 2;
-  static constexpr int n2 = n * n, n3 = n * n * n;
-  static constexpr int L = TP * n2;  // line pairs per phase (one per working thread)
-  static constexpr int Q4 = TP, Q5 = TP * n, Q6 = TP * n2 + PassBPkPad<n>::value;
-  static constexpr int stage = n * Q6;  // float4 per stage
-  static constexpr int tile = TP * n3;  // float4 per tile of a field (= float2 pairs of the material tile)
-  static constexpr unsigned plane_bytes = (unsigned)(TP * n2 * sizeof(float4));
-  static constexpr int threads = (L + 31) / 32 * 32;
-  static constexpr unsigned e_bytes = (unsigned)(tile * sizeof(float2));  // material tile
-  static constexpr size_t smem_bytes = 2 * (size_t)stage * sizeof(float4) + 2 * (size_t)e_bytes + 2 * sizeof(uint64_t);
-  static constexpr int max_regs = n <= 10 ? FAME_PASSB32_REGS : 255;
-};
-
-// poll_limit / arm_only: fault-path self-test (fame_selftest_bounded_wait); arm_only
-// arms each stage barrier for the unit's bytes and issues no copy, so the bounded
-// wait runs out with nothing in flight.
-template <int n>
-__global__ void __launch_bounds__(PassBPkGeom<n>::threads) __maxnreg__(PassBPkGeom<n>::max_regs)
-    k_passB_pk(float4* __restrict__ work, const float2* __restrict__ Et, int nfields, long long NF4, Gate gate,
-               unsigned* fault, unsigned poll_limit, int arm_only) {
-  if (gate.off()) return;
-  using G = PassBPkGeom<n>;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  float4* stg = reinterpret_cast<float4*>(smem_raw);
-  float2* es = reinterpret_cast<float2*>(smem_raw + 2 * (size_t)G::stage * sizeof(float4));
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * (size_t)G::stage * sizeof(float4) + 2 * (size_t)G::e_bytes);
-  constexpr int tiles = G::n3 / G::TT;
-  const int U = tiles * nfields;
-  const int u0 = (int)((long long)blockIdx.x * U / gridDim.x);
-  const int u1 = (int)((long long)(blockIdx.x + 1) * U / gridDim.x);
-  if (u0 >= u1) return;
-  const int k0 = u0 / nfields;
-  const int tid = threadIdx.x;
-
-  auto issue = [&](int u, int s) {
-    const int k = u / nfields, f = u - k * nfields;
-    const bool needE = (u == u0) || (f == 0);
-    mbar_arrive_expect_tx(&bar[s], n * G::plane_bytes + (needE ? G::e_bytes : 0u));
-    if (arm_only) return;
-    const float4* src = work + (long long)f * NF4 + (long long)k * G::tile;
-    float4* dst = stg + s * G::stage;
-#pragma unroll 1
-    for (int p = 0; p < n; ++p) bulk_g2s(dst + p * G::Q6, src + p * G::TP * G::n2, G::plane_bytes, &bar[s]);
-    if (needE) bulk_g2s(es + ((k - k0) & 1) * G::tile, Et + (long long)k * G::tile, G::e_bytes, &bar[s]);
-  };
-
-  if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
-    mbar_init_fence();
-    issue(u0, 0);
-    if (u0 + 1 < u1) issue(u0 + 1, 1);
-  }
-  __syncthreads();
-
-  const bool act = tid < G::L;
-  const int tp = tid % G::TP, r = tid / G::TP, ra = r % n, rb = r / n;
-  const int b1 = tp + G::Q5 * rb + G::Q6 * ra;  // axis-4 line pair (p, i6 = ra, i5 = rb)
-  const int b2 = tp + G::Q4 * ra + G::Q5 * rb;  // axis-6 line pair (p, i4 = ra, i5 = rb)
-  const int b3 = tp + G::Q4 * ra + G::Q6 * rb;  // axis-5 line pair (p, i4 = ra, i6 = rb)
-  const int gout = tp + G::TP * (n * rb + G::n2 * ra);  // (p, i4 = 0, i5 = rb, i6 = ra) within a tile
-
-#pragma unroll 1
-  for (int u = u0, i = 0; u < u1; ++u, ++i) {
-    const int s = i & 1;
-    const int k = u / nfields, f = u - k * nfields;
-    const float2* Ek = es + ((k - k0) & 1) * G::tile + tid;
-    const bool landed = mbar_wait(&bar[s], (unsigned)((i >> 1) & 1), poll_limit);
-    if (!__syncthreads_and(landed)) {  // bounded wait, agreed on by the whole CTA
-      if (fault && tid == 0) atomicOr(fault, 1u);
-      return;
-    }
-    float4* S = stg + s * G::stage;
-    if (act) line_pk<n, +1>(S + b1, G::Q4);
-    __syncthreads();
-    if (act) line_pk<n, +1>(S + b2, G::Q6);
-    __syncthreads();
-    if (act) {
-      float4* p = S + b3;
-      F2 re[n], im[n];
-#pragma unroll
-      for (int j = 0; j < n; ++j) {
-        const float4 v = p[j * G::Q5];
-        re[j] = F2(make_float2(v.x, v.y));
-        im[j] = F2(make_float2(v.z, v.w));
-      }
-      Dft<n, +1, F2>::run(re, im);
-#pragma unroll
-      for (int j = 0; j < n; ++j) {
-        const F2 e(Ek[j * G::L]);
-        re[j] = re[j] * e;
-        im[j] = im[j] * e;
-      }
-      Dft<n, -1, F2>::run(re, im);
-#pragma unroll
-      for (int j = 0; j < n; ++j) p[j * G::Q5] = make_float4(re[j].v.x, re[j].v.y, im[j].v.x, im[j].v.y);
-    }
-    __syncthreads();
-    if (act) line_pk<n, -1>(S + b2, G::Q6);
-    __syncthreads();
-    F2 re[n], im[n];
-    if (act) {
-#pragma unroll
-      for (int j = 0; j < n; ++j) {
-        const float4 v = S[b1 + j * G::Q4];
-        re[j] = F2(make_float2(v.x, v.y));
-        im[j] = F2(make_float2(v.z, v.w));
-      }
-      Dft<n, -1, F2>::run(re, im);
-    }
-    __syncthreads();  // stage s has been read out: refill it
-    if (tid == 0 && u + 2 < u1) {
-      fence_proxy_async_smem();
-      issue(u + 2, s);
-    }
-    if (act) {
-      float4* dst = work + (long long)f * NF4 + (long long)k * G::tile + gout;
-#pragma unroll
-      for (int j = 0; j < n; ++j) dst[j * G::TP] = make_float4(re[j].v.x, re[j].v.y, im[j].v.x, im[j].v.y);
     }
   }
 }

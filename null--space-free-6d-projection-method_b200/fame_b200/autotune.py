@@ -25,7 +25,7 @@ __all__ = ["tune_krinv_schedule", "DEFAULT_CANDIDATES", "COLUMN_CANDIDATES"]
 
 DEFAULT_CANDIDATES = ((2, 1), (4, 1), (8, 1), (16, 1), (4, 0))
 # passColumns values per grid length 2N (0 = the built-in default)
-COLUMN_CANDIDATES = {6: (0, 4, 6), 8: (0, 2, 4), 10: (0, 1, 4)}
+COLUMN_CANDIDATES = {6: (0, 4, 6), 8: (0, 2, 4), 10: (0, 2, 4)}
 
 
 def tune_krinv_schedule(sys: QSystem, precision="mixed", tolCG=1e-10, maxitCG=3000, candidates=DEFAULT_CANDIDATES,
