@@ -417,7 +417,7 @@ def run_fame(args):
     cpu = None
     parity = None
     if rank == 0 and world == 1:
-        legs = cpu_oracle_legs(N, n3_solve=True)
+        legs = cpu_oracle_legs(N, n3_solve=True, tight=True)
         cpu = cpu_line(legs, steps_in_solve=res_mixed["info"]["steps"])
         parity = gpu_parity(F, legs, ops, sysq, S, dev)
 
@@ -467,7 +467,7 @@ def run_fame(args):
 
 
 # ------------------------------------------------------------ CPU reference
-def cpu_oracle_legs(N, n3_solve=True):
+def cpu_oracle_legs(N, n3_solve=True, tight=False):
     """CPU legs on the host cores, through the oracle only (this function loads no CUDA
     library): (i) one explicit K_r^{-1} action at N on the normalised start vector, with
     the reference algorithm (plain Mhat PCG, tolCG 1e-10: exp1/make_explicit_krinv_compact.m);
@@ -489,6 +489,8 @@ def cpu_oracle_legs(N, n3_solve=True):
     y = op(v0)
     out["action"] = {"N": N, "seconds": time.perf_counter() - t0, "iters": stats()["totalMhatIterations"],
                      "y": y, "v0": v0}
+    if tight:  # the same action at tolCG 1e-13 (untimed): the common exact reference for parity
+        out["action"]["y_tight"] = O.make_explicit_krinv_compact(S, 1e-13, SV["maxitCG"])[0](v0)
     if n3_solve:
         S3 = O.build_q_system(3, W.P_GOLDEN, W.Q_PHYS, O.material_separable_cos(3, 12.0))
         t0 = time.perf_counter()
@@ -518,7 +520,9 @@ def cpu_line(legs, steps_in_solve, kind="port"):
 def gpu_parity(F, legs, ops, sysq, S, dev):
     """Parity of the benchmarked GPU paths against the oracle on the same inputs: the N=5
     K_r^{-1} action on the normalised start vector (both precision forms, and a tight FP64
-    action as the common exact reference), and the N=3 eigenvalues at the benchmark settings
+    action as the common exact reference; at tolCG 1e-10 the oracle's own action is ~3e-9
+    from the exact one, so the GPU and the oracle are also compared with both at tolCG
+    1e-13), and the N=3 eigenvalues at the benchmark settings
     (raw 1/theta and after Rayleigh-Ritz, against the oracle's raw and refined values)."""
     import numpy as np
     import torch
@@ -533,6 +537,8 @@ def gpu_parity(F, legs, ops, sysq, S, dev):
     tight = F.make_explicit_krinv_compact(sysq, 1e-13, 3000, precision="fp64")[0]
     y_t = tight(vd).cpu().numpy()
     out["krinv_n%d_oracle_rel_vs_tight" % a["N"]] = rel(y_o, y_t)
+    if "y_tight" in a:  # both sides at tolCG 1e-13: GPU FP64 vs the oracle
+        out["krinv_n%d_tight_rel_vs_oracle_tight" % a["N"]] = rel(y_t, a["y_tight"])
     for prec in ("fp64", "mixed"):
         y = ops[prec](vd).cpu().numpy()
         out["krinv_n%d_%s_rel_vs_oracle" % (a["N"], prec)] = rel(y, y_o)
