@@ -77,10 +77,14 @@ int ctx_workspace(fame_ctx* ctx, size_t bytes, void** out);
 struct TaylorTcPlan {
   int Npad = 0, stages = 0, ntiles = 0, groups = 0;
   int nsplit = 1, Nc = 0;  // monomial columns split over nsplit CTAs of Nc columns each
+  int Csep = 0;            // columns (of a CTA's Nc) whose cross products accumulate apart
+  bool graded = false;     // the degree-p monomials take the last columns (taylor_tc_columns)
   long long Kc = 0, nslices = 0;
   size_t smem = 0, out_floats = 0;
 };
-TaylorTcPlan taylor_tc_plan(long long NF, int nB, int L);
+TaylorTcPlan taylor_tc_plan(long long NF, int nB, int L, int p);
+// col[a] (Npad entries): output column of monomial a (alist3: L triples a1, a2, a3).
+void taylor_tc_columns(const TaylorTcPlan& plan, const int* alist3, int L, int p, int* col);
 // Centers on a tensor grid: center b = (ax[b % m1], ax[m1 + (b / m1) % m2], ax[m1 + m2 + b / (m1 m2)]).
 struct TaylorTcGrid {
   const double* ax = nullptr;  // device, m1 + m2 + m3 values (nullptr: centers are general)
@@ -89,8 +93,8 @@ struct TaylorTcGrid {
 constexpr int kTaylorTcMaxAxis = 24;  // m1 + m2 + m3 at most for the factorised phases
 // gamma[b L + a] = coef[a] sum_j c_j e^{i q_j.r_b} q_j^a, with alistPacked[a] = a1 | a2 << 8 | a3 << 16.
 int taylor_moments_tc(const TaylorTcPlan& plan, cudaStream_t s, const double2* c, const double* Q, long long NF,
-                      const double* centers, int nB, const int* alistPacked, int L, int p, const double2* coef,
-                      float* out, double2* gamma, const TaylorTcGrid& grid);
+                      const double* centers, int nB, const int* alistPacked, const int* col, int L, int p,
+                      const double2* coef, float* out, double2* gamma, const TaylorTcGrid& grid);
 // Batched complex GEMM C = A B (FP64 complex, element strides) as split-FP32
 // (3xTF32) tcgen05 products (zgemm_tc.cu).
 int zgemm_3xtf32(const double2* A, const double2* B, double2* C, int M, int N, int K, long long sam, long long sak,

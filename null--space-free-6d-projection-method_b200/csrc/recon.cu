@@ -441,18 +441,22 @@ static int taylor_impl(fame_ctx* ctx, const void* coeff, const double* qModes, l
   const int L = (int)cf.size();
   if (L > 512) return fail(FAME_ERR_UNSUPPORTED, "too many Taylor terms");
   const int nChunks = (int)((NF + kTayChunk - 1) / kTayChunk);
-  const TaylorTcPlan tp = tc ? taylor_tc_plan(NF, nBlocks, L) : TaylorTcPlan{};
-  std::vector<int> packed;
-  if (tc)
+  const TaylorTcPlan tp = tc ? taylor_tc_plan(NF, nBlocks, L, p) : TaylorTcPlan{};
+  std::vector<int> packed, tcol;
+  if (tc) {
     for (int a = 0; a < L; ++a) packed.push_back(al[3 * a] | al[3 * a + 1] << 8 | al[3 * a + 2] << 16);
+    tcol.resize(tp.Npad);
+    taylor_tc_columns(tp, al.data(), L, p, tcol.data());
+  }
   cudaStream_t s = ctx->stream;
-  int *dal, *dpk;
+  int *dal, *dpk, *dcol;
   double2 *dcf, *partial, *gamma;
   double *centers, *dfix, *dax;
   float* tout;
   auto carve = [&](Carve& cv) {
     dal = cv.take<int>(al.size());
     dpk = cv.take<int>(tc ? packed.size() : 1);
+    dcol = cv.take<int>(tc ? tcol.size() : 1);
     dcf = cv.take<double2>(cf.size());
     partial = cv.take<double2>(tc ? 1 : (size_t)nChunks * nBlocks * L);
     gamma = cv.take<double2>((size_t)nBlocks * L);
@@ -484,6 +488,7 @@ static int taylor_impl(fame_ctx* ctx, const void* coeff, const double* qModes, l
       ::fame::count_launch();
     } else {
       cudaMemcpyAsync(dpk, packed.data(), packed.size() * sizeof(int), cudaMemcpyHostToDevice, s);
+      cudaMemcpyAsync(dcol, tcol.data(), tcol.size() * sizeof(int), cudaMemcpyHostToDevice, s);
       // centers on a tensor grid (the Yee block partition's are): the moment kernel then
       // factorises the phases per axis
       TaylorTcGrid grid;
@@ -494,8 +499,8 @@ static int taylor_impl(fame_ctx* ctx, const void* coeff, const double* qModes, l
         grid.ax = dax;
       }
       cudaGetLastError();
-      st = taylor_moments_tc(tp, s, (const double2*)coeff, qModes, NF, centers, nBlocks, dpk, L, p, dcf, tout, gamma,
-                             grid);
+      st = taylor_moments_tc(tp, s, (const double2*)coeff, qModes, NF, centers, nBlocks, dpk, dcol, L, p, dcf, tout,
+                             gamma, grid);
     }
     // one grid column per block; x-extent covers the largest block
     std::vector<long long> hp(nBlocks + 1);

@@ -4,11 +4,10 @@
 // (exp2/taylor_on_blocks_exp3.m:53-54,65-73: the moment GEMM Qalpha^T (c .* phase)).
 //
 // One CTA owns a slice of Kc modes, a tile of 64 block centers and Nc of the
-// monomial columns (the columns are split over two CTAs when 2 Nc would exceed the
-// 512 TMEM columns).  Per stage of 32 modes its threads write into shared memory, in
+// monomial columns.  Per stage of 32 modes its threads write into shared memory, in
 // the 128-byte swizzled K-major UMMA layout and split into TF32 head + tail (3xTF32):
 //   A (128 x 32): rows 2b, 2b+1 = Re, Im of c_j exp(i q_j . r_b)
-//   B (Nc x 32):  row a = qx^a1 qy^a2 qz^a3                           (FP64 products)
+//   B (Nc x 32):  row col(a) = qx^a1 qy^a2 qz^a3                       (FP64 products)
 // When the block centers form a tensor grid (the Yee block partition does), the
 // phase factorises per axis, exp(i q.r_b) = ex(bx) ey(by) ez(bz): the generators
 // first tabulate the m1 + m2 + m3 axis phases of the stage's 32 modes in shared
@@ -16,14 +15,19 @@
 // products per center; otherwise each center's phase is reduced in FP64 and taken
 // by sincosf.  Fifteen generator warps fill a stage and arrive on its "full"
 // mbarrier; a sixteenth warp waits for it and issues tcgen05.mma kind::tf32 with
-// Ahi*Bhi into one FP32 TMEM accumulator (columns [0, Nc)) and Ahi*Blo + Alo*Bhi into
-// a second one (columns [Nc, 2 Nc)): the tensor cores round each FP32 accumulation
-// toward zero, and keeping the 2^-11 smaller cross products apart leaves the large
-// head*head sum with a third of the roundings.  It commits to the stage's "empty"
-// mbarrier while the generators fill the other stage.  The epilogue adds the two
-// accumulators and writes the slice's partial moments (FP32); a second kernel sums
-// the slices in FP64 in a fixed order.  Neither Qalpha (L x NF) nor the phase matrix
-// ever exists in HBM: the kernel reads 40 bytes per mode.
+// Ahi*Bhi into one FP32 TMEM accumulator (columns [0, Nc)) and Ahi*Blo + Alo*Bhi of
+// the first Csep columns into a second one (columns [Nc, Nc + Csep)): the tensor
+// cores round each FP32 accumulation toward zero, and keeping the 2^-11 smaller
+// cross products apart leaves the large head*head sum with a third of the
+// roundings.  The cross products of columns [Csep, Nc) accumulate into the head*head
+// columns.  The host places the monomials of degree p, whose moments weigh least in
+// the Taylor sum, in those last columns (col() is a permutation), and splits the
+// columns over two CTAs only when even then the degree < p columns would not fit in
+// the 512 TMEM columns.  It commits to the stage's "empty" mbarrier while the
+// generators fill the other stage.  The epilogue adds the two accumulators and
+// writes the slice's partial moments (FP32); a second kernel sums the slices in FP64
+// in a fixed order.  Neither Qalpha (L x NF) nor the phase matrix ever exists in
+// HBM: the kernel reads 40 bytes per mode.
 #include "internal.cuh"
 #include "umma.cuh"
 
@@ -61,7 +65,8 @@ struct TcArgs {
   const double* centers;  // nB x 3
   int nB;
   const int* alist;     // L packed multi-indices a1 | a2 << 8 | a3 << 16
-  int L, p, Npad, Nc, stages;
+  const int* col;       // Npad: output column of monomial a (identity past L)
+  int L, p, Npad, Nc, Csep, stages;
   long long Kc;
   float* out;           // [slice][tile][128][Npad]
   const double* ax;     // tensor-grid centers (or nullptr)
@@ -89,8 +94,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_taylor_moments_tc(TcArgs a, uns
   const int Nc = a.Nc, S = a.stages;
   const uint32_t bB = b_bytes(Nc), stB = stage_bytes(Nc);
   double* cen = reinterpret_cast<double*>(sm + (size_t)S * stB);  // [kBT][3]
-  int* al = reinterpret_cast<int*>(cen + kBT * 3);                  // [kLmax]
-  float2* tab = reinterpret_cast<float2*>(al + kLmax);              // [2][kMaxAxis][kKC]
+  int* col = reinterpret_cast<int*>(cen + kBT * 3);                 // [kLmax]: column of monomial c0 + r
+  float2* tab = reinterpret_cast<float2*>(col + kLmax);             // [2][kMaxAxis][kKC]
   double* axv = reinterpret_cast<double*>(tab + 2 * kMaxAxis * kKC);  // [kMaxAxis]
   uint64_t* full = reinterpret_cast<uint64_t*>(axv + kMaxAxis);     // [2]: stage written
   uint64_t* empty = full + 2;                                       // [2]: stage read by the MMAs
@@ -107,10 +112,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_taylor_moments_tc(TcArgs a, uns
   const int nbl = a.nB - bt * kBT < kBT ? a.nB - bt * kBT : kBT;
   const bool factored = a.ax != nullptr;
   const int nax = factored ? a.m1 + a.m2 + a.m3 : 0;
-  const uint32_t need = 2u * (uint32_t)Nc;
+  const int Csep = a.Csep;
+  const uint32_t need = (uint32_t)(Nc + Csep);
   const uint32_t ncols = need <= 32 ? 32u : need <= 64 ? 64u : need <= 128 ? 128u : need <= 256 ? 256u : 512u;
 
-  for (int t = tid; t < a.L; t += kThreads) al[t] = a.alist[t];
+  for (int t = tid; t < Nc; t += kThreads) col[t] = a.col[c0 + t] - c0;
   for (int t = tid; t < kBT * 3; t += kThreads) cen[t] = t / 3 < nbl ? a.centers[(long long)bt * kBT * 3 + t] : 0.0;
   for (int t = tid; t < nax; t += kThreads) axv[t] = a.ax[t];
   if (tid == 0) {
@@ -147,7 +153,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_taylor_moments_tc(TcArgs a, uns
       return w >= kGenWarps ? Nc : rs;
     };
     const int r0 = row_start(warp), r1 = row_start(warp + 1);
-    const int e0 = c0 + r0 < a.L ? al[c0 + r0] : 0;
+    const int e0 = c0 + r0 < a.L ? a.alist[c0 + r0] : 0;
     double cx[kBPW], cy[kBPW], cz[kBPW];
     int tx[kBPW], ty[kBPW], tz[kBPW];  // axis-table rows of the centers (factorised phases)
 #pragma unroll
@@ -243,8 +249,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_taylor_moments_tc(TcArgs a, uns
         for (int r = r0; r < rL; ++r) {
           float h, l;
           umma::tf32_split_f32((float)m, h, l);
-          put(Bhi, r, lane, h);
-          put(Blo, r, lane, l);
+          const int rc = col[r];
+          put(Bhi, rc, lane, h);
+          put(Blo, rc, lane, l);
           if (left3 > 0) {
             --left3;
             m *= qz;
@@ -260,8 +267,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_taylor_moments_tc(TcArgs a, uns
           }
         }
         for (int r = rL > r0 ? rL : r0; r < r1; ++r) {
-          put(Bhi, r, lane, 0.0f);
-          put(Blo, r, lane, 0.0f);
+          put(Bhi, col[r], lane, 0.0f);
+          put(Blo, col[r], lane, 0.0f);
         }
       }
       fence_proxy_async_smem();  // generic-proxy writes -> tensor-core reads
@@ -269,7 +276,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_taylor_moments_tc(TcArgs a, uns
     }
   } else {
     // MMA warp: wait for each stage, issue its 3xTF32 products, release it on completion
-    const uint32_t id = umma::idesc_tf32(128, Nc);
     for (int i = 0; i < nch; ++i) {
       const int s = i % S;
       const bool ok = !*abortf && mbar_wait(&full[s], (unsigned)((i / S) & 1));
@@ -283,12 +289,27 @@ __global__ void __launch_bounds__(kThreads, 1) k_taylor_moments_tc(TcArgs a, uns
         for (int kk = 0; kk < kKC / 8; ++kk) {
           const uint64_t ahi = umma::desc_kmajor_sw128(sa + kk * 32u);
           const uint64_t alo = umma::desc_kmajor_sw128(sa + kABytes + kk * 32u);
-          const uint64_t bhi = umma::desc_kmajor_sw128(sa + 2u * kABytes + kk * 32u);
-          const uint64_t blo = umma::desc_kmajor_sw128(sa + 2u * kABytes + bB + kk * 32u);
+          const uint32_t b0 = sa + 2u * kABytes + kk * 32u;  // B head; the tail follows bB bytes later
           const uint32_t acc = (i | kk) != 0 ? 1u : 0u;
-          umma::mma_tf32(tmem, ahi, bhi, id, acc);                    // head * head
-          umma::mma_tf32(tmem + (uint32_t)Nc, ahi, blo, id, acc);     // cross products
-          umma::mma_tf32(tmem + (uint32_t)Nc, alo, bhi, id, 1u);
+          // head * head over all Nc columns, at most 256 per MMA (B row c starts c * 128 bytes in)
+          for (int c = 0; c < Nc; c += 256) {
+            const int w = Nc - c < 256 ? Nc - c : 256;
+            umma::mma_tf32(tmem + (uint32_t)c, ahi, umma::desc_kmajor_sw128(b0 + c * 128u), umma::idesc_tf32(128, w), acc);
+          }
+          // cross products of columns [0, Csep) into their own accumulator
+          for (int c = 0; c < Csep; c += 256) {
+            const int w = Csep - c < 256 ? Csep - c : 256;
+            const uint32_t id = umma::idesc_tf32(128, w), d = tmem + (uint32_t)(Nc + c);
+            umma::mma_tf32(d, ahi, umma::desc_kmajor_sw128(b0 + bB + c * 128u), id, acc);
+            umma::mma_tf32(d, alo, umma::desc_kmajor_sw128(b0 + c * 128u), id, 1u);
+          }
+          // cross products of columns [Csep, Nc) into the head * head columns (after their
+          // head * head product of this step, which initialises them on the first step)
+          if (Csep < Nc) {
+            const uint32_t id = umma::idesc_tf32(128, Nc - Csep), d = tmem + (uint32_t)Csep;
+            umma::mma_tf32(d, ahi, umma::desc_kmajor_sw128(b0 + bB + Csep * 128u), id, 1u);
+            umma::mma_tf32(d, alo, umma::desc_kmajor_sw128(b0 + Csep * 128u), id, 1u);
+          }
         }
         umma::commit(&empty[s]);
       }
@@ -308,7 +329,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_taylor_moments_tc(TcArgs a, uns
     for (int cb = warp >> 2; cb < Nc / 16; cb += (kGenWarps + 1) / 4) {
       uint32_t hh[16], cr[16];
       umma::ld_32x32b_x16_wait(tmem + lane_base + (uint32_t)(cb * 16), hh);
-      umma::ld_32x32b_x16_wait(tmem + lane_base + (uint32_t)(Nc + cb * 16), cr);
+      if (cb * 16 < Csep) {
+        umma::ld_32x32b_x16_wait(tmem + lane_base + (uint32_t)(Nc + cb * 16), cr);
+      } else {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) cr[u] = 0u;  // +0.0f: these columns hold both sums
+      }
       float4* o = reinterpret_cast<float4*>(orow + cb * 16);
 #pragma unroll
       for (int u = 0; u < 4; ++u)
@@ -342,11 +368,12 @@ __global__ void k_taylor_tc_sum_slices(const float* __restrict__ out, long long 
 
 // gamma[b L + a] = coef[a] * (Re + i Im) of the group sums, groups in order
 __global__ void k_taylor_tc_finish(const double* __restrict__ part, int groups, long long per, int Npad, int L, int nB,
-                                   const double2* __restrict__ coef, double2* __restrict__ gamma) {
+                                   const int* __restrict__ col, const double2* __restrict__ coef,
+                                   double2* __restrict__ gamma) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= (long long)nB * L) return;
   const int b = (int)(t / L), al = (int)(t % L);
-  const long long e = ((long long)(b / kBT) * 128 + 2 * (b % kBT)) * Npad + al;
+  const long long e = ((long long)(b / kBT) * 128 + 2 * (b % kBT)) * Npad + col[al];
   double re = 0.0, im = 0.0;
   for (int g = 0; g < groups; ++g) {
     re += part[(long long)g * per + e];
@@ -358,11 +385,23 @@ __global__ void k_taylor_tc_finish(const double* __restrict__ part, int groups, 
 
 }  // namespace
 
-TaylorTcPlan taylor_tc_plan(long long NF, int nB, int L) {
+TaylorTcPlan taylor_tc_plan(long long NF, int nB, int L, int p) {
   TaylorTcPlan pl{};
   pl.Npad = std::max(32, (L + 31) / 32 * 32);
-  pl.nsplit = 2 * pl.Npad > 512 ? 2 : 1;  // head*head and cross accumulators: 2 Nc <= 512 TMEM columns
-  pl.Nc = pl.Npad / pl.nsplit;             // a multiple of 16
+  // head*head (Nc columns) and cross (Csep columns) accumulators share the 512 TMEM columns
+  const int low = p * (p + 1) * (p + 2) / 6;  // monomials of degree < p
+  if (2 * pl.Npad <= 512) {                   // every column keeps its cross products apart
+    pl.nsplit = 1;
+    pl.Nc = pl.Csep = pl.Npad;
+  } else if (pl.Npad + (low + 15) / 16 * 16 <= 512) {  // all but the degree-p columns do
+    pl.nsplit = 1;
+    pl.Nc = pl.Npad;
+    pl.Csep = (512 - pl.Npad) / 16 * 16;
+    pl.graded = true;
+  } else {  // two CTAs per slice, Npad / 2 columns each, all cross products apart
+    pl.nsplit = 2;
+    pl.Nc = pl.Csep = pl.Npad / 2;  // a multiple of 16
+  }
   pl.stages = tc_smem(pl.Nc, 2) <= 227 * 1024 ? 2 : 1;
   pl.smem = tc_smem(pl.Nc, pl.stages);
   pl.ntiles = (nB + kBT - 1) / kBT;
@@ -378,10 +417,19 @@ TaylorTcPlan taylor_tc_plan(long long NF, int nB, int L) {
   return pl;
 }
 
+void taylor_tc_columns(const TaylorTcPlan& pl, const int* alist3, int L, int p, int* col) {
+  int lo = 0, hi = pl.graded ? p * (p + 1) * (p + 2) / 6 : 0;
+  for (int a = 0; a < pl.Npad; ++a) {
+    const bool top = a < L && alist3[3 * a] + alist3[3 * a + 1] + alist3[3 * a + 2] == p;
+    col[a] = !pl.graded || a >= L ? a : top ? hi++ : lo++;
+  }
+}
+
 int taylor_moments_tc(const TaylorTcPlan& pl, cudaStream_t s, const double2* c, const double* Q, long long NF,
-                      const double* centers, int nB, const int* alistPacked, int L, int p, const double2* coef,
-                      float* out, double2* gamma, const TaylorTcGrid& grid) {
-  if (L > kLmax || L > pl.Npad || p > kPmax || pl.Nc > 256 || pl.Nc % 16 != 0 || pl.smem > 227 * 1024)
+                      const double* centers, int nB, const int* alistPacked, const int* col, int L, int p,
+                      const double2* coef, float* out, double2* gamma, const TaylorTcGrid& grid) {
+  if (L > kLmax || L > pl.Npad || p > kPmax || pl.Nc + pl.Csep > 512 || pl.Nc % 16 != 0 || pl.Csep % 16 != 0 ||
+      pl.Csep > pl.Nc || pl.smem > 227 * 1024)
     return fail(FAME_ERR_UNSUPPORTED, "tensor-core Taylor moments: order too high");
   if (grid.ax && (grid.m1 < 1 || grid.m2 < 1 || grid.m3 < 1 || grid.m1 * grid.m2 * grid.m3 != nB ||
                   grid.m1 + grid.m2 + grid.m3 > kMaxAxis))
@@ -393,7 +441,7 @@ int taylor_moments_tc(const TaylorTcPlan& pl, cudaStream_t s, const double2* c, 
                : FAME_ERR_CUDA;
   }();
   if (attr != FAME_OK) return fail(attr, "tensor-core Taylor moments: shared-memory limit");
-  TcArgs a{Q, c, NF, centers, nB, alistPacked, L, p, pl.Npad, pl.Nc, pl.stages, pl.Kc, out,
+  TcArgs a{Q, c, NF, centers, nB, alistPacked, col, L, p, pl.Npad, pl.Nc, pl.Csep, pl.stages, pl.Kc, out,
            grid.ax, grid.m1, grid.m2, grid.m3};
   dim3 g3((unsigned)pl.nslices, (unsigned)pl.ntiles, (unsigned)pl.nsplit);
   k_taylor_moments_tc<<<g3, kThreads, pl.smem, s>>>(a, fault_word());
@@ -403,7 +451,7 @@ int taylor_moments_tc(const TaylorTcPlan& pl, cudaStream_t s, const double2* c, 
   k_taylor_tc_sum_slices<<<dim3((unsigned)((per + 255) / 256), (unsigned)pl.groups), 256, 0, s>>>(out, pl.nslices, per,
                                                                                                 pl.groups, part);
   k_taylor_tc_finish<<<(unsigned)(((long long)nB * L + 255) / 256), 256, 0, s>>>(part, pl.groups, per, pl.Npad, L, nB,
-                                                                                 coef, gamma);
+                                                                                 col, coef, gamma);
   ::fame::count_launch(2);
   FAME_CUDA_TRY(cudaGetLastError());
   return FAME_OK;

@@ -27,6 +27,9 @@ constexpr int kZM = 64;                        // complex rows per CTA (128 accu
 constexpr int kZKC = 16;                       // complex k per stage
 constexpr int kZStages = 2;
 constexpr uint32_t kZABytes = 128u * 128u;     // one TF32 part of A' per stage
+constexpr int kAPer = kZM * kZKC / kZGenThreads;  // A values per generator thread and stage
+constexpr int kBBatch = 8;                        // B values per generator thread and load batch
+static_assert(kAPer * kZGenThreads == kZM * kZKC, "A tile divides over the generator threads");
 
 __host__ __device__ inline uint32_t zb_bytes(int nt) { return (uint32_t)nt * 128u; }
 __host__ __device__ inline uint32_t zstage_bytes(int nt) { return 2u * (kZABytes + zb_bytes(nt)); }
@@ -95,31 +98,67 @@ __global__ void __launch_bounds__(kZThreads, 1) k_zgemm_3xtf32(ZgArgs g, unsigne
         const int kc0 = i * kZKC;
         unsigned char* Ahi = stg;
         unsigned char* Alo = stg + kZABytes;
-        // A: 64 x 16 complex, consecutive threads along the contiguous dimension
-        for (int idx = tid; idx < kZM * kZKC; idx += kZGenThreads) {
-          const int m = aMfast ? idx % kZM : idx / kZKC, k = aMfast ? idx / kZM : idx % kZKC;
-          double2 v = make_double2(0.0, 0.0);
-          if (m0 + m < g.M && kc0 + k < g.K) v = A[(long long)(m0 + m) * g.sam + (long long)(kc0 + k) * g.sak];
-          float rh, rl, ih, il;
-          umma::tf32_split_fast(v.x, rh, rl);
-          umma::tf32_split_fast(v.y, ih, il);
-          put2(Ahi, 2 * m, 2 * k, rh, -ih);
-          put2(Alo, 2 * m, 2 * k, rl, -il);
-          put2(Ahi, 2 * m + 1, 2 * k, ih, rh);
-          put2(Alo, 2 * m + 1, 2 * k, il, rl);
-        }
-        // B: Nt x 16 complex
         unsigned char* Bhi = stg + 2 * kZABytes;
         unsigned char* Blo = Bhi + bB;
-        for (int idx = tid; idx < Nt * kZKC; idx += kZGenThreads) {
-          const int n = bNfast ? idx % Nt : idx / kZKC, k = bNfast ? idx / Nt : idx % kZKC;
-          double2 v = make_double2(0.0, 0.0);
-          if (n0 + n < g.N && kc0 + k < g.K) v = B[(long long)(kc0 + k) * g.sbk + (long long)(n0 + n) * g.sbn];
-          float rh, rl, ih, il;
-          umma::tf32_split_fast(v.x, rh, rl);
-          umma::tf32_split_fast(v.y, ih, il);
-          put2(Bhi, n, 2 * k, rh, ih);
-          put2(Blo, n, 2 * k, rl, il);
+        // every load of a batch is issued before the first split: the stage then waits for
+        // one global-memory latency per batch instead of one per element
+        auto a_at = [&](int idx, int& m, int& k) {
+          m = aMfast ? idx % kZM : idx / kZKC;
+          k = aMfast ? idx / kZM : idx % kZKC;
+        };
+        auto b_at = [&](int idx, int& n, int& k) {
+          n = bNfast ? idx % Nt : idx / kZKC;
+          k = bNfast ? idx / Nt : idx % kZKC;
+        };
+        // A: 64 x 16 complex (kAPer per thread), with the first batch of B
+        double2 va[kAPer], vb[kBBatch];
+#pragma unroll
+        for (int u = 0; u < kAPer; ++u) {
+          int m, k;
+          a_at(tid + u * kZGenThreads, m, k);
+          va[u] = m0 + m < g.M && kc0 + k < g.K
+                      ? __ldg(A + (long long)(m0 + m) * g.sam + (long long)(kc0 + k) * g.sak)
+                      : make_double2(0.0, 0.0);
+        }
+        const int nB = Nt * kZKC;  // B: Nt x 16 complex
+#pragma unroll 1
+        for (int b0 = 0; b0 < nB; b0 += kBBatch * kZGenThreads) {
+#pragma unroll
+          for (int u = 0; u < kBBatch; ++u) {
+            const int idx = b0 + tid + u * kZGenThreads;
+            int n, k;
+            b_at(idx, n, k);
+            vb[u] = idx < nB && n0 + n < g.N && kc0 + k < g.K
+                        ? __ldg(B + (long long)(kc0 + k) * g.sbk + (long long)(n0 + n) * g.sbn)
+                        : make_double2(0.0, 0.0);
+          }
+          if (b0 == 0) {
+#pragma unroll
+            for (int u = 0; u < kAPer; ++u) {
+              int m, k;
+              a_at(tid + u * kZGenThreads, m, k);
+              float rh, rl, ih, il;
+              umma::tf32_split_fast(va[u].x, rh, rl);
+              umma::tf32_split_fast(va[u].y, ih, il);
+              put2(Ahi, 2 * m, 2 * k, rh, -ih);
+              put2(Alo, 2 * m, 2 * k, rl, -il);
+              put2(Ahi, 2 * m + 1, 2 * k, ih, rh);
+              put2(Alo, 2 * m + 1, 2 * k, il, rl);
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < kBBatch; ++u) {
+            const int idx = b0 + tid + u * kZGenThreads;
+            if (idx < nB) {
+              int n, k;
+              b_at(idx, n, k);
+              float rh, rl, ih, il;
+              umma::tf32_split_fast(vb[u].x, rh, rl);
+              umma::tf32_split_fast(vb[u].y, ih, il);
+              put2(Bhi, n, 2 * k, rh, ih);
+              put2(Blo, n, 2 * k, rl, il);
+            }
+          }
         }
       }
       fence_proxy_async_smem();  // generic-proxy writes -> tensor-core reads
