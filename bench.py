@@ -43,7 +43,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["fame", "reference"], default="fame")
     ap.add_argument("--N", type=int, default=N_BENCH)
-    ap.add_argument("--case", choices=["chain", "pcg", "solve", "yee", "recon", "grad", "osi"], default=None,
+    ap.add_argument("--case", choices=["chain", "pcg", "solve", "yee", "recon", "grad", "osi", "rank1"], default=None,
                     help="run one piece of the step alone (for profiling), print its device time")
     ap.add_argument("--precision", choices=["fp32", "fp64", "mixed"], default="mixed")
     ap.add_argument("--reps", type=int, default=3)
@@ -576,6 +576,8 @@ def run_case(args):
         return grad_case(F, args)
     if args.case == "osi":
         return osi_case(F, args)
+    if args.case == "rank1":
+        return rank1_case(F, args)
     N = args.N
     NF = (2 * N) ** 6
     cfg = F.configs
@@ -641,6 +643,47 @@ def grad_case(F, args):
                       "seconds_solve_recover_adjoint": t, "lambda": lam.tolist(),
                       "dlambda_ddelta": dlam[:, 0].tolist(),
                       "fd_rel_err_ddelta": float(np.max(np.abs(dlam[:, 0] - fd) / np.abs(fd)))}), flush=True)
+
+
+def rank1_case(F, args):
+    """The rank-1 lattice transforms of the radix plan at N (exp1/rank1_exact_fft_scatter.m,
+    exp1/rank1_exact_ifft_gather.m; M = 2N (4N-1)^5): device time of one scatter (embed +
+    length-M FFT) and one gather (length-M inverse FFT + gather), median of ``--reps``, and the
+    HBM rate of their Stockham passes (each pass reads and writes M complex128)."""
+    import numpy as np
+    import torch
+    N = args.N
+    n = 2 * N
+    B = 2 * n - 1
+    NF, M = n ** 6, n * B ** 5
+    codes = np.zeros(NF, dtype=np.int64)
+    tmp = np.arange(NF, dtype=np.int64)
+    for j in range(6):  # exp1/build_radix_exact_rank1_plan_scalar.m:33-41
+        codes += (tmp % n) * B ** j
+        tmp //= n
+    target = (codes + (n - 1) * sum(B ** j for j in range(6))) % M
+    plan = dict(NF=NF, M=M, inputIdx=(codes + 1).astype(np.uint32), targetIdx=(target + 1).astype(np.uint32))
+    x = F.start_vector(7, NF)
+    ts = {"scatter": [], "gather": []}
+    for _ in range(max(1, args.reps) + 1):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record()
+        X = F.rank1_exact_fft_scatter(x, plan)
+        e[1].record()
+        F.rank1_exact_ifft_gather(X, plan)
+        e[2].record()
+        torch.cuda.synchronize()
+        ts["scatter"].append(e[0].elapsed_time(e[1]) / 1e3)
+        ts["gather"].append(e[1].elapsed_time(e[2]) / 1e3)
+    med = {k: sorted(v[1:])[len(v[1:]) // 2] for k, v in ts.items()}
+    passes, m = 0, M
+    for r in (27, 23, 19, 16, 15, 14, 13, 12, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2):
+        while m % r == 0:
+            m //= r
+            passes += 1
+    print(json.dumps({"case": "rank1", "N": N, "M": M, "NF": NF, "passes": passes,
+                      "scatter_s": med["scatter"], "gather_s": med["gather"],
+                      "stockham_gbs_gather": passes * 2 * M * 16 / med["gather"] / 1e9}), flush=True)
 
 
 def osi_case(F, args):

@@ -115,6 +115,22 @@ FAME_API int fame_selftest_bounded_wait(fame_mass* m, unsigned poll_limit);
 FAME_API int fame_applyMij_rank1_exact(fame_mass* m, const uint32_t* inputIdx, const uint32_t* targetIdx,
                               long long M, const void* x, void* y, int nrhs);
 
+/* Replaces rank1_exact_fft_scatter(x,plan) — exp1/rank1_exact_fft_scatter.m:1-13.
+ * Xfft (M x nrhs, column-major, device complex128) = the length-M DFT (MATLAB fft) of the
+ * embedding of x (NF x nrhs) at the plan's 1-based inputIdx (device uint32, NF entries).
+ * M may be any product of factors <= 27 (the radix plans' M = nGrid (2 nGrid - 1)^5 are);
+ * FAME_ERR_UNSUPPORTED otherwise.  FAME_ERR_INVALID for an index outside [1, M]
+ * (rank1_exact_fft_scatter:BadSize is the caller's check of x's NF rows).  Uses
+ * M complex128 of context workspace; synchronises the context's stream. */
+FAME_API int fame_rank1_exact_fft_scatter(fame_ctx* ctx, const void* x, int nrhs, const uint32_t* inputIdx,
+                                          long long NF, long long M, void* Xfft);
+/* Replaces rank1_exact_ifft_gather(Yfft,plan) — exp1/rank1_exact_ifft_gather.m:1-11.
+ * y (NF x nrhs) = ifft(Yfft)(targetIdx) for Yfft (M x nrhs, device complex128, read only)
+ * and the plan's 1-based targetIdx (device uint32, NF).  Same M rule and errors as the
+ * scatter; uses 2 M complex128 of context workspace; synchronises the stream. */
+FAME_API int fame_rank1_exact_ifft_gather(fame_ctx* ctx, const void* Yfft, int nrhs, const uint32_t* targetIdx,
+                                          long long NF, long long M, void* y);
+
 /* ---- block-diagonal basis maps (complex128, n modes, nrhs columns) ---- */
 /* exp1/apply_V_blockdiag.m:1-17: y(3n x nrhs) = V x(2n x nrhs) */
 FAME_API int fame_apply_V_blockdiag(fame_ctx* ctx, const void* x, const void* V11, const void* V12,

@@ -1,4 +1,4 @@
-"""Write twiddles.cuh: cos/sin(2*pi*e/n) for the small FFT radices (n <= 14).
+"""Write twiddles.cuh: cos/sin(2*pi*e/n) for the small FFT radices (n <= 27).
 
 Values are evaluated with 50-digit decimal Taylor series and rounded once to
 binary64, so every constant is the correctly rounded value.
@@ -28,6 +28,7 @@ def _pi():
 
 
 PI = _pi()
+NMAX = 27  # the 6D passes use n <= 14; the length-M rank-1 FFT radices go to 27
 
 
 def _cos_sin(frac):
@@ -48,20 +49,20 @@ def _cos_sin(frac):
 
 def main():
     cases_c, cases_s = [], []
-    for n in range(1, 15):
+    for n in range(1, NMAX + 1):
         for e in range(n):
             c, s = _cos_sin(Fraction(e, n) % 1)
-            cases_c.append(f"    case {n * 16 + e}: return {c!r};")
-            cases_s.append(f"    case {n * 16 + e}: return {s!r};")
+            cases_c.append(f"    case {n * 32 + e}: return {c!r};")
+            cases_s.append(f"    case {n * 32 + e}: return {s!r};")
     out = [
-        "// cos(2*pi*e/n) and sin(2*pi*e/n) for n in [1,14], e in [0,n), correctly",
+        f"// cos(2*pi*e/n) and sin(2*pi*e/n) for n in [1,{NMAX}], e in [0,n), correctly",
         "// rounded to binary64.  Generated by gen_twiddles.py; do not edit.",
         "#pragma once",
         "namespace fame {",
         "__host__ __device__ constexpr double tw_cos(int n, int e) {",
-        "  switch (n * 16 + e) {", *cases_c, "    default: return 0.0;", "  }", "}",
+        "  switch (n * 32 + e) {", *cases_c, "    default: return 0.0;", "  }", "}",
         "__host__ __device__ constexpr double tw_sin(int n, int e) {",
-        "  switch (n * 16 + e) {", *cases_s, "    default: return 0.0;", "  }", "}",
+        "  switch (n * 32 + e) {", *cases_s, "    default: return 0.0;", "  }", "}",
         "}  // namespace fame", "",
     ]
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "twiddles.cuh")

@@ -54,9 +54,9 @@ namespace fame {
 // device allocation helpers recorded for cleanup by the owner
 int dalloc(void** p, size_t bytes);
 void dfree(void* p);
-// While alive, dalloc/dfree of this host thread allocate from the device's default
-// memory pool in the order of stream s (all work on the blocks must be queued on s):
-// frees then no longer synchronise the whole device.  Used by concurrent solves.
+// While alive, dalloc/dfree of this host thread allocate from the library's memory
+// pool in the order of stream s (all work on the blocks must be queued on s): frees
+// then no longer synchronise the whole device.  Used by concurrent solves.
 struct StreamOrderedAlloc {
   explicit StreamOrderedAlloc(cudaStream_t s);
   ~StreamOrderedAlloc();

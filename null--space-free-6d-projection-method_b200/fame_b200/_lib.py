@@ -80,6 +80,8 @@ SIGNATURES = {
     "fame_mass_apply": [P, I, P, P, I, I],
     "fame_selftest_bounded_wait": [P, C.c_uint],
     "fame_applyMij_rank1_exact": [P, P, P, LL, P, P, I],
+    "fame_rank1_exact_fft_scatter": [P, P, I, P, LL, LL, P],
+    "fame_rank1_exact_ifft_gather": [P, P, I, P, LL, LL, P],
     "fame_apply_V_blockdiag": [P, P, P, P, P, P, P, P, LL, I, P],
     "fame_apply_VH_blockdiag": [P, P, P, P, P, P, P, P, LL, I, P],
     "fame_solveV1_blockdiag": [P, P, P, P, P, P, P, LL, I, P],

@@ -22,7 +22,7 @@ __all__ = [
     "solveV1_blockdiag", "solveV1H_blockdiag", "QSystem", "build_q_system",
     "make_explicit_krinv_compact", "make_nested_krinv_instrumented", "KrInv", "Lanczos",
     "start_vector", "FameError", "apply_Mhat_C_scalar_compact", "kernel_launches", "solve_batch",
-    "rayleigh_ritz",
+    "rayleigh_ritz", "rank1_exact_fft_scatter", "rank1_exact_ifft_gather",
 ]
 
 
@@ -187,6 +187,40 @@ class MassBackend:
             self.close()
         except Exception:
             pass
+
+
+def _plan_idx(plan, key, dev):
+    return torch.as_tensor(np.ascontiguousarray(np.asarray(plan[key], dtype=np.uint32).ravel()).view(np.int32)).to(dev)
+
+
+def rank1_exact_fft_scatter(x, plan, ctx: Context | None = None):
+    """exp1/rank1_exact_fft_scatter.m:1-13 — Xfft = fft of x embedded at plan.inputIdx (length plan.M).
+
+    ``plan`` needs ``NF``, ``M`` and the 1-based ``inputIdx`` (uint32); x is NF or NF x nrhs
+    complex128 on the device; the result is M or M x nrhs.
+    """
+    ctx = ctx or default_context()
+    xc, n, k = _colmajor(x)
+    NF, M = int(plan["NF"]), int(plan["M"])
+    if n != NF:
+        raise FameError(L.FAME_ERR_INVALID, "rank1_exact_fft_scatter:BadSize")
+    X, view = _new_colmajor(M, k, x)
+    call("fame_rank1_exact_fft_scatter", ctx.bind(), _ptr(xc), k, _ptr(_plan_idx(plan, "inputIdx", x.device)), NF, M,
+         _ptr(X))
+    return X if view is None else view
+
+
+def rank1_exact_ifft_gather(Yfft, plan, ctx: Context | None = None):
+    """exp1/rank1_exact_ifft_gather.m:1-11 — y = ifft(Yfft) at plan.targetIdx (NF rows)."""
+    ctx = ctx or default_context()
+    Yc, m, k = _colmajor(Yfft)
+    NF, M = int(plan["NF"]), int(plan["M"])
+    if m != M:
+        raise FameError(L.FAME_ERR_INVALID, "rank1_exact_ifft_gather:BadSize")
+    y, view = _new_colmajor(NF, k, Yfft)
+    call("fame_rank1_exact_ifft_gather", ctx.bind(), _ptr(Yc), k, _ptr(_plan_idx(plan, "targetIdx", Yfft.device)),
+         NF, M, _ptr(y))
+    return y if view is None else view
 
 
 def _map(name, x, diags, n, rows_in, rows_out, ctx):

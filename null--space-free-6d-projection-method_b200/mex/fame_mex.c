@@ -17,6 +17,8 @@
  *   s = fame_mex('krinv_stats', k)                   struct with the init_stats totals
  *   [ev, ew, iter, info] = fame_mex('lanczos', k, nev, tol, maxiter, p, v0)
  *   [lambda, relres] = fame_mex('rayleigh_ritz', b, h, Y)   Y refined in place (returned as 3rd output)
+ *   X = fame_mex('rank1_exact_fft_scatter', x, plan)  plan: struct with M, NF, inputIdx (uint32, 1-based)
+ *   y = fame_mex('rank1_exact_ifft_gather', Y, plan)  plan: struct with M, NF, targetIdx
  *   fame_mex('destroy', handle)                      any handle made above
  * Handles are uint64 scalars; all work is ordered on the legacy default stream (as MATLAB's
  * GPU operations) and synchronised before the gateway returns.
@@ -264,6 +266,36 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     else mxDestroyArray(rel);
     if (nlhs > 2) plhs[2] = mxGPUCreateMxArrayOnGPU(gY);
     mxGPUDestroyGPUArray(gY);
+  } else if (!strcmp(cmd, "rank1_exact_fft_scatter") || !strcmp(cmd, "rank1_exact_ifft_gather")) {
+    /* exp1/rank1_exact_fft_scatter.m:1-13, exp1/rank1_exact_ifft_gather.m:1-11 */
+    const int scatter = !strcmp(cmd, "rank1_exact_fft_scatter");
+    const mxArray* plan = prhs[2];
+    const mxArray* fi = mxGetField(plan, 0, scatter ? "inputIdx" : "targetIdx");
+    const long long M = (long long)field_or(plan, "M", -1), NF = (long long)field_or(plan, "NF", -1);
+    const void *x, *idx;
+    void* y;
+    mwSize r, c;
+    const mxGPUArray* gx = gpu_in(prhs[1], mxDOUBLE_CLASS, mxCOMPLEX, &x, &r, &c);
+    const mxGPUArray* gi;
+    mxGPUArray* gy;
+    if (!fi || M <= 0 || NF <= 0) mexErrMsgIdAndTxt("fame:BadPlan", "plan needs M, NF and the index vector");
+    if ((long long)r != (scatter ? NF : M))
+      mexErrMsgIdAndTxt(scatter ? "rank1_exact_fft_scatter:BadSize" : "rank1_exact_ifft_gather:BadSize",
+                        scatter ? "x must have plan.NF rows." : "Yfft must have plan.M rows.");
+    gi = mxGPUCreateFromMxArray(fi);  /* a host index vector is copied to the device */
+    if (mxGPUGetClassID(gi) != mxUINT32_CLASS || (long long)mxGPUGetNumberOfElements(gi) != NF)
+      mexErrMsgIdAndTxt("fame:BadPlan", "the plan's index vector must be uint32 with NF entries");
+    idx = mxGPUGetDataReadOnly(gi);
+    gy = gpu_out((mwSize)(scatter ? M : NF), c, mxDOUBLE_CLASS, &y);
+    if (scatter)
+      check(fame_rank1_exact_fft_scatter(ctx(), x, (int)c, (const uint32_t*)idx, NF, M, y));
+    else
+      check(fame_rank1_exact_ifft_gather(ctx(), x, (int)c, (const uint32_t*)idx, NF, M, y));
+    check(fame_ctx_sync(ctx()));
+    plhs[0] = mxGPUCreateMxArrayOnGPU(gy);
+    mxGPUDestroyGPUArray(gx);
+    mxGPUDestroyGPUArray(gi);
+    mxGPUDestroyGPUArray(gy);
   } else if (!strcmp(cmd, "destroy")) {
     handle_t* h = unwrap(prhs[1], 0);
     check(fame_ctx_sync(ctx()));

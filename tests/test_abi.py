@@ -102,6 +102,24 @@ def test_twiddle_header_is_generated_and_exact():
     pkg = os.path.join(ROOT, "null--space-free-6d-projection-method_b200", "csrc")
     txt = open(os.path.join(pkg, "twiddles.cuh")).read()
     vals = dict(re.findall(r"case (\d+): return ([-0-9.e]+);", txt.split("tw_sin")[0]))
-    assert float(vals[str(5 * 16 + 1)]) == math.cos(2 * math.pi / 5) or \
-        abs(float(vals[str(5 * 16 + 1)]) - math.cos(2 * math.pi / 5)) < 1e-16
-    assert float(vals[str(3 * 16 + 1)]) == -0.5
+    assert float(vals[str(5 * 32 + 1)]) == math.cos(2 * math.pi / 5) or \
+        abs(float(vals[str(5 * 32 + 1)]) - math.cos(2 * math.pi / 5)) < 1e-16
+    assert float(vals[str(3 * 32 + 1)]) == -0.5
+    # every length up to 27 (the rank-1 FFT radices), within a few ulps of libm on a rounded argument
+    for n in range(1, 28):
+        for e in range(n):
+            assert abs(float(vals[str(n * 32 + e)]) - math.cos(2 * math.pi * e / n)) < 2e-15, (n, e)
+
+
+def test_mex_gateway_compiles_against_the_c_abi():
+    """mex/fame_mex.c type-checks against include/fame.h (MATLAB's API declared by stubs)."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("gcc not available")
+    src = os.path.join(ROOT, "null--space-free-6d-projection-method_b200", "mex", "fame_mex.c")
+    r = subprocess.run([gcc, "-std=c99", "-fsyntax-only", "-Wall", "-Wextra", "-Wno-unused-parameter", "-Werror",
+                        "-I", os.path.join(ROOT, "tests", "mex_stub"), "-I", os.path.join(ROOT, "include"), src],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
