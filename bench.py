@@ -43,7 +43,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["fame", "reference"], default="fame")
     ap.add_argument("--N", type=int, default=N_BENCH)
-    ap.add_argument("--case", choices=["chain", "pcg", "solve", "yee", "recon", "grad", "osi", "rank1"], default=None,
+    ap.add_argument("--case", choices=["chain", "pcg", "solve", "yee", "recon", "grad", "osi", "rank1", "peaks"],
+                    default=None,
                     help="run one piece of the step alone (for profiling), print its device time")
     ap.add_argument("--precision", choices=["fp32", "fp64", "mixed"], default="mixed")
     ap.add_argument("--reps", type=int, default=3)
@@ -578,6 +579,8 @@ def run_case(args):
         return osi_case(F, args)
     if args.case == "rank1":
         return rank1_case(F, args)
+    if args.case == "peaks":
+        return peaks_case(args)
     N = args.N
     NF = (2 * N) ** 6
     cfg = F.configs
@@ -643,6 +646,42 @@ def grad_case(F, args):
                       "seconds_solve_recover_adjoint": t, "lambda": lam.tolist(),
                       "dlambda_ddelta": dlam[:, 0].tolist(),
                       "fd_rel_err_ddelta": float(np.max(np.abs(dlam[:, 0] - fd) / np.abs(fd)))}), flush=True)
+
+
+def peaks_case(args):
+    """Roofline denominators for the tensor-core and FP64 kernels, measured on this GPU with
+    the vendor library (cuBLAS through torch.matmul; used as the yardstick only, never on the
+    solver path): dense TF32 GEMM and FP64 GEMM throughput, 8192^3, after warm-up, median of
+    ``--reps`` bursts of 10 products timed with CUDA events."""
+    import torch
+    dev = torch.device("cuda", 0)
+    out = {"case": "peaks"}
+    prev = torch.backends.cuda.matmul.allow_tf32
+    try:
+        for name, dt, tf32 in (("tf32_tflops", torch.float32, True), ("fp64_tflops", torch.float64, False),
+                               ("fp32_simt_tflops", torch.float32, False)):
+            torch.backends.cuda.matmul.allow_tf32 = tf32
+            n = 8192
+            a = torch.randn(n, n, dtype=dt, device=dev)
+            b = torch.randn(n, n, dtype=dt, device=dev)
+            c = torch.empty(n, n, dtype=dt, device=dev)
+            for _ in range(3):
+                torch.matmul(a, b, out=c)
+            torch.cuda.synchronize()
+            rates = []
+            for _ in range(max(3, args.reps)):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(10):
+                    torch.matmul(a, b, out=c)
+                e1.record()
+                torch.cuda.synchronize()
+                rates.append(10 * 2 * n ** 3 / (e0.elapsed_time(e1) / 1e3) / 1e12)
+            out[name] = sorted(rates)[len(rates) // 2]
+            del a, b, c
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+    print(json.dumps(out), flush=True)
 
 
 def rank1_case(F, args):

@@ -59,6 +59,37 @@ __global__ void __launch_bounds__(256) k_stockham(const double2* __restrict__ in
   }
 }
 
+// The first pass (Ns = 1): thread j's R outputs are the contiguous run [j R, j R + R), so a
+// warp's direct stores would touch 32 separate segments.  The block's 128 R outputs form one
+// contiguous run: they go through shared memory and leave with consecutive threads on
+// consecutive addresses.
+constexpr int kFirstThreads = 128;
+template <int R, int SIGN>
+__global__ void __launch_bounds__(kFirstThreads) k_stockham_first(const double2* __restrict__ in,
+                                                                  double2* __restrict__ out, long long M) {
+  extern __shared__ double2 stage[];  // [kFirstThreads * R]
+  const long long T = M / R;
+  for (long long j0 = blockIdx.x * (long long)kFirstThreads; j0 < T; j0 += (long long)gridDim.x * kFirstThreads) {
+    const long long j = j0 + threadIdx.x;
+    if (j < T) {
+      double re[R], im[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const double2 v = in[j + r * T];
+        re[r] = v.x;
+        im[r] = v.y;
+      }
+      Dft<R, SIGN, double>::run(re, im);
+#pragma unroll
+      for (int r = 0; r < R; ++r) stage[threadIdx.x * R + r] = make_double2(re[r], im[r]);
+    }
+    __syncthreads();
+    const long long base = j0 * R, len = (T - j0 < kFirstThreads ? T - j0 : kFirstThreads) * R;
+    for (int t = threadIdx.x; t < len; t += kFirstThreads) out[base + t] = stage[t];
+    __syncthreads();  // the stage is rewritten by the next chunk
+  }
+}
+
 // emb (M) = 0 except emb[inputIdx[i] - 1] = x[i]; bad index -> flag (the write is skipped)
 __global__ void k_rank1_scatter(const double2* __restrict__ x, const uint32_t* __restrict__ idx, long long NF,
                                 long long M, double2* __restrict__ emb, unsigned* bad) {
@@ -110,8 +141,19 @@ int launch_pass(int R, const double2* in, double2* out, long long M, long long N
     constexpr int RR = kRadices[I];
     if (R != RR) return launch_pass<SIGN, I + 1>(R, in, out, M, Ns, s);
     const long long T = M / RR;
-    const int blocks = (int)std::min<long long>((T + 255) / 256, (long long)num_sms() * 8);
-    k_stockham<RR, SIGN><<<blocks, 256, 0, s>>>(in, out, M, Ns);
+    if (Ns == 1) {
+      constexpr size_t smem = (size_t)kFirstThreads * RR * sizeof(double2);
+      static int attr = cudaFuncSetAttribute(k_stockham_first<RR, SIGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem) == cudaSuccess
+                            ? FAME_OK
+                            : fail(FAME_ERR_CUDA, "rank-1 FFT: shared-memory limit");
+      FAME_TRY(attr);
+      const int blocks = (int)std::min<long long>((T + kFirstThreads - 1) / kFirstThreads, (long long)num_sms() * 8);
+      k_stockham_first<RR, SIGN><<<blocks, kFirstThreads, smem, s>>>(in, out, M);
+    } else {
+      const int blocks = (int)std::min<long long>((T + 255) / 256, (long long)num_sms() * 8);
+      k_stockham<RR, SIGN><<<blocks, 256, 0, s>>>(in, out, M, Ns);
+    }
     ::fame::count_launch();
     FAME_CUDA_TRY(cudaGetLastError());
     return FAME_OK;

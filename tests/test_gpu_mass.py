@@ -31,7 +31,7 @@ def test_applyMij_fft_fp64_matches_oracle(cuda_device, N):
     assert _rel(y, y_ref) < 1e-13
 
 
-@pytest.mark.parametrize("N", [2, 4, 5])
+@pytest.mark.parametrize("N", [1, 2, 4, 5, 6, 7])
 def test_mass_handles_fp64(cuda_device, N):
     import fame_b200 as F
     NF = (2 * N) ** 6
@@ -56,7 +56,7 @@ def test_mass_handles_fp64(cuda_device, N):
     assert _rel(c12[:NF], O.mass_stencil_bandlimited(x12[:NF], N, 12.0)) < 1e-13
 
 
-@pytest.mark.parametrize("N", [2, 3, 5, 6])
+@pytest.mark.parametrize("N", [1, 2, 3, 5, 6, 7])
 def test_mass_fp32(cuda_device, N):
     import fame_b200 as F
     NF = (2 * N) ** 6

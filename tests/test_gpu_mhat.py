@@ -70,3 +70,26 @@ def test_mhat_noalloc_matches_oracle(cuda_device, dtype):
     torch.cuda.synchronize()
     err = _rel(y.cpu().numpy().astype(np.complex128), O.apply_Mhat_C_scalar_compact(x, S))
     assert err < TOL[dtype], err
+
+
+@pytest.mark.parametrize("N", [6, 7])
+def test_mhat_hermitian_positive_at_the_largest_grids(cuda_device, N):
+    """2N = 12 and 14 (the largest supported grids, NF = 2,985,984 and 7,529,536): Mhat is
+    Hermitian positive definite (exp1/apply_Mhat_C_scalar_compact.m:8-21 is B^* (I (x) M) B
+    with an isometry B), so <y, Mhat x> = conj(<x, Mhat y>) and <x, Mhat x> > 0, FP64."""
+    import fame_b200 as F
+    E = F.configs.material_separable_cos(N, 12.0, device=cuda_device)
+    m = F.MassBackend(E, N)
+    s = F.build_q_system(m, F.configs.P_GOLDEN, F.configs.Q_PHYS)
+    x = F.start_vector(11, s.NF)
+    y = F.start_vector(12, s.NF)
+    Mx = F.apply_Mhat_C_scalar_compact(x, s)
+    My = F.apply_Mhat_C_scalar_compact(y, s)
+    a = complex(torch.vdot(y, Mx).item())
+    b = complex(torch.vdot(x, My).item()).conjugate()
+    assert abs(a - b) <= 1e-12 * abs(a)
+    q = complex(torch.vdot(x, Mx).item())
+    assert abs(q.imag) <= 1e-12 * q.real and q.real > 0
+    # the material bounds the Rayleigh quotient: 1 <= eps <= 13 and B is an isometry
+    r = q.real / float(torch.vdot(x, x).real.item())
+    assert 1.0 - 1e-12 <= r <= 13.0 + 1e-12
