@@ -134,7 +134,7 @@ class FameError(RuntimeError):
 
 def _load():
     if not os.path.exists(LIB_PATH):
-        raise ImportError("libfame_b200.so is not built (%s); run build.py or __graft_entry__.build()"
+        raise ImportError("libfame_b200.so is not built (%s); run build.py in the package directory"
                           % LIB_PATH)
     lib = C.CDLL(LIB_PATH)
     for name, argt in SIGNATURES.items():

@@ -45,7 +45,7 @@ def main():
     lam2 = O.solve_modes(St, nev=10, p=40, tol=1e-10, tolCG=1e-12)["lam"]
     S3 = O.build_q_system(3, P_GOLDEN, Q_PHYS, O.material_separable_cos(3))
     lam3 = O.solve_modes(S3, nev=10, p=40, tol=1e-10, tolCG=1e-12)["lam"]
-    out["eigs"] = dict(n2_tracking=lam2, n3_baseline=lam3,
+    out["eigs"] = dict(n2_tracking=lam2, n3_golden_cos=lam3,
                        kat_n2=np.array([1.201276300237e-02, 4.496454358674e-02]))
     # Yee-field reconstruction, N=1: direct and multi-center Taylor (p=6, 8 centers)
     S1 = O.build_q_system(1, P_GOLDEN, Q_PHYS, O.material_separable_cos(1))

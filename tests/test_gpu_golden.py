@@ -54,6 +54,27 @@ def test_krinv_and_eigs_vs_fixture(cuda_device, precision):
     assert np.max(np.abs(lam - de["n2_tracking"]) / de["n2_tracking"]) < 1e-10
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_n3_benchmark_system_eigs_vs_fixture(cuda_device, precision):
+    """The 10 smallest eigenvalues of the N=3 benchmark system (golden-ratio P, separable
+    cos material, q = (0.05, 0.04, 0.03)) frozen from the oracle at tol 1e-10, tolCG 1e-12;
+    the GPU solve at the same settings, with and without its Rayleigh-Ritz step."""
+    import fame_b200 as F
+    de = load("eigs")
+    m = F.MassBackend(F.configs.material_separable_cos(3, 12.0, device=cuda_device), 3)
+    s = F.build_q_system(m, F.configs.P_GOLDEN, F.configs.Q_PHYS)
+    op, _ = F.make_explicit_krinv_compact(s, 1e-12, 3000, precision=precision)
+    v0 = F.start_vector(F.configs.SEED, s.nr)
+    Y, theta, _, info = F.Lanczos(op, None, None, s.nr, 10, 1e-10, 30, 40, v0)
+    assert info["converged"]
+    ref = de["n3_golden_cos"]
+    lam = np.sort(1.0 / (theta.cpu().numpy() if torch.is_tensor(theta) else np.asarray(theta)))
+    assert np.max(np.abs(lam - ref) / ref) < 1e-10, lam
+    lam_rr, _ = F.rayleigh_ritz(s, Y)
+    lam_rr = np.sort(np.asarray(lam_rr))
+    assert np.max(np.abs(lam_rr - ref) / ref) < 1e-10, lam_rr
+
+
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
 def test_reference_kat_n5_tracked_modes(cuda_device, precision):
     """exp3/make_config_experiment4.m:38-52, exp3/solve_tracked_modes_exp4.m:37-42: the

@@ -120,7 +120,7 @@ def test_lanczos_reference_kat_n2(cuda_device, precision):
     assert np.max(np.abs(lam - sol["lam"]) / sol["lam"]) < 1e-10
 
 
-def test_lanczos_baseline_n3_fp64_and_mixed(cuda_device):
+def test_lanczos_n3_benchmark_system_fp64_and_mixed(cuda_device):
     """The N=3 benchmark system (golden-ratio P, separable-cos material).
 
     With a tight inner tolerance (1e-12) both precision forms give eigenvalues within
