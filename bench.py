@@ -773,8 +773,8 @@ def osi_case(F, args):
 
 def recon_case(F, cfg, sysq, v0, args):
     """Eigenmode 10 at N=5 on the n = 40 window (h = 0.0125): ``--reps`` times the three
-    components by the batched 3xTF32 direct grid and by 3xTF32 Taylor (p = 10, 4^3 centers),
-    timed per repetition (for profiling the reconstruction kernels)."""
+    components by the batched direct grid (FP64 and 3xTF32) and by 3xTF32 Taylor (p = 10,
+    4^3 centers), timed per repetition (for profiling the reconstruction kernels)."""
     import numpy as np
     import torch
     S = cfg.SOLVE
@@ -788,7 +788,8 @@ def recon_case(F, cfg, sysq, v0, args):
     Qm = F.build_projected_q_modes(sysq)
     blocks = F.build_yee_block_partition(sz, 4)
     out = {}
-    for name, fn in (("direct_3xtf32", lambda: F.reconstruct_fields_direct_grid(x3, sysq, axes, tensor_cores=True)),
+    for name, fn in (("direct_fp64", lambda: F.reconstruct_fields_direct_grid(x3, sysq, axes, tensor_cores=False)),
+                     ("direct_3xtf32", lambda: F.reconstruct_fields_direct_grid(x3, sysq, axes, tensor_cores=True)),
                      ("taylor_3xtf32", lambda: [F.taylor_on_blocks(x3[c * NF:(c + 1) * NF], Qm, pts[c], 10, blocks,
                                                                    tensor_cores=True) for c in range(3)])):
         ts = []

@@ -88,8 +88,12 @@ __global__ void k_pair_permute(const double2* coeff, int n, double2* Cp) {
   }
 }
 
-// Batched complex GEMM C(m,n) = sum_k A(m,k) B(k,n) with element strides,
-// FP64, 32x32 output tile per CTA, 16-deep k tiles in shared memory.
+// Batched complex GEMM C(m,n) = sum_k A(m,k) B(k,n) with element strides, FP64.
+// 16 x 16 threads; each thread owns RM x RN outputs (rows tx + 16 a, columns ty + 16 b), so
+// a CTA covers (16 RM) x (16 RN); the tile shape follows the GEMM's shape (zgemm).  k runs in
+// tiles of 8 through two shared-memory buffers: the global loads of tile t + 1 are issued
+// before the products of tile t, and each operand is read along whichever of its two
+// dimensions is contiguous in memory.
 struct GemmArgs {
   const double2* A;
   const double2* B;
@@ -99,57 +103,119 @@ struct GemmArgs {
   long long bA, bB, bC;  // batch strides (blockIdx.z)
   int bdivB = 1;         // B advances by bB every bdivB batch entries
 };
-constexpr int kGT = 32, kGK = 16;
+constexpr int kGKT = 8;
+template <int RM, int RN>
 __global__ void __launch_bounds__(256) k_zgemm(GemmArgs g) {
-  __shared__ double2 As[kGK][kGT + 1];
-  __shared__ double2 Bs[kGK][kGT + 1];
+  constexpr int TM = 16 * RM, TN = 16 * RN;
+  constexpr int AE = TM * kGKT / 256, BE = TN * kGKT / 256;  // elements per thread and k tile
+  static_assert(AE * 256 == TM * kGKT && BE * 256 == TN * kGKT, "tile loads divide over the threads");
+  __shared__ double2 As[2][kGKT][TM + 1];
+  __shared__ double2 Bs[2][kGKT][TN + 1];
   const double2* A = g.A + g.bA * blockIdx.z;
   const double2* B = g.B + g.bB * (blockIdx.z / g.bdivB);
   double2* Cm = g.C + g.bC * blockIdx.z;
-  const int m0 = blockIdx.x * kGT, n0 = blockIdx.y * kGT;
-  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;  // 16 x 16 threads, 2 x 2 outputs each
-  double2 acc[2][2];
-  for (int a = 0; a < 2; ++a)
-    for (int b = 0; b < 2; ++b) acc[a][b] = make_double2(0.0, 0.0);
-  for (int k0 = 0; k0 < g.K; k0 += kGK) {
-    for (int t = threadIdx.x; t < kGK * kGT; t += blockDim.x) {
-      const int kk = t / kGT, mm = t % kGT;
+  const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN;
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  const bool aMfast = g.sam == 1, bNfast = g.sbn == 1;
+  // element e of this thread in the A (TM x 8) and B (8 x TN) tiles
+  auto a_at = [&](int e, int& mm, int& kk) {
+    const int t = threadIdx.x + 256 * e;
+    mm = aMfast ? t % TM : t / kGKT;
+    kk = aMfast ? t / TM : t % kGKT;
+  };
+  auto b_at = [&](int e, int& nn, int& kk) {
+    const int t = threadIdx.x + 256 * e;
+    nn = bNfast ? t % TN : t / kGKT;
+    kk = bNfast ? t / TN : t % kGKT;
+  };
+  double2 ra[AE], rb[BE];
+  auto load = [&](int k0) {
+#pragma unroll
+    for (int e = 0; e < AE; ++e) {
+      int mm, kk;
+      a_at(e, mm, kk);
       const int m = m0 + mm, k = k0 + kk;
-      As[kk][mm] = (m < g.M && k < g.K) ? A[m * g.sam + k * g.sak] : make_double2(0.0, 0.0);
-      const int nn = t % kGT, kb = t / kGT;
-      const int n = n0 + nn, k2 = k0 + kb;
-      Bs[kb][nn] = (n < g.N && k2 < g.K) ? B[k2 * g.sbk + n * g.sbn] : make_double2(0.0, 0.0);
+      ra[e] = (m < g.M && k < g.K) ? A[m * g.sam + k * g.sak] : make_double2(0.0, 0.0);
     }
-    __syncthreads();
-#pragma unroll 4
-    for (int kk = 0; kk < kGK; ++kk) {
-      double2 a[2], b[2];
-      for (int q = 0; q < 2; ++q) {
-        a[q] = As[kk][tx + 16 * q];
-        b[q] = Bs[kk][ty + 16 * q];
-      }
-      for (int qa = 0; qa < 2; ++qa)
-        for (int qb = 0; qb < 2; ++qb) {
-          acc[qa][qb].x += a[qa].x * b[qb].x - a[qa].y * b[qb].y;
-          acc[qa][qb].y += a[qa].x * b[qb].y + a[qa].y * b[qb].x;
+#pragma unroll
+    for (int e = 0; e < BE; ++e) {
+      int nn, kk;
+      b_at(e, nn, kk);
+      const int n = n0 + nn, k = k0 + kk;
+      rb[e] = (n < g.N && k < g.K) ? B[k * g.sbk + n * g.sbn] : make_double2(0.0, 0.0);
+    }
+  };
+  auto stash = [&](int buf) {
+#pragma unroll
+    for (int e = 0; e < AE; ++e) {
+      int mm, kk;
+      a_at(e, mm, kk);
+      As[buf][kk][mm] = ra[e];
+    }
+#pragma unroll
+    for (int e = 0; e < BE; ++e) {
+      int nn, kk;
+      b_at(e, nn, kk);
+      Bs[buf][kk][nn] = rb[e];
+    }
+  };
+  double2 acc[RM][RN];
+#pragma unroll
+  for (int a = 0; a < RM; ++a)
+#pragma unroll
+    for (int b = 0; b < RN; ++b) acc[a][b] = make_double2(0.0, 0.0);
+  load(0);
+  stash(0);
+  __syncthreads();
+  int buf = 0;
+  for (int k0 = 0; k0 < g.K; k0 += kGKT) {
+    const bool more = k0 + kGKT < g.K;
+    if (more) load(k0 + kGKT);
+#pragma unroll
+    for (int kk = 0; kk < kGKT; ++kk) {
+      double2 a[RM], b[RN];
+#pragma unroll
+      for (int q = 0; q < RM; ++q) a[q] = As[buf][kk][tx + 16 * q];
+#pragma unroll
+      for (int q = 0; q < RN; ++q) b[q] = Bs[buf][kk][ty + 16 * q];
+#pragma unroll
+      for (int qa = 0; qa < RM; ++qa)
+#pragma unroll
+        for (int qb = 0; qb < RN; ++qb) {
+          acc[qa][qb].x = fma(a[qa].x, b[qb].x, fma(-a[qa].y, b[qb].y, acc[qa][qb].x));
+          acc[qa][qb].y = fma(a[qa].x, b[qb].y, fma(a[qa].y, b[qb].x, acc[qa][qb].y));
         }
     }
+    if (more) stash(buf ^ 1);  // buffer buf ^ 1 was last read before the previous barrier
     __syncthreads();
+    buf ^= 1;
   }
-  for (int qa = 0; qa < 2; ++qa)
-    for (int qb = 0; qb < 2; ++qb) {
+#pragma unroll
+  for (int qa = 0; qa < RM; ++qa)
+#pragma unroll
+    for (int qb = 0; qb < RN; ++qb) {
       const int m = m0 + tx + 16 * qa, n = n0 + ty + 16 * qb;
       if (m < g.M && n < g.N) Cm[m * g.scm + n * g.scn] = acc[qa][qb];
     }
 }
 
-int zgemm(const GemmArgs& g, int batch, cudaStream_t s) {
-  dim3 grid((g.M + kGT - 1) / kGT, (g.N + kGT - 1) / kGT, batch);
+template <int RM, int RN> int zgemm_t(const GemmArgs& g, int batch, cudaStream_t s) {
+  dim3 grid((g.M + 16 * RM - 1) / (16 * RM), (g.N + 16 * RN - 1) / (16 * RN), batch);
   if (grid.y > 65535) return fail(FAME_ERR_UNSUPPORTED, "zgemm: N too large");
-  k_zgemm<<<grid, 256, 0, s>>>(g);
+  k_zgemm<RM, RN><<<grid, 256, 0, s>>>(g);
   ::fame::count_launch();
   FAME_CUDA_TRY(cudaGetLastError());
   return FAME_OK;
+}
+
+// 64-wide tiles along a dimension of 256 or more, 32-wide otherwise (the factorised
+// direct sum's GEMMs: T1 = 83 x 10^4, T2 = 83 x 83 batched, u = 6889 x 83 at n = 40, N = 5)
+int zgemm(const GemmArgs& g, int batch, cudaStream_t s) {
+  const bool wm = g.M >= 256, wn = g.N >= 256;
+  if (wm && wn) return zgemm_t<4, 4>(g, batch, s);
+  if (wm) return zgemm_t<4, 2>(g, batch, s);
+  if (wn) return zgemm_t<2, 4>(g, batch, s);
+  return zgemm_t<2, 2>(g, batch, s);
 }
 
 // ------------------------------------------------------------------ Taylor
