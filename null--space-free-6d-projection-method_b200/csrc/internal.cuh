@@ -97,9 +97,11 @@ int taylor_moments_tc(const TaylorTcPlan& plan, cudaStream_t s, const double2* c
                       const double2* coef, float* out, double2* gamma, const TaylorTcGrid& grid);
 // Batched complex GEMM C = A B (FP64 complex, element strides) as split-FP32
 // (3xTF32) tcgen05 products (zgemm_tc.cu).
+// scratch: zgemm_3xtf32_scratch(...) bytes of device memory for the split operand panels.
+size_t zgemm_3xtf32_scratch(int M, int N, int K, int batch, int bdivB);
 int zgemm_3xtf32(const double2* A, const double2* B, double2* C, int M, int N, int K, long long sam, long long sak,
                  long long sbk, long long sbn, long long scm, long long scn, long long bA, long long bB, long long bC,
-                 int batch, cudaStream_t s, int bdivB = 1);
+                 int batch, cudaStream_t s, int bdivB, void* scratch);
 // A Hermitian operator on n-vectors of complex128 for the restarted Lanczos
 // (lanczos.cu): y = A x on ctx's stream; *ws holds the reusable basis workspace.
 struct LanczosOperator {

@@ -386,22 +386,30 @@ static int direct_grid_impl(fame_basis* bs, const void* coeff, int ncomp, const 
   cudaStream_t s = bs->ctx->stream;
   // workspace pieces (per component, consecutive): phase tables, permuted coefficients,
   // two GEMM intermediates
-  auto carve = [&](Carve& cv, double2** Tx, double2** Ty, double2** Tz, double2** Cp, double2** T1, double2** T2) {
+  // the 3xTF32 GEMMs' split operand panels (one GEMM at a time: the largest of the three)
+  const size_t panels = !tc ? 0
+                            : std::max({zgemm_3xtf32_scratch(nx, (int)(n2 * n2), (int)n2, ncomp, 1),
+                                        zgemm_3xtf32_scratch(nx, ny, (int)n2, (int)(ncomp * n2), (int)n2),
+                                        zgemm_3xtf32_scratch(nx * ny, nz, (int)n2, ncomp, 1)});
+  auto carve = [&](Carve& cv, double2** Tx, double2** Ty, double2** Tz, double2** Cp, double2** T1, double2** T2,
+                   unsigned char** Pn) {
     *Tx = cv.take<double2>((size_t)ncomp * nx * n2);
     *Ty = cv.take<double2>((size_t)ncomp * ny * n2);
     *Tz = cv.take<double2>((size_t)ncomp * nz * n2);
     *Cp = cv.take<double2>((size_t)ncomp * NF);
     *T1 = cv.take<double2>((size_t)ncomp * nx * n2 * n2);
     *T2 = cv.take<double2>((size_t)ncomp * nx * ny * n2);
+    *Pn = cv.take<unsigned char>(panels > 0 ? panels : 1);
   };
   double2 *Tx, *Ty, *Tz, *Cp, *T1, *T2;
+  unsigned char* Pn;
   Carve size_only;
-  carve(size_only, &Tx, &Ty, &Tz, &Cp, &T1, &T2);
+  carve(size_only, &Tx, &Ty, &Tz, &Cp, &T1, &T2, &Pn);
   void* ws = nullptr;
   int st = ctx_workspace(bs->ctx, size_only.used, &ws);
   Carve cv;
   cv.base = static_cast<char*>(ws);
-  carve(cv, &Tx, &Ty, &Tz, &Cp, &T1, &T2);
+  carve(cv, &Tx, &Ty, &Tz, &Cp, &T1, &T2, &Pn);
   const double* k = bs->info.kLift;
   if (st == FAME_OK) {
     for (int c = 0; c < ncomp; ++c) {
@@ -428,7 +436,7 @@ static int direct_grid_impl(fame_basis* bs, const void* coeff, int ncomp, const 
     for (int t = 0; t < 3 && st == FAME_OK; ++t) {
       const GemmArgs& g = *gs[t];
       st = tc ? zgemm_3xtf32(g.A, g.B, g.C, g.M, g.N, g.K, g.sam, g.sak, g.sbk, g.sbn, g.scm, g.scn, g.bA, g.bB, g.bC,
-                             batches[t], s, g.bdivB)
+                             batches[t], s, g.bdivB, Pn)
               : zgemm(g, batches[t], s);
     }
   }

@@ -6,71 +6,128 @@
 //   A' row 2m   = (Re A[m,k], -Im A[m,k]) for k = 0..K-1,
 //   A' row 2m+1 = (Im A[m,k],  Re A[m,k]),
 //   B' row n    = (Re B[k,n],  Im B[k,n]),
-// so D[2m][n] = Re C[m,n] and D[2m+1][n] = Im C[m,n].  A CTA owns 64 rows m and up
-// to 256 columns n; per stage of 16 complex k (32 TF32 values of K', one 128-byte
-// swizzle atom) eight generator warps load the FP64 operands, split them and write
-// the swizzled K-major UMMA layout, and a ninth warp issues tcgen05.mma kind::tf32.
-// head*head accumulates in one TMEM accumulator and the two cross products in a
-// second one: the tensor cores round the FP32 accumulation toward zero, and the
-// cross products are 2^-11 smaller, so only the head*head sum carries that bias.
-// The epilogue adds the two accumulators in FP64.
+// so D[2m][n] = Re C[m,n] and D[2m+1][n] = Im C[m,n].
+//
+// Two kernels.  k_zsplit splits each operand once, in a bandwidth-bound pass, into
+// panels already in the shared-memory form of the MMA: per (row tile, stage of 16
+// complex k = 32 TF32 values of K', one 128-byte swizzle atom) a head part and a
+// tail part, each rows x 128 bytes in the 128-byte swizzled K-major UMMA layout,
+// one contiguous block per (tile, stage).  k_zgemm_3xtf32 then streams those blocks:
+// one thread issues a bulk copy per stage (completed on the stage's mbarrier), one
+// thread issues tcgen05.mma kind::tf32 -- head*head into one TMEM accumulator, the two
+// cross products into a second (the tensor cores round the FP32 accumulation toward
+// zero, and the cross products are 2^-11 smaller, so only the head*head sum carries
+// that bias) -- and commits to the stage's release mbarrier; the epilogue (four warps,
+// one per 32 TMEM lanes) adds the two accumulators in FP64.  An A panel tile is 64
+// complex rows (128 accumulator lanes); a B panel tile is Nt <= 256 columns.  Operands
+// shared by several output tiles (the phase tables of the direct sum) are split once
+// instead of once per tile.
 #include "internal.cuh"
 #include "umma.cuh"
 
 namespace fame {
 namespace {
 
-constexpr int kZGenWarps = 8;
-constexpr int kZGenThreads = kZGenWarps * 32;
-constexpr int kZThreads = kZGenThreads + 32;  // + the MMA-issuing warp
-constexpr int kZM = 64;                        // complex rows per CTA (128 accumulator lanes)
-constexpr int kZKC = 16;                       // complex k per stage
-constexpr int kZStages = 2;
-constexpr uint32_t kZABytes = 128u * 128u;     // one TF32 part of A' per stage
-constexpr int kAPer = kZM * kZKC / kZGenThreads;  // A values per generator thread and stage
-constexpr int kBBatch = 8;                        // B values per generator thread and load batch
-static_assert(kAPer * kZGenThreads == kZM * kZKC, "A tile divides over the generator threads");
+constexpr int kZM = 64;                     // complex rows per A tile (128 accumulator lanes)
+constexpr int kZKC = 16;                    // complex k per stage
+constexpr int kZThreads = 128;              // producer (thread 0), MMA issuer (thread 32), epilogue (all)
+constexpr uint32_t kZABytes = 128u * 128u;  // one TF32 part of an A stage
 
 __host__ __device__ inline uint32_t zb_bytes(int nt) { return (uint32_t)nt * 128u; }
 __host__ __device__ inline uint32_t zstage_bytes(int nt) { return 2u * (kZABytes + zb_bytes(nt)); }
-inline size_t zsmem(int nt) { return 1024 + (size_t)kZStages * zstage_bytes(nt) + 128; }
+inline int zstages(int nt) { return zstage_bytes(nt) * 3u + 2048u <= 227u * 1024u ? 3 : 2; }
+inline size_t zsmem(int nt) { return 1024 + (size_t)zstages(nt) * zstage_bytes(nt) + 128; }
 
-struct ZgArgs {
-  const double2* A;
-  const double2* B;
-  double2* C;
-  int M, N, K, Nt;
-  long long sam, sak, sbk, sbn, scm, scn;
-  long long bA, bB, bC;
-  int bdivB;  // B advances by bB every bdivB batch entries
+// Operand panels: element (real row r, K' index kk) of stage ks of tile t of batch b sits at
+// byte ((b * tiles + t) * stages + ks) * 2 * part + half * part + sw128_offset(r, kk),
+// part = real rows per tile * 128 bytes (head: half 0, tail: half 1).
+struct SplitArgs {
+  const double2* src;
+  long long s_row, s_k, s_batch;  // element strides of (complex row, k, batch)
+  int rows, K, batches;
+  int tile_rows;                   // complex rows per tile: 64 (A role) or Nt (B role)
+  int a_role;                      // A: two real rows (Re, -Im), (Im, Re); B: one (Re, Im)
+  unsigned char* out;
 };
 
-__device__ __forceinline__ void put2(unsigned char* base, int row, int k, float x, float y) {
-  *reinterpret_cast<float2*>(base + umma::sw128_offset(row, k)) = make_float2(x, y);
+// One CTA per panel block (batch, tile, stage): the tile's FP64 values are read along the
+// operand's contiguous dimension into shared memory, then written as whole 128-byte rows,
+// 16 bytes (four TF32 values of K' = two complex k) per thread.
+constexpr int kSplitThreads = 256;
+constexpr int kSplitMaxRows = 256;  // complex rows of a tile (B role, Nt <= 256)
+__global__ void __launch_bounds__(kSplitThreads) k_zsplit(SplitArgs a) {
+  extern __shared__ double2 tile_raw[];  // [kZKC][tile_rows + 1]: [k][complex row]
+  const int pitch = a.tile_rows + 1;
+  const int tiles = (a.rows + a.tile_rows - 1) / a.tile_rows;
+  const int stages = (a.K + kZKC - 1) / kZKC;
+  const int ks = blockIdx.x % stages, t = (blockIdx.x / stages) % tiles, b = blockIdx.x / (stages * tiles);
+  const int r0 = t * a.tile_rows, k0 = ks * kZKC, n = a.tile_rows * kZKC;
+  const bool rfast = a.s_row == 1;  // read along the contiguous dimension
+  const double2* src = a.src + (long long)b * a.s_batch;
+  for (int e = threadIdx.x; e < n; e += kSplitThreads) {
+    const int rr = rfast ? e % a.tile_rows : e / kZKC, kk = rfast ? e / a.tile_rows : e % kZKC;
+    const int r = r0 + rr, k = k0 + kk;
+    tile_raw[kk * pitch + rr] = (r < a.rows && k < a.K) ? __ldg(src + (long long)r * a.s_row + (long long)k * a.s_k)
+                                                        : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  const int real_rows = a.tile_rows * (a.a_role ? 2 : 1);
+  const size_t part = (size_t)real_rows * 128u;
+  unsigned char* blk = a.out + ((size_t)((long long)b * tiles + t) * stages + ks) * 2 * part;
+  // 16-byte chunk c of real row R holds K' = 4c .. 4c+3, i.e. complex k = 2c, 2c+1
+  for (int e = threadIdx.x; e < real_rows * 8; e += kSplitThreads) {
+    const int R = e / 8, c = e % 8;
+    float hv[4], lv[4];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const double2 v = tile_raw[(2 * c + h) * pitch + (a.a_role ? R / 2 : R)];
+      float rh, rl, ih, il;
+      umma::tf32_split_fast(v.x, rh, rl);
+      umma::tf32_split_fast(v.y, ih, il);
+      const bool second = a.a_role && (R & 1);  // A rows: (Re, -Im) then (Im, Re)
+      hv[2 * h] = second ? ih : rh;
+      hv[2 * h + 1] = second ? rh : (a.a_role ? -ih : ih);
+      lv[2 * h] = second ? il : rl;
+      lv[2 * h + 1] = second ? rl : (a.a_role ? -il : il);
+    }
+    const uint32_t off = umma::sw128_offset(R, 4 * c);
+    *reinterpret_cast<float4*>(blk + off) = make_float4(hv[0], hv[1], hv[2], hv[3]);
+    *reinterpret_cast<float4*>(blk + part + off) = make_float4(lv[0], lv[1], lv[2], lv[3]);
+  }
 }
+
+struct ZgArgs {
+  const unsigned char* Ap;  // A panels (64-row tiles), per batch
+  const unsigned char* Bp;  // B panels (Nt-row tiles), per B batch
+  double2* C;
+  int M, N, K, Nt, S;
+  long long scm, scn, bC;
+  int bdivB;  // B panel batch = blockIdx.z / bdivB
+};
 
 __global__ void __launch_bounds__(kZThreads, 1) k_zgemm_3xtf32(ZgArgs g, unsigned* fault) {
   extern __shared__ unsigned char smraw[];
   unsigned char* sm = smraw + ((1024u - (smem_u32(smraw) & 1023u)) & 1023u);
-  const int Nt = g.Nt;
+  const int Nt = g.Nt, S = g.S;
   const uint32_t bB = zb_bytes(Nt), stB = zstage_bytes(Nt);
-  uint64_t* full = reinterpret_cast<uint64_t*>(sm + (size_t)kZStages * stB);  // [2]
-  uint64_t* empty = full + 2;                                                 // [2]
-  uint64_t* done = full + 4;
-  uint32_t* slot = reinterpret_cast<uint32_t*>(full + 5);
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm + (size_t)S * stB);  // [S]: stage landed
+  uint64_t* empty = full + S;                                          // [S]: stage read by the MMAs
+  uint64_t* done = full + 2 * S;                                       // every MMA complete
+  uint32_t* slot = reinterpret_cast<uint32_t*>(done + 1);
   volatile int* abortf = reinterpret_cast<volatile int*>(slot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * kZM, n0 = blockIdx.y * Nt;
-  const double2* A = g.A + g.bA * blockIdx.z;
-  const double2* B = g.B + g.bB * (blockIdx.z / g.bdivB);
-  double2* Cm = g.C + g.bC * blockIdx.z;
   const int nch = (g.K + kZKC - 1) / kZKC;
+  const size_t astride = 2 * (size_t)kZABytes, bstride = 2 * (size_t)bB;  // bytes per stage of a tile
+  const unsigned char* Ap = g.Ap + ((size_t)blockIdx.z * gridDim.x + blockIdx.x) * nch * astride;
+  const unsigned char* Bp = g.Bp + ((size_t)(blockIdx.z / g.bdivB) * gridDim.y + blockIdx.y) * nch * bstride;
+  double2* Cm = g.C + g.bC * blockIdx.z;
   const uint32_t ncols = 2 * Nt <= 32 ? 32u : 2 * Nt <= 64 ? 64u : 2 * Nt <= 128 ? 128u : 2 * Nt <= 256 ? 256u : 512u;
 
   if (tid == 0) {
-    for (int s = 0; s < kZStages; ++s) {
-      mbar_init(&full[s], kZGenThreads);
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
     mbar_init(done, 1);
@@ -86,123 +143,60 @@ __global__ void __launch_bounds__(kZThreads, 1) k_zgemm_3xtf32(ZgArgs g, unsigne
   umma::fence_after_sync();
   const uint32_t tmem = *slot;  // columns [0, Nt): head*head; [Nt, 2 Nt): cross products
 
-  if (warp < kZGenWarps) {
-    const bool aMfast = g.sam == 1, bNfast = g.sbn == 1 && g.sbk != 1;
+  if (tid == 0) {
+    // producer: stage i of the A and B panels into buffer i % S once the MMAs of i - S are done
+    int issued = 0;
     for (int i = 0; i < nch; ++i) {
-      const int s = i % kZStages;
-      unsigned char* stg = sm + (size_t)s * stB;
-      bool ok = !*abortf;
-      if (ok && i >= kZStages) ok = mbar_wait(&empty[s], (unsigned)((i / kZStages - 1) & 1));
-      if (!ok) *abortf = 1;
-      if (ok) {
-        const int kc0 = i * kZKC;
-        unsigned char* Ahi = stg;
-        unsigned char* Alo = stg + kZABytes;
-        unsigned char* Bhi = stg + 2 * kZABytes;
-        unsigned char* Blo = Bhi + bB;
-        // every load of a batch is issued before the first split: the stage then waits for
-        // one global-memory latency per batch instead of one per element
-        auto a_at = [&](int idx, int& m, int& k) {
-          m = aMfast ? idx % kZM : idx / kZKC;
-          k = aMfast ? idx / kZM : idx % kZKC;
-        };
-        auto b_at = [&](int idx, int& n, int& k) {
-          n = bNfast ? idx % Nt : idx / kZKC;
-          k = bNfast ? idx / Nt : idx % kZKC;
-        };
-        // A: 64 x 16 complex (kAPer per thread), with the first batch of B
-        double2 va[kAPer], vb[kBBatch];
-#pragma unroll
-        for (int u = 0; u < kAPer; ++u) {
-          int m, k;
-          a_at(tid + u * kZGenThreads, m, k);
-          va[u] = m0 + m < g.M && kc0 + k < g.K
-                      ? __ldg(A + (long long)(m0 + m) * g.sam + (long long)(kc0 + k) * g.sak)
-                      : make_double2(0.0, 0.0);
-        }
-        const int nB = Nt * kZKC;  // B: Nt x 16 complex
-#pragma unroll 1
-        for (int b0 = 0; b0 < nB; b0 += kBBatch * kZGenThreads) {
-#pragma unroll
-          for (int u = 0; u < kBBatch; ++u) {
-            const int idx = b0 + tid + u * kZGenThreads;
-            int n, k;
-            b_at(idx, n, k);
-            vb[u] = idx < nB && n0 + n < g.N && kc0 + k < g.K
-                        ? __ldg(B + (long long)(kc0 + k) * g.sbk + (long long)(n0 + n) * g.sbn)
-                        : make_double2(0.0, 0.0);
-          }
-          if (b0 == 0) {
-#pragma unroll
-            for (int u = 0; u < kAPer; ++u) {
-              int m, k;
-              a_at(tid + u * kZGenThreads, m, k);
-              float rh, rl, ih, il;
-              umma::tf32_split_fast(va[u].x, rh, rl);
-              umma::tf32_split_fast(va[u].y, ih, il);
-              put2(Ahi, 2 * m, 2 * k, rh, -ih);
-              put2(Alo, 2 * m, 2 * k, rl, -il);
-              put2(Ahi, 2 * m + 1, 2 * k, ih, rh);
-              put2(Alo, 2 * m + 1, 2 * k, il, rl);
-            }
-          }
-#pragma unroll
-          for (int u = 0; u < kBBatch; ++u) {
-            const int idx = b0 + tid + u * kZGenThreads;
-            if (idx < nB) {
-              int n, k;
-              b_at(idx, n, k);
-              float rh, rl, ih, il;
-              umma::tf32_split_fast(vb[u].x, rh, rl);
-              umma::tf32_split_fast(vb[u].y, ih, il);
-              put2(Bhi, n, 2 * k, rh, ih);
-              put2(Blo, n, 2 * k, rl, il);
-            }
-          }
-        }
+      const int s = i % S;
+      if (*abortf) break;
+      if (i >= S && !mbar_wait(&empty[s], (unsigned)((i / S - 1) & 1))) {
+        *abortf = 1;
+        break;
       }
-      fence_proxy_async_smem();  // generic-proxy writes -> tensor-core reads
-      mbar_arrive(&full[s]);
+      unsigned char* stg = sm + (size_t)s * stB;
+      mbar_arrive_expect_tx(&full[s], (unsigned)(astride + bstride));
+      bulk_g2s(stg, Ap + (size_t)i * astride, (unsigned)astride, &full[s]);
+      bulk_g2s(stg + astride, Bp + (size_t)i * bstride, (unsigned)bstride, &full[s]);
+      issued = i + 1;
     }
-  } else {
+    // copies issued for stages the MMAs never consumed still land in this CTA's shared
+    // memory: wait for them (bounded) before the CTA may exit
+    if (*abortf)
+      for (int i = issued - S < 0 ? 0 : issued - S; i < issued; ++i) mbar_wait(&full[i % S], (unsigned)((i / S) & 1));
+  } else if (tid == 32) {
     const uint32_t id = umma::idesc_tf32(128, Nt);
     for (int i = 0; i < nch; ++i) {
-      const int s = i % kZStages;
-      const bool ok = !*abortf && mbar_wait(&full[s], (unsigned)((i / kZStages) & 1));
-      if (!ok) {
+      const int s = i % S;
+      if (*abortf || !mbar_wait(&full[s], (unsigned)((i / S) & 1))) {
         *abortf = 1;
         break;
       }
       umma::fence_after_sync();
-      if (lane == 0) {
-        const uint32_t sa = smem_u32(sm + (size_t)s * stB);
-        for (int kk = 0; kk < 2 * kZKC / 8; ++kk) {
-          const uint32_t o = kk * 32u, acc = (i | kk) != 0 ? 1u : 0u;
-          const uint64_t ahi = umma::desc_kmajor_sw128(sa + o), alo = umma::desc_kmajor_sw128(sa + kZABytes + o);
-          const uint64_t bhi = umma::desc_kmajor_sw128(sa + 2u * kZABytes + o);
-          const uint64_t blo = umma::desc_kmajor_sw128(sa + 2u * kZABytes + bB + o);
-          umma::mma_tf32(tmem, ahi, bhi, id, acc);
-          umma::mma_tf32(tmem + (uint32_t)Nt, ahi, blo, id, acc);
-          umma::mma_tf32(tmem + (uint32_t)Nt, alo, bhi, id, 1u);
-        }
-        umma::commit(&empty[s]);
+      const uint32_t sa = smem_u32(sm + (size_t)s * stB);
+      for (int kk = 0; kk < 2 * kZKC / 8; ++kk) {
+        const uint32_t o = kk * 32u, acc = (i | kk) != 0 ? 1u : 0u;
+        const uint64_t ahi = umma::desc_kmajor_sw128(sa + o), alo = umma::desc_kmajor_sw128(sa + kZABytes + o);
+        const uint64_t bhi = umma::desc_kmajor_sw128(sa + 2u * kZABytes + o);
+        const uint64_t blo = umma::desc_kmajor_sw128(sa + 2u * kZABytes + bB + o);
+        umma::mma_tf32(tmem, ahi, bhi, id, acc);
+        umma::mma_tf32(tmem + (uint32_t)Nt, ahi, blo, id, acc);
+        umma::mma_tf32(tmem + (uint32_t)Nt, alo, bhi, id, 1u);
       }
-      __syncwarp();
+      umma::commit(&empty[s]);
     }
-    if (lane == 0) umma::commit(done);
-    __syncwarp();
+    umma::commit(done);  // arrives once every MMA issued above has completed
   }
+  __syncwarp();
   const bool fin = mbar_wait(done, 0u);
   const bool ok = __syncthreads_and(fin && !*abortf);
-  if (ok && warp < kZGenWarps) {
+  if (ok) {
     umma::fence_after_sync();
-    const int q = warp & 3;                       // TMEM lanes 32 q .. 32 q + 31
-    const int m = m0 + (q * 32 + lane) / 2;       // lane pair (2j, 2j+1) = (Re, Im) of row m
+    const int m = m0 + (warp * 32 + lane) / 2;  // TMEM lane pair (2j, 2j+1) = (Re, Im) of row m
     const bool odd = lane & 1;
-    for (int cc = warp >> 2; cc < Nt / 32; cc += kZGenWarps / 4) {
+    for (int cc = 0; cc < Nt / 32; ++cc) {
       uint32_t hh[32], xx[32];
-      umma::ld_32x32b_x32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(cc * 32), hh);
-      umma::ld_32x32b_x32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(Nt + cc * 32), xx);
+      umma::ld_32x32b_x32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cc * 32), hh);
+      umma::ld_32x32b_x32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(Nt + cc * 32), xx);
       umma::wait_ld(hh);
       umma::wait_ld(xx);
       // the even lane stores columns 0..15 of the chunk, the odd lane 16..31
@@ -227,13 +221,44 @@ __global__ void __launch_bounds__(kZThreads, 1) k_zgemm_3xtf32(ZgArgs g, unsigne
   }
 }
 
+inline int z_nt(int N) { return std::min(256, (N + 31) / 32 * 32); }
+inline size_t panel_bytes(int rows, int K, int batches, int tile_rows, bool a_role) {
+  const size_t tiles = (size_t)(rows + tile_rows - 1) / tile_rows, stages = (size_t)(K + kZKC - 1) / kZKC;
+  return (size_t)batches * tiles * stages * 2 * (size_t)tile_rows * (a_role ? 2 : 1) * 128u;
+}
+
+int split(const double2* src, long long s_row, long long s_k, long long s_batch, int rows, int K, int batches,
+          int tile_rows, bool a_role, unsigned char* out, cudaStream_t s) {
+  if (tile_rows > kSplitMaxRows) return fail(FAME_ERR_UNSUPPORTED, "zgemm_3xtf32: panel tile too tall");
+  SplitArgs a{src, s_row, s_k, s_batch, rows, K, batches, tile_rows, a_role ? 1 : 0, out};
+  const long long blocks = (long long)batches * ((rows + tile_rows - 1) / tile_rows) * ((K + kZKC - 1) / kZKC);
+  if (blocks > 0x7fffffffLL) return fail(FAME_ERR_UNSUPPORTED, "zgemm_3xtf32: too many panel blocks");
+  static int attr = cudaFuncSetAttribute(k_zsplit, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(kZKC * (kSplitMaxRows + 1) * sizeof(double2))) == cudaSuccess
+                        ? FAME_OK
+                        : fail(FAME_ERR_CUDA, "zgemm_3xtf32: split shared-memory limit");
+  FAME_TRY(attr);
+  k_zsplit<<<(unsigned)blocks, kSplitThreads, (size_t)kZKC * (tile_rows + 1) * sizeof(double2), s>>>(a);
+  ::fame::count_launch();
+  FAME_CUDA_TRY(cudaGetLastError());
+  return FAME_OK;
+}
+
 }  // namespace
+
+size_t zgemm_3xtf32_scratch(int M, int N, int K, int batch, int bdivB) {
+  const int d = bdivB < 1 ? 1 : bdivB, bbatches = (batch + d - 1) / d;
+  return 1024 + (panel_bytes(M, K, batch, kZM, true) + 1023) / 1024 * 1024 +
+         panel_bytes(N, K, bbatches, z_nt(N), false);
+}
 
 int zgemm_3xtf32(const double2* A, const double2* B, double2* C, int M, int N, int K, long long sam, long long sak,
                  long long sbk, long long sbn, long long scm, long long scn, long long bA, long long bB, long long bC,
-                 int batch, cudaStream_t s, int bdivB) {
-  if (M <= 0 || N <= 0 || K <= 0 || batch <= 0) return fail(FAME_ERR_INVALID, "zgemm_3xtf32: empty shape");
-  const int Nt = std::min(256, (N + 31) / 32 * 32);
+                 int batch, cudaStream_t s, int bdivB, void* scratch) {
+  if (M <= 0 || N <= 0 || K <= 0 || batch <= 0 || !scratch)
+    return fail(FAME_ERR_INVALID, "zgemm_3xtf32: empty shape or no scratch");
+  if (bdivB < 1) return fail(FAME_ERR_INVALID, "zgemm_3xtf32: batch divisor");
+  const int Nt = z_nt(N), S = zstages(Nt);
   const size_t smem = zsmem(Nt);
   static int attr = [] {
     return cudaFuncSetAttribute(k_zgemm_3xtf32, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) ==
@@ -244,8 +269,14 @@ int zgemm_3xtf32(const double2* A, const double2* B, double2* C, int M, int N, i
   if (attr != FAME_OK) return fail(attr, "zgemm_3xtf32: shared-memory limit");
   const long long gy = (N + Nt - 1) / Nt;
   if (gy > 65535 || batch > 65535) return fail(FAME_ERR_UNSUPPORTED, "zgemm_3xtf32: grid too large");
-  if (bdivB < 1) return fail(FAME_ERR_INVALID, "zgemm_3xtf32: batch divisor");
-  ZgArgs g{A, B, C, M, N, K, Nt, sam, sak, sbk, sbn, scm, scn, bA, bB, bC, bdivB};
+  // panels (1024-byte aligned): A' per batch, B' per distinct B (every bdivB batches)
+  unsigned char* base = static_cast<unsigned char*>(scratch);
+  unsigned char* Ap = base + ((1024u - (reinterpret_cast<uintptr_t>(base) & 1023u)) & 1023u);
+  unsigned char* Bp = Ap + (panel_bytes(M, K, batch, kZM, true) + 1023) / 1024 * 1024;
+  const int bbatches = (batch + bdivB - 1) / bdivB;
+  FAME_TRY(split(A, sam, sak, bA, M, K, batch, kZM, true, Ap, s));
+  FAME_TRY(split(B, sbn, sbk, bB, N, K, bbatches, Nt, false, Bp, s));
+  ZgArgs g{Ap, Bp, C, M, N, K, Nt, S, scm, scn, bC, bdivB};
   dim3 grid((unsigned)((M + kZM - 1) / kZM), (unsigned)gy, (unsigned)batch);
   k_zgemm_3xtf32<<<grid, kZThreads, smem, s>>>(g, fault_word());
   ::fame::count_launch();
