@@ -96,12 +96,24 @@ int taylor_moments_tc(const TaylorTcPlan& plan, cudaStream_t s, const double2* c
                       const double* centers, int nB, const int* alistPacked, const int* col, int L, int p,
                       const double2* coef, float* out, double2* gamma, const TaylorTcGrid& grid);
 // Batched complex GEMM C = A B (FP64 complex, element strides) as split-FP32
-// (3xTF32) tcgen05 products (zgemm_tc.cu).
-// scratch: zgemm_3xtf32_scratch(...) bytes of device memory for the split operand panels.
-size_t zgemm_3xtf32_scratch(int M, int N, int K, int batch, int bdivB);
-int zgemm_3xtf32(const double2* A, const double2* B, double2* C, int M, int N, int K, long long sam, long long sak,
-                 long long sbk, long long sbn, long long scm, long long scn, long long bA, long long bB, long long bC,
-                 int batch, cudaStream_t s, int bdivB, void* scratch);
+// (3xTF32) tcgen05 products (zgemm_tc.cu), in two steps: the operands are split into
+// head/tail TF32 panels in the UMMA shared-memory layout (up to four operands per launch),
+// then the GEMM streams the panels.  A panels: rows = M (complex rows m), batches = the
+// GEMM's batch; B panels: rows = N (columns n), cols_for_b = N, batches = the distinct B
+// operands (the GEMM uses B panel batch z / bdivB).  Strides are those of the FP64 operand:
+// A (s_row, s_k) = (sam, sak), B = (sbn, sbk).  Panel buffers are 1024-byte aligned.
+struct ZPanelJob {
+  const double2* src;
+  long long s_row, s_k, s_batch;
+  int rows, K, batches;
+  bool a_role;
+  int cols_for_b;  // B role: the GEMM's N (sets the panel tile)
+  unsigned char* out;
+};
+size_t zpanel_bytes(const ZPanelJob& job);
+int zsplit_panels(const ZPanelJob* jobs, int njobs, cudaStream_t s);
+int zgemm_3xtf32_panels(const unsigned char* Ap, const unsigned char* Bp, double2* C, int M, int N, int K,
+                        long long scm, long long scn, long long bC, int batch, int bdivB, cudaStream_t s);
 // A Hermitian operator on n-vectors of complex128 for the restarted Lanczos
 // (lanczos.cu): y = A x on ctx's stream; *ws holds the reusable basis workspace.
 struct LanczosOperator {

@@ -386,11 +386,16 @@ static int direct_grid_impl(fame_basis* bs, const void* coeff, int ncomp, const 
   cudaStream_t s = bs->ctx->stream;
   // workspace pieces (per component, consecutive): phase tables, permuted coefficients,
   // two GEMM intermediates
-  // the 3xTF32 GEMMs' split operand panels (one GEMM at a time: the largest of the three)
-  const size_t panels = !tc ? 0
-                            : std::max({zgemm_3xtf32_scratch(nx, (int)(n2 * n2), (int)n2, ncomp, 1),
-                                        zgemm_3xtf32_scratch(nx, ny, (int)n2, (int)(ncomp * n2), (int)n2),
-                                        zgemm_3xtf32_scratch(nx * ny, nz, (int)n2, ncomp, 1)});
+  // 3xTF32 operand panels (zgemm_tc.cu): Tx (A of T1), Cp (B of T1), Ty (B of T2), Tz (B of
+  // u), split together before T1; T1 (A of T2) and then T2 (A of u) share one region
+  const int in2 = (int)n2;
+  ZPanelJob jTx{nullptr, 1, nx, (long long)nx * n2, nx, in2, ncomp, true, 0, nullptr};
+  ZPanelJob jCp{nullptr, n2, 1, NF, (int)(n2 * n2), in2, ncomp, false, (int)(n2 * n2), nullptr};
+  ZPanelJob jTy{nullptr, 1, ny, (long long)ny * n2, ny, in2, ncomp, false, ny, nullptr};
+  ZPanelJob jTz{nullptr, 1, nz, (long long)nz * n2, nz, in2, ncomp, false, nz, nullptr};
+  ZPanelJob jT1{nullptr, 1, nx, (long long)nx * n2, nx, in2, ncomp * in2, true, 0, nullptr};
+  ZPanelJob jT2{nullptr, 1, (long long)nx * ny, (long long)nx * ny * n2, nx * ny, in2, ncomp, true, 0, nullptr};
+  const size_t pbig = tc ? std::max(zpanel_bytes(jT1), zpanel_bytes(jT2)) : 0;
   auto carve = [&](Carve& cv, double2** Tx, double2** Ty, double2** Tz, double2** Cp, double2** T1, double2** T2,
                    unsigned char** Pn) {
     *Tx = cv.take<double2>((size_t)ncomp * nx * n2);
@@ -399,7 +404,17 @@ static int direct_grid_impl(fame_basis* bs, const void* coeff, int ncomp, const 
     *Cp = cv.take<double2>((size_t)ncomp * NF);
     *T1 = cv.take<double2>((size_t)ncomp * nx * n2 * n2);
     *T2 = cv.take<double2>((size_t)ncomp * nx * ny * n2);
-    *Pn = cv.take<unsigned char>(panels > 0 ? panels : 1);
+    if (tc) {  // panel buffers start on 1024-byte boundaries of the actual addresses (sizes
+               // are multiples of 1024); the sizing pass reserves the largest padding
+      const uintptr_t at = reinterpret_cast<uintptr_t>(cv.base) + cv.used;
+      cv.used += cv.base ? (1024 - (at & 1023)) & 1023 : 1024;
+      for (ZPanelJob* j : {&jTx, &jCp, &jTy, &jTz}) {
+        j->out = cv.take<unsigned char>((zpanel_bytes(*j) + 1023) / 1024 * 1024);
+      }
+      *Pn = cv.take<unsigned char>(pbig);
+    } else {
+      *Pn = nullptr;
+    }
   };
   double2 *Tx, *Ty, *Tz, *Cp, *T1, *T2;
   unsigned char* Pn;
@@ -433,11 +448,26 @@ static int direct_grid_impl(fame_basis* bs, const void* coeff, int ncomp, const 
                 (long long)nx * ny * n2, (long long)nz * n2, (long long)nx * ny * nz};
     const GemmArgs* gs[3] = {&g1, &g2, &g3};
     const int batches[3] = {ncomp, (int)(ncomp * n2), ncomp};
-    for (int t = 0; t < 3 && st == FAME_OK; ++t) {
-      const GemmArgs& g = *gs[t];
-      st = tc ? zgemm_3xtf32(g.A, g.B, g.C, g.M, g.N, g.K, g.sam, g.sak, g.sbk, g.sbn, g.scm, g.scn, g.bA, g.bB, g.bC,
-                             batches[t], s, g.bdivB, Pn)
-              : zgemm(g, batches[t], s);
+    if (!tc) {
+      for (int t = 0; t < 3 && st == FAME_OK; ++t) st = zgemm(*gs[t], batches[t], s);
+    } else {
+      jTx.src = Tx;
+      jCp.src = Cp;
+      jTy.src = Ty;
+      jTz.src = Tz;
+      jT1.src = T1;
+      jT2.src = T2;
+      jT1.out = jT2.out = Pn;
+      const ZPanelJob first[4] = {jTx, jCp, jTy, jTz};
+      st = zsplit_panels(first, 4, s);
+      if (st == FAME_OK)
+        st = zgemm_3xtf32_panels(jTx.out, jCp.out, T1, g1.M, g1.N, g1.K, g1.scm, g1.scn, g1.bC, ncomp, 1, s);
+      if (st == FAME_OK) st = zsplit_panels(&jT1, 1, s);
+      if (st == FAME_OK)
+        st = zgemm_3xtf32_panels(Pn, jTy.out, T2, g2.M, g2.N, g2.K, g2.scm, g2.scn, g2.bC, ncomp * in2, in2, s);
+      if (st == FAME_OK) st = zsplit_panels(&jT2, 1, s);
+      if (st == FAME_OK)
+        st = zgemm_3xtf32_panels(Pn, jTz.out, (double2*)u, g3.M, g3.N, g3.K, g3.scm, g3.scn, g3.bC, ncomp, 1, s);
     }
   }
   return st;

@@ -55,12 +55,23 @@ struct SplitArgs {
 // 16 bytes (four TF32 values of K' = two complex k) per thread.
 constexpr int kSplitThreads = 256;
 constexpr int kSplitMaxRows = 256;  // complex rows of a tile (B role, Nt <= 256)
-__global__ void __launch_bounds__(kSplitThreads) k_zsplit(SplitArgs a) {
+// several operands in one launch: job j owns blocks [first[j], first[j + 1])
+constexpr int kMaxSplitJobs = 4;
+struct SplitJobs {
+  SplitArgs job[kMaxSplitJobs];
+  int first[kMaxSplitJobs + 1];
+  int njobs;
+};
+__global__ void __launch_bounds__(kSplitThreads) k_zsplit(SplitJobs jobs) {
   extern __shared__ double2 tile_raw[];  // [kZKC][tile_rows + 1]: [k][complex row]
+  int j = 0;
+  while (j + 1 < jobs.njobs && (int)blockIdx.x >= jobs.first[j + 1]) ++j;
+  const SplitArgs& a = jobs.job[j];
+  const int bid = (int)blockIdx.x - jobs.first[j];
   const int pitch = a.tile_rows + 1;
   const int tiles = (a.rows + a.tile_rows - 1) / a.tile_rows;
   const int stages = (a.K + kZKC - 1) / kZKC;
-  const int ks = blockIdx.x % stages, t = (blockIdx.x / stages) % tiles, b = blockIdx.x / (stages * tiles);
+  const int ks = bid % stages, t = (bid / stages) % tiles, b = bid / (stages * tiles);
   const int r0 = t * a.tile_rows, k0 = ks * kZKC, n = a.tile_rows * kZKC;
   const bool rfast = a.s_row == 1;  // read along the contiguous dimension
   const double2* src = a.src + (long long)b * a.s_batch;
@@ -227,37 +238,48 @@ inline size_t panel_bytes(int rows, int K, int batches, int tile_rows, bool a_ro
   return (size_t)batches * tiles * stages * 2 * (size_t)tile_rows * (a_role ? 2 : 1) * 128u;
 }
 
-int split(const double2* src, long long s_row, long long s_k, long long s_batch, int rows, int K, int batches,
-          int tile_rows, bool a_role, unsigned char* out, cudaStream_t s) {
-  if (tile_rows > kSplitMaxRows) return fail(FAME_ERR_UNSUPPORTED, "zgemm_3xtf32: panel tile too tall");
-  SplitArgs a{src, s_row, s_k, s_batch, rows, K, batches, tile_rows, a_role ? 1 : 0, out};
-  const long long blocks = (long long)batches * ((rows + tile_rows - 1) / tile_rows) * ((K + kZKC - 1) / kZKC);
-  if (blocks > 0x7fffffffLL) return fail(FAME_ERR_UNSUPPORTED, "zgemm_3xtf32: too many panel blocks");
+}  // namespace
+
+size_t zpanel_bytes(const ZPanelJob& j) {
+  return panel_bytes(j.rows, j.K, j.batches, j.a_role ? kZM : z_nt(j.cols_for_b), j.a_role);
+}
+
+int zsplit_panels(const ZPanelJob* jobs, int njobs, cudaStream_t s) {
+  if (njobs < 1 || njobs > kMaxSplitJobs) return fail(FAME_ERR_INVALID, "zsplit_panels: job count");
+  SplitJobs sj{};
+  long long blocks = 0;
+  int max_rows = 0;
+  for (int j = 0; j < njobs; ++j) {
+    const ZPanelJob& z = jobs[j];
+    const int tile_rows = z.a_role ? kZM : z_nt(z.cols_for_b);
+    if (!z.src || !z.out || z.rows <= 0 || z.K <= 0 || z.batches <= 0 || tile_rows > kSplitMaxRows ||
+        (reinterpret_cast<uintptr_t>(z.out) & 1023u) != 0)
+      return fail(FAME_ERR_INVALID, "zsplit_panels: job");
+    sj.job[j] = SplitArgs{z.src, z.s_row, z.s_k, z.s_batch, z.rows, z.K, z.batches, tile_rows, z.a_role ? 1 : 0, z.out};
+    sj.first[j] = (int)blocks;
+    blocks += (long long)z.batches * ((z.rows + tile_rows - 1) / tile_rows) * ((z.K + kZKC - 1) / kZKC);
+    max_rows = std::max(max_rows, tile_rows);
+    if (blocks > 0x7fffffffLL) return fail(FAME_ERR_UNSUPPORTED, "zsplit_panels: too many panel blocks");
+  }
+  sj.first[njobs] = (int)blocks;
+  sj.njobs = njobs;
   static int attr = cudaFuncSetAttribute(k_zsplit, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)(kZKC * (kSplitMaxRows + 1) * sizeof(double2))) == cudaSuccess
                         ? FAME_OK
-                        : fail(FAME_ERR_CUDA, "zgemm_3xtf32: split shared-memory limit");
+                        : fail(FAME_ERR_CUDA, "zsplit_panels: shared-memory limit");
   FAME_TRY(attr);
-  k_zsplit<<<(unsigned)blocks, kSplitThreads, (size_t)kZKC * (tile_rows + 1) * sizeof(double2), s>>>(a);
+  k_zsplit<<<(unsigned)blocks, kSplitThreads, (size_t)kZKC * (max_rows + 1) * sizeof(double2), s>>>(sj);
   ::fame::count_launch();
   FAME_CUDA_TRY(cudaGetLastError());
   return FAME_OK;
 }
 
-}  // namespace
-
-size_t zgemm_3xtf32_scratch(int M, int N, int K, int batch, int bdivB) {
-  const int d = bdivB < 1 ? 1 : bdivB, bbatches = (batch + d - 1) / d;
-  return 1024 + (panel_bytes(M, K, batch, kZM, true) + 1023) / 1024 * 1024 +
-         panel_bytes(N, K, bbatches, z_nt(N), false);
-}
-
-int zgemm_3xtf32(const double2* A, const double2* B, double2* C, int M, int N, int K, long long sam, long long sak,
-                 long long sbk, long long sbn, long long scm, long long scn, long long bA, long long bB, long long bC,
-                 int batch, cudaStream_t s, int bdivB, void* scratch) {
-  if (M <= 0 || N <= 0 || K <= 0 || batch <= 0 || !scratch)
-    return fail(FAME_ERR_INVALID, "zgemm_3xtf32: empty shape or no scratch");
-  if (bdivB < 1) return fail(FAME_ERR_INVALID, "zgemm_3xtf32: batch divisor");
+int zgemm_3xtf32_panels(const unsigned char* Ap, const unsigned char* Bp, double2* C, int M, int N, int K,
+                        long long scm, long long scn, long long bC, int batch, int bdivB, cudaStream_t s) {
+  if (M <= 0 || N <= 0 || K <= 0 || batch <= 0 || !Ap || !Bp || !C || bdivB < 1)
+    return fail(FAME_ERR_INVALID, "zgemm_3xtf32: arguments");
+  if ((reinterpret_cast<uintptr_t>(Ap) & 1023u) != 0 || (reinterpret_cast<uintptr_t>(Bp) & 1023u) != 0)
+    return fail(FAME_ERR_INVALID, "zgemm_3xtf32: panels must be 1024-byte aligned");
   const int Nt = z_nt(N), S = zstages(Nt);
   const size_t smem = zsmem(Nt);
   static int attr = [] {
@@ -269,13 +291,6 @@ int zgemm_3xtf32(const double2* A, const double2* B, double2* C, int M, int N, i
   if (attr != FAME_OK) return fail(attr, "zgemm_3xtf32: shared-memory limit");
   const long long gy = (N + Nt - 1) / Nt;
   if (gy > 65535 || batch > 65535) return fail(FAME_ERR_UNSUPPORTED, "zgemm_3xtf32: grid too large");
-  // panels (1024-byte aligned): A' per batch, B' per distinct B (every bdivB batches)
-  unsigned char* base = static_cast<unsigned char*>(scratch);
-  unsigned char* Ap = base + ((1024u - (reinterpret_cast<uintptr_t>(base) & 1023u)) & 1023u);
-  unsigned char* Bp = Ap + (panel_bytes(M, K, batch, kZM, true) + 1023) / 1024 * 1024;
-  const int bbatches = (batch + bdivB - 1) / bdivB;
-  FAME_TRY(split(A, sam, sak, bA, M, K, batch, kZM, true, Ap, s));
-  FAME_TRY(split(B, sbn, sbk, bB, N, K, bbatches, Nt, false, Bp, s));
   ZgArgs g{Ap, Bp, C, M, N, K, Nt, S, scm, scn, bC, bdivB};
   dim3 grid((unsigned)((M + kZM - 1) / kZM), (unsigned)gy, (unsigned)batch);
   k_zgemm_3xtf32<<<grid, kZThreads, smem, s>>>(g, fault_word());
