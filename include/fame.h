@@ -276,7 +276,9 @@ FAME_API int fame_reconstruct_direct_grid(fame_basis* b, const void* coeff, cons
                                           void* u);
 /* (No reference counterpart) the same factorised sum with the three complex GEMMs as
  * split-FP32 (3xTF32) tcgen05 tensor-core products (phase tables and result FP64;
- * relative field error ~2e-6 against fame_reconstruct_direct_grid). */
+ * relative field error ~2e-6 against fame_reconstruct_direct_grid).  The operands are
+ * split once into TF32 head/tail panels held in the context's workspace (about twice
+ * the FP64 intermediates: ~0.3 GB at N=5 on a 83^3 window, ~2.5 GB on 403^3). */
 FAME_API int fame_reconstruct_direct_grid_3xtf32(fame_basis* b, const void* coeff, const double* xs, int nx,
                                                  const double* ys, int ny, const double* zs, int nz,
                                                  void* u);

@@ -61,45 +61,52 @@ struct SplitJobs {
   SplitArgs job[kMaxSplitJobs];
   int first[kMaxSplitJobs + 1];
   int njobs;
+  int pitch;  // shared tile row pitch: the largest per-CTA row share of the jobs, plus one
 };
+// A CTA covers at most kSplitRows complex rows of a panel block (B blocks of Nt = 256 rows
+// take two CTAs: the rows of a block are independent), so its shared tile stays within 33 KB.
+constexpr int kSplitRows = 128;
+__device__ __forceinline__ int split_subs(const SplitArgs& a) { return (a.tile_rows + kSplitRows - 1) / kSplitRows; }
 __global__ void __launch_bounds__(kSplitThreads) k_zsplit(SplitJobs jobs) {
-  extern __shared__ double2 tile_raw[];  // [kZKC][tile_rows + 1]: [k][complex row]
+  extern __shared__ double2 tile_raw[];  // [kZKC][pitch]: [k][complex row of this CTA's share]
+  const int pitch = jobs.pitch;
   int j = 0;
   while (j + 1 < jobs.njobs && (int)blockIdx.x >= jobs.first[j + 1]) ++j;
   const SplitArgs& a = jobs.job[j];
   const int bid = (int)blockIdx.x - jobs.first[j];
-  const int pitch = a.tile_rows + 1;
   const int tiles = (a.rows + a.tile_rows - 1) / a.tile_rows;
-  const int stages = (a.K + kZKC - 1) / kZKC;
-  const int ks = bid % stages, t = (bid / stages) % tiles, b = bid / (stages * tiles);
-  const int r0 = t * a.tile_rows, k0 = ks * kZKC, n = a.tile_rows * kZKC;
+  const int stages = (a.K + kZKC - 1) / kZKC, subs = split_subs(a);
+  const int ks = bid % stages, rest = bid / stages, h = rest % subs, t = (rest / subs) % tiles,
+            b = rest / (subs * tiles);
+  const int rr0 = h * kSplitRows, nr = a.tile_rows - rr0 < kSplitRows ? a.tile_rows - rr0 : kSplitRows;
+  const int r0 = t * a.tile_rows + rr0, k0 = ks * kZKC;
   const bool rfast = a.s_row == 1;  // read along the contiguous dimension
   const double2* src = a.src + (long long)b * a.s_batch;
-  for (int e = threadIdx.x; e < n; e += kSplitThreads) {
-    const int rr = rfast ? e % a.tile_rows : e / kZKC, kk = rfast ? e / a.tile_rows : e % kZKC;
+  for (int e = threadIdx.x; e < nr * kZKC; e += kSplitThreads) {
+    const int rr = rfast ? e % nr : e / kZKC, kk = rfast ? e / nr : e % kZKC;
     const int r = r0 + rr, k = k0 + kk;
     tile_raw[kk * pitch + rr] = (r < a.rows && k < a.K) ? __ldg(src + (long long)r * a.s_row + (long long)k * a.s_k)
                                                         : make_double2(0.0, 0.0);
   }
   __syncthreads();
-  const int real_rows = a.tile_rows * (a.a_role ? 2 : 1);
-  const size_t part = (size_t)real_rows * 128u;
+  const int per = a.a_role ? 2 : 1;  // real rows per complex row
+  const size_t part = (size_t)a.tile_rows * per * 128u;
   unsigned char* blk = a.out + ((size_t)((long long)b * tiles + t) * stages + ks) * 2 * part;
   // 16-byte chunk c of real row R holds K' = 4c .. 4c+3, i.e. complex k = 2c, 2c+1
-  for (int e = threadIdx.x; e < real_rows * 8; e += kSplitThreads) {
-    const int R = e / 8, c = e % 8;
+  for (int e = threadIdx.x; e < nr * per * 8; e += kSplitThreads) {
+    const int Rl = e / 8, c = e % 8, R = rr0 * per + Rl;  // Rl: real row within this CTA's share
     float hv[4], lv[4];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const double2 v = tile_raw[(2 * c + h) * pitch + (a.a_role ? R / 2 : R)];
+    for (int q = 0; q < 2; ++q) {
+      const double2 v = tile_raw[(2 * c + q) * pitch + Rl / per];
       float rh, rl, ih, il;
       umma::tf32_split_fast(v.x, rh, rl);
       umma::tf32_split_fast(v.y, ih, il);
       const bool second = a.a_role && (R & 1);  // A rows: (Re, -Im) then (Im, Re)
-      hv[2 * h] = second ? ih : rh;
-      hv[2 * h + 1] = second ? rh : (a.a_role ? -ih : ih);
-      lv[2 * h] = second ? il : rl;
-      lv[2 * h + 1] = second ? rl : (a.a_role ? -il : il);
+      hv[2 * q] = second ? ih : rh;
+      hv[2 * q + 1] = second ? rh : (a.a_role ? -ih : ih);
+      lv[2 * q] = second ? il : rl;
+      lv[2 * q + 1] = second ? rl : (a.a_role ? -il : il);
     }
     const uint32_t off = umma::sw128_offset(R, 4 * c);
     *reinterpret_cast<float4*>(blk + off) = make_float4(hv[0], hv[1], hv[2], hv[3]);
@@ -248,7 +255,7 @@ int zsplit_panels(const ZPanelJob* jobs, int njobs, cudaStream_t s) {
   if (njobs < 1 || njobs > kMaxSplitJobs) return fail(FAME_ERR_INVALID, "zsplit_panels: job count");
   SplitJobs sj{};
   long long blocks = 0;
-  int max_rows = 0;
+  int share = 1;
   for (int j = 0; j < njobs; ++j) {
     const ZPanelJob& z = jobs[j];
     const int tile_rows = z.a_role ? kZM : z_nt(z.cols_for_b);
@@ -257,18 +264,15 @@ int zsplit_panels(const ZPanelJob* jobs, int njobs, cudaStream_t s) {
       return fail(FAME_ERR_INVALID, "zsplit_panels: job");
     sj.job[j] = SplitArgs{z.src, z.s_row, z.s_k, z.s_batch, z.rows, z.K, z.batches, tile_rows, z.a_role ? 1 : 0, z.out};
     sj.first[j] = (int)blocks;
-    blocks += (long long)z.batches * ((z.rows + tile_rows - 1) / tile_rows) * ((z.K + kZKC - 1) / kZKC);
-    max_rows = std::max(max_rows, tile_rows);
+    blocks += (long long)z.batches * ((z.rows + tile_rows - 1) / tile_rows) * ((z.K + kZKC - 1) / kZKC) *
+              ((tile_rows + kSplitRows - 1) / kSplitRows);
+    share = std::max(share, std::min(tile_rows, kSplitRows));
     if (blocks > 0x7fffffffLL) return fail(FAME_ERR_UNSUPPORTED, "zsplit_panels: too many panel blocks");
   }
   sj.first[njobs] = (int)blocks;
   sj.njobs = njobs;
-  static int attr = cudaFuncSetAttribute(k_zsplit, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)(kZKC * (kSplitMaxRows + 1) * sizeof(double2))) == cudaSuccess
-                        ? FAME_OK
-                        : fail(FAME_ERR_CUDA, "zsplit_panels: shared-memory limit");
-  FAME_TRY(attr);
-  k_zsplit<<<(unsigned)blocks, kSplitThreads, (size_t)kZKC * (max_rows + 1) * sizeof(double2), s>>>(sj);
+  sj.pitch = share + 1;
+  k_zsplit<<<(unsigned)blocks, kSplitThreads, (size_t)kZKC * sj.pitch * sizeof(double2), s>>>(sj);
   ::fame::count_launch();
   FAME_CUDA_TRY(cudaGetLastError());
   return FAME_OK;
