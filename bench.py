@@ -364,8 +364,22 @@ def run_fame(args):
             return time.perf_counter() - t0
         t_seq = sequential("mixed")
         t_seq64 = sequential("fp64")
+        # the autotuner's schedule and pass tile shape per N (tuning untimed, like the handles)
+        t0 = time.perf_counter()
+        tuned = F.tune_batch(Ns, mats, qs, cfg.P_GOLDEN, tolCG=S["tolCG"])
+        t_tune = time.perf_counter() - t0
+        F.solve_batch(Ns, mats, qs, cfg.P_GOLDEN, nev=S["nev"], tol=S["tol"], p=S["p"], tolCG=S["tolCG"], tuned=tuned)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        lam_t, _ = F.solve_batch(Ns, mats, qs, cfg.P_GOLDEN, nev=S["nev"], tol=S["tol"], p=S["p"], tolCG=S["tolCG"],
+                                 tuned=tuned)
+        torch.cuda.synchronize()
+        t_tuned = time.perf_counter() - t0
         bloch = {"points": len(Ns), "N": Ns, "batched_s": round(t_batch, 4), "sequential_s": round(t_seq, 4),
                  "batch_speedup": round(t_seq / t_batch, 3),
+                 "batched_tuned_s": round(t_tuned, 4), "tuned": {str(k): v for k, v in tuned.items()},
+                 "tuning_s": round(t_tune, 2),
+                 "tuned_lambda_max_rel_diff": float(np.max(np.abs(lam_t - lam_b) / np.abs(lam_b))),
                  "fp64_sequential_s": round(t_seq64, 4),
                  "mixed_batched_vs_fp64_sequential": round(t_seq64 / t_batch, 3),
                  "converged": all(i["converged"] for i in infos_b),

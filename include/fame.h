@@ -380,6 +380,13 @@ FAME_API int fame_solve_batch(int device, int count, const int* N, const double*
                               const double* q, const double* P, const fame_krinv_opts* o, int nev,
                               double tol, int maxiter, int p, unsigned long long seed,
                               double* theta, fame_lanczos_info* info, int* status);
+/* (No reference counterpart) the same with one K_r^{-1} options struct per instance
+ * (opts: count entries), e.g. the launch schedule and pass tile shape the autotuner
+ * chose for each instance's N. */
+FAME_API int fame_solve_batch_each(int device, int count, const int* N, const double* const* E,
+                                   const double* q, const double* P, const fame_krinv_opts* opts, int nev,
+                                   double tol, int maxiter, int p, unsigned long long seed,
+                                   double* theta, fame_lanczos_info* info, int* status);
 /* Start vector of the shared counter-based generator (complex128, device). */
 FAME_API int fame_start_vector(fame_ctx* ctx, unsigned long long seed, long long n, void* v);
 

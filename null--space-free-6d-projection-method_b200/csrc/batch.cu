@@ -3,10 +3,12 @@
 // exp4/run_exp4_medium.m:37-109).  Each instance gets its own context,
 // stream, mass, basis and K_r^{-1} handles and runs the restarted Lanczos in
 // its own host thread, so the GPU interleaves the kernels of small and large
-// instances; the per-iteration PCG bodies replay captured CUDA graphs.  Device
-// memory is allocated stream-ordered from the default pool on each instance's
-// stream and every handle is released only after all instances finished, so no
-// instance's free synchronises the device under the others.
+// instances; the per-iteration PCG bodies replay captured CUDA graphs, and each
+// instance may carry its own K_r^{-1} options (the schedule and pass tile shape the
+// autotuner picked for its N).  Device memory is allocated stream-ordered from the
+// library's pool on each instance's stream and every handle is released only after
+// all instances finished, so no instance's free synchronises the device under the
+// others.
 #include <algorithm>
 #include <cstring>
 #include <string>
@@ -72,11 +74,11 @@ void release_job(BatchJob* j) {
 
 }  // namespace
 
-extern "C" int fame_solve_batch(int device, int count, const int* Ns, const double* const* E,
-                                const double* q, const double* P, const fame_krinv_opts* o, int nev,
-                                double tol, int maxiter, int p, unsigned long long seed, double* theta,
-                                fame_lanczos_info* info, int* status) {
-  if (count < 1 || !Ns || !E || !q || !P || !theta || nev < 1)
+static int solve_batch(int device, int count, const int* Ns, const double* const* E, const double* q,
+                       const double* P, const fame_krinv_opts* o, int per_instance, int nev, double tol,
+                       int maxiter, int p, unsigned long long seed, double* theta, fame_lanczos_info* info,
+                       int* status) {
+  if (count < 1 || !Ns || !E || !q || !P || !theta || nev < 1 || (per_instance && !o))
     return fail(FAME_ERR_INVALID, "fame_solve_batch arguments");
   std::vector<BatchJob> jobs(count);
   for (int i = 0; i < count; ++i) {
@@ -87,7 +89,7 @@ extern "C" int fame_solve_batch(int device, int count, const int* Ns, const doub
     std::memcpy(j.q, q + 3 * i, sizeof(j.q));
     j.P = P;
     fame_krinv_default_opts(&j.o);
-    if (o) j.o = *o;
+    if (o) j.o = per_instance ? o[i] : *o;
     j.nev = nev;
     j.tol = tol;
     j.maxiter = maxiter;
@@ -124,4 +126,18 @@ extern "C" int fame_solve_batch(int device, int count, const int* Ns, const doub
   }
   if (first != FAME_OK) return fail(first, msg);
   return FAME_OK;
+}
+
+extern "C" int fame_solve_batch(int device, int count, const int* Ns, const double* const* E,
+                                const double* q, const double* P, const fame_krinv_opts* o, int nev,
+                                double tol, int maxiter, int p, unsigned long long seed, double* theta,
+                                fame_lanczos_info* info, int* status) {
+  return solve_batch(device, count, Ns, E, q, P, o, 0, nev, tol, maxiter, p, seed, theta, info, status);
+}
+
+extern "C" int fame_solve_batch_each(int device, int count, const int* Ns, const double* const* E,
+                                     const double* q, const double* P, const fame_krinv_opts* opts, int nev,
+                                     double tol, int maxiter, int p, unsigned long long seed, double* theta,
+                                     fame_lanczos_info* info, int* status) {
+  return solve_batch(device, count, Ns, E, q, P, opts, 1, nev, tol, maxiter, p, seed, theta, info, status);
 }

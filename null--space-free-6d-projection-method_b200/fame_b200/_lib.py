@@ -121,6 +121,9 @@ SIGNATURES = {
     "fame_solve_batch": [I, I, C.POINTER(I), C.POINTER(P), C.POINTER(D), C.POINTER(D),
                          C.POINTER(fame_krinv_opts), I, D, I, I, C.c_ulonglong, C.POINTER(D),
                          C.POINTER(fame_lanczos_info), C.POINTER(I)],
+    "fame_solve_batch_each": [I, I, C.POINTER(I), C.POINTER(P), C.POINTER(D), C.POINTER(D),
+                              C.POINTER(fame_krinv_opts), I, D, I, I, C.c_ulonglong, C.POINTER(D),
+                              C.POINTER(fame_lanczos_info), C.POINTER(I)],
 }
 
 

@@ -22,7 +22,7 @@ __all__ = [
     "solveV1_blockdiag", "solveV1H_blockdiag", "QSystem", "build_q_system",
     "make_explicit_krinv_compact", "make_nested_krinv_instrumented", "KrInv", "Lanczos",
     "start_vector", "FameError", "apply_Mhat_C_scalar_compact", "kernel_launches", "solve_batch",
-    "rayleigh_ritz", "rank1_exact_fft_scatter", "rank1_exact_ifft_gather",
+    "rayleigh_ritz", "rank1_exact_fft_scatter", "rank1_exact_ifft_gather", "tune_batch",
 ]
 
 
@@ -510,11 +510,14 @@ def rayleigh_ritz(sys: QSystem, Y):
 
 
 def solve_batch(Ns, materials, qs, P, nev=10, tol=1e-8, maxiter=30, p=40, tolCG=1e-10,
-                precision="mixed", seed=None, device=None):
+                precision="mixed", seed=None, device=None, tuned=None):
     """Solve independent Bloch points of uneven size concurrently (one call).
 
-    ``materials[i]`` is the float64 device eps grid of instance i.  Returns
-    ``(lam, infos)`` with lam (count x nev) ascending eigenvalues lambda = 1/theta.
+    ``materials[i]`` is the float64 device eps grid of instance i.  ``tuned`` maps a grid
+    size N to K_r^{-1} options (``checkEvery``, ``useGraphs``, ``passColumns``, e.g. from
+    ``tune_batch``) applied to every instance of that N; other instances use the
+    defaults.  Returns ``(lam, infos)`` with lam (count x nev) ascending eigenvalues
+    lambda = 1/theta.
     """
     from . import configs
     count = len(Ns)
@@ -524,14 +527,31 @@ def solve_batch(Ns, materials, qs, P, nev=10, tol=1e-8, maxiter=30, p=40, tolCG=
     Narr = (C.c_int * count)(*[int(n) for n in Ns])
     qarr = (C.c_double * (3 * count))(*np.asarray(qs, dtype=np.float64).reshape(-1))
     Parr = (C.c_double * 18)(*np.asarray(P, dtype=np.float64).reshape(6, 3).reshape(-1, order="F"))
-    o = _opts(kind=L.FAME_KRINV_EXPLICIT, tolCG=tolCG, maxitCG=3000,
-              prec_mode=L.FAME_PREC_MIXED if precision == "mixed" else L.FAME_PREC_FP64)
+    base = dict(kind=L.FAME_KRINV_EXPLICIT, tolCG=tolCG, maxitCG=3000,
+                prec_mode=L.FAME_PREC_MIXED if precision == "mixed" else L.FAME_PREC_FP64)
+    opts = (L.fame_krinv_opts * count)(*[_opts(**base, **((tuned or {}).get(int(n), {}))) for n in Ns])
     theta = (C.c_double * (count * nev))()
     infos = (L.fame_lanczos_info * count)()
     status = (C.c_int * count)()
     torch.cuda.synchronize(dev)
-    call("fame_solve_batch", dev, count, Narr, Earr, qarr, Parr, C.byref(o), nev, float(tol), int(maxiter),
+    call("fame_solve_batch_each", dev, count, Narr, Earr, qarr, Parr, opts, nev, float(tol), int(maxiter),
          int(p), C.c_ulonglong(configs.SEED if seed is None else seed), theta, infos, status)
     th = np.array(theta[:]).reshape(count, nev)
     return np.sort(1.0 / th, axis=1), [dict(steps=i.steps, converged=bool(i.converged), nconv=i.nconv)
                                        for i in infos]
+
+
+def tune_batch(Ns, materials, qs, P, precision="mixed", tolCG=1e-10, **kw):
+    """The autotuner (``autotune.tune_krinv_schedule``) run once per distinct grid size of a
+    batch, on its first instance: returns ``{N: options}`` for ``solve_batch(tuned=...)``."""
+    from .autotune import tune_krinv_schedule
+    out = {}
+    for n, E, q in zip(Ns, materials, qs):
+        n = int(n)
+        if n in out:
+            continue
+        sysq = build_q_system(MassBackend(E, n), P, q)
+        out[n] = tune_krinv_schedule(sysq, precision=precision, tolCG=tolCG, **kw)[0]
+        torch.cuda.synchronize()
+        del sysq
+    return out

@@ -167,6 +167,25 @@ def test_batched_bloch_path_matches_single_solves(cuda_device):
         np.testing.assert_allclose(lam[i], np.sort(1.0 / th), rtol=1e-10)
 
 
+def test_batched_bloch_path_with_tuned_options(cuda_device):
+    """The autotuner's per-N choices (schedule, pass tile shape) reach every instance of that N
+    (fame_solve_batch_each) and change only how the work is launched: the eigenvalues equal
+    those of the default options."""
+    import fame_b200 as F
+    Ns = [3, 2, 3, 2]
+    qs = [(0.05, 0.04, 0.03), (0.1, 0.02, 0.03), (0.2, 0.1, 0.05), (0.25, 0.25, 0.1)]
+    mats = [F.configs.material_separable_cos(N, device=cuda_device) for N in Ns]
+    tuned = F.tune_batch(Ns, mats, qs, F.configs.P_GOLDEN, tolCG=1e-12, reps=1)
+    assert sorted(tuned) == [2, 3] and all({"checkEvery", "useGraphs", "passColumns"} <= set(v) for v in tuned.values())
+    kw = dict(nev=6, tol=1e-10, tolCG=1e-12)
+    lam0, _ = F.solve_batch(Ns, mats, qs, F.configs.P_GOLDEN, **kw)
+    forced = {3: dict(checkEvery=16, useGraphs=1, passColumns=4), 2: dict(checkEvery=2, useGraphs=0)}
+    for opts in (tuned, forced):
+        lam, infos = F.solve_batch(Ns, mats, qs, F.configs.P_GOLDEN, tuned=opts, **kw)
+        assert all(i["converged"] for i in infos)
+        np.testing.assert_allclose(lam, lam0, rtol=1e-9)
+
+
 @pytest.mark.parametrize("N,p,nb", [(2, 6, 2), (2, 10, 3), (3, 8, 2), (2, 12, 2), (2, 0, 1), (4, 10, 5)])
 def test_taylor_3xtf32_tensor_cores_vs_fp64(cuda_device, N, p, nb):
     """Split-FP32 (3xTF32) tensor-core block moments (operands generated on chip, FP32
