@@ -13,7 +13,8 @@
 // complex k = 32 TF32 values of K', one 128-byte swizzle atom) a head part and a
 // tail part, each rows x 128 bytes in the 128-byte swizzled K-major UMMA layout,
 // one contiguous block per (tile, stage).  k_zgemm_3xtf32 then streams those blocks:
-// one thread issues a bulk copy per stage (completed on the stage's mbarrier), one
+// one thread issues the A and B bulk copies of each stage (completed on the stage's
+// mbarrier), one
 // thread issues tcgen05.mma kind::tf32 -- head*head into one TMEM accumulator, the two
 // cross products into a second (the tensor cores round the FP32 accumulation toward
 // zero, and the cross products are 2^-11 smaller, so only the head*head sum carries
@@ -50,9 +51,9 @@ struct SplitArgs {
   unsigned char* out;
 };
 
-// One CTA per panel block (batch, tile, stage): the tile's FP64 values are read along the
-// operand's contiguous dimension into shared memory, then written as whole 128-byte rows,
-// 16 bytes (four TF32 values of K' = two complex k) per thread.
+// A CTA takes (a share of the rows of) one panel block (batch, tile, stage): the FP64 values
+// are read along the operand's contiguous dimension into shared memory, then written as
+// whole 128-byte rows, 16 bytes (four TF32 values of K' = two complex k) per thread.
 constexpr int kSplitThreads = 256;
 constexpr int kSplitMaxRows = 256;  // complex rows of a tile (B role, Nt <= 256)
 // several operands in one launch: job j owns blocks [first[j], first[j + 1])
