@@ -195,8 +195,9 @@ def run_fame(args):
     sysq = F.build_q_system(mass, cfg.P_GOLDEN, cfg.Q_PHYS)
     v0 = F.start_vector(cfg.SEED, sysq.nr)
     ops = {}
-    for prec in ("mixed", "fp64"):
-        ops[prec] = F.make_explicit_krinv_compact(sysq, S["tolCG"], S["maxitCG"], precision=prec)[0]
+    ops["mixed"] = F.make_explicit_krinv_compact(sysq, S["tolCG"], S["maxitCG"], precision="mixed",
+                                                 **cfg.MIXED_OPTS)[0]
+    ops["fp64"] = F.make_explicit_krinv_compact(sysq, S["tolCG"], S["maxitCG"], precision="fp64")[0]
     # the reference algorithm's inner solve (plain Mhat CG, exp1/make_explicit_krinv_compact.m:43) in FP64
     ops["fp64_plain"] = F.make_explicit_krinv_compact(sysq, S["tolCG"], S["maxitCG"], precision="fp64",
                                                       mhatPreconditioner=0)[0]
@@ -347,11 +348,11 @@ def run_fame(args):
         qs = [np.array(qv) for qv in qs]
         qs[0] = qs[0] + cfg.GAMMA_SHIFT  # the reduction is singular at Gamma
         mats = [cfg.material_separable_cos(Nq, 12.0, device=dev) for Nq in Ns]
-        F.solve_batch(Ns, mats, qs, cfg.P_GOLDEN, nev=S["nev"], tol=S["tol"], p=S["p"], tolCG=S["tolCG"])
+        F.solve_batch(Ns, mats, qs, cfg.P_GOLDEN, nev=S["nev"], tol=S["tol"], p=S["p"], tolCG=S["tolCG"], **cfg.MIXED_OPTS)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         lam_b, infos_b = F.solve_batch(Ns, mats, qs, cfg.P_GOLDEN, nev=S["nev"], tol=S["tol"], p=S["p"],
-                                       tolCG=S["tolCG"])
+                                       tolCG=S["tolCG"], **cfg.MIXED_OPTS)
         torch.cuda.synchronize()
         t_batch = time.perf_counter() - t0
 
@@ -359,20 +360,21 @@ def run_fame(args):
             t0 = time.perf_counter()
             for i in range(len(Ns)):
                 F.solve_batch([Ns[i]], [mats[i]], [qs[i]], cfg.P_GOLDEN, nev=S["nev"], tol=S["tol"], p=S["p"],
-                              tolCG=S["tolCG"], precision=prec)
+                              tolCG=S["tolCG"], precision=prec, **(cfg.MIXED_OPTS if prec == "mixed" else {}))
             torch.cuda.synchronize()
             return time.perf_counter() - t0
         t_seq = sequential("mixed")
         t_seq64 = sequential("fp64")
         # the autotuner's schedule and pass tile shape per N (tuning untimed, like the handles)
         t0 = time.perf_counter()
-        tuned = F.tune_batch(Ns, mats, qs, cfg.P_GOLDEN, tolCG=S["tolCG"])
+        tuned = F.tune_batch(Ns, mats, qs, cfg.P_GOLDEN, tolCG=S["tolCG"], **cfg.MIXED_OPTS)
         t_tune = time.perf_counter() - t0
-        F.solve_batch(Ns, mats, qs, cfg.P_GOLDEN, nev=S["nev"], tol=S["tol"], p=S["p"], tolCG=S["tolCG"], tuned=tuned)
+        F.solve_batch(Ns, mats, qs, cfg.P_GOLDEN, nev=S["nev"], tol=S["tol"], p=S["p"], tolCG=S["tolCG"], tuned=tuned,
+                      **cfg.MIXED_OPTS)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         lam_t, _ = F.solve_batch(Ns, mats, qs, cfg.P_GOLDEN, nev=S["nev"], tol=S["tol"], p=S["p"], tolCG=S["tolCG"],
-                                 tuned=tuned)
+                                 tuned=tuned, **cfg.MIXED_OPTS)
         torch.cuda.synchronize()
         t_tuned = time.perf_counter() - t0
         bloch = {"points": len(Ns), "N": Ns, "batched_s": round(t_batch, 4), "sequential_s": round(t_seq, 4),
@@ -404,7 +406,8 @@ def run_fame(args):
             vd = v0_h.to(dev, non_blocking=True)
             m2 = F.MassBackend(Ed, N)
             s2 = F.build_q_system(m2, cfg.P_GOLDEN, cfg.Q_PHYS)
-            op2, _ = F.make_explicit_krinv_compact(s2, S["tolCG"], S["maxitCG"], precision="mixed")
+            op2, _ = F.make_explicit_krinv_compact(s2, S["tolCG"], S["maxitCG"], precision="mixed",
+                                                   **cfg.MIXED_OPTS)
             Y, theta, _, _ = F.Lanczos(op2, None, None, s2.nr, S["nev"], S["tol"], S["maxRestart"], S["p"], vd)
             lam, _ = F.rayleigh_ritz(s2, Y)  # the eigenvalues arrive on the host with the call
             torch.cuda.synchronize()
@@ -565,7 +568,8 @@ def gpu_parity(F, legs, ops, sysq, S, dev):
         E3 = F.configs.material_separable_cos(3, 12.0, device=dev)
         m3 = F.MassBackend(E3, 3)
         s3 = F.build_q_system(m3, F.configs.P_GOLDEN, F.configs.Q_PHYS)
-        op3 = F.make_explicit_krinv_compact(s3, S["tolCG"], S["maxitCG"], precision="mixed")[0]
+        op3 = F.make_explicit_krinv_compact(s3, S["tolCG"], S["maxitCG"], precision="mixed",
+                                            **F.configs.MIXED_OPTS)[0]
         Y, theta, _, info = F.Lanczos(op3, None, None, s3.nr, S["nev"], S["tol"], S["maxRestart"], S["p"],
                                       F.start_vector(F.configs.SEED, s3.nr))
         lam_raw = np.sort(1.0 / theta)
@@ -614,7 +618,8 @@ def run_case(args):
         x = torch.randn(NF, dtype=torch.complex128 if prec == "fp64" else torch.complex64, device=dev)
         body = lambda: F.apply_Mhat_C_scalar_compact(x, sysq)  # noqa: E731
     else:
-        op = F.make_explicit_krinv_compact(sysq, S["tolCG"], S["maxitCG"], precision=prec)[0]
+        op = F.make_explicit_krinv_compact(sysq, S["tolCG"], S["maxitCG"], precision=prec,
+                                           **(cfg.MIXED_OPTS if prec == "mixed" else {}))[0]
         if args.case == "pcg":
             q = (v0 / torch.linalg.norm(v0)).reshape(-1, 1)
             body = lambda: op(q)  # noqa: E731

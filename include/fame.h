@@ -213,7 +213,7 @@ typedef struct {
   int maxitM;      /* nested (1600) */
   double epsC;     /* nested preconditioner scale epsC*r./sigma_r (4) */
   int useKrPreconditioner; /* nested (1) */
-  double tolInner32; /* mixed: relative tolerance of each FP32 correction solve (1e-5) */
+  double tolInner32; /* mixed: relative tolerance of each FP32 correction solve (3e-6) */
   int maxRefine;     /* mixed: max FP64 refinement steps per solve (20) */
   int checkEvery;    /* PCG iterations queued between host convergence checks (4) */
   int verifyTrueResidual; /* confirm convergence on the true residual, as MATLAB pcg (1) */
@@ -225,6 +225,11 @@ typedef struct {
   int passColumns; /* columns per CTA of the inner solves' pass A/C kernels: 0 = built-in default;
                       alternatives 2, 4 (2N = 10), 2, 4 (2N = 8), 4, 6 (2N = 6); other values
                       fall back to the default (fame_b200.autotune picks it per problem) */
+  double refineTarget; /* explicit, mixed: the FP64 refinement of each Mhat solve stops once
+                          ||bhat - Mhat u|| <= refineTarget * tolCG * ||bhat||, in (0, 1] (0.1).
+                          1 is the stopping rule of the reference's pcg (relres <= tolCG); the
+                          default stops a decade lower, so that the Lanczos eigenvalues before
+                          any Rayleigh-Ritz step stay within tolCG of those of the FP64 form */
 } fame_krinv_opts;
 FAME_API int fame_krinv_default_opts(fame_krinv_opts* o);
 FAME_API int fame_krinv_create(fame_basis* b, fame_mass* m, const fame_krinv_opts* o, fame_krinv** out);

@@ -148,14 +148,19 @@ int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
     float* partials32 = reinterpret_cast<float*>(K->partials);
     const MhatCoef<double> c = c64;
     int refine = 0;
-    // refine to 0.1*tolCG: the FP32 corrections leave no FP64-PCG overshoot, so the
-    // target is set one decade tighter to keep eigenvalues within 1e-10 of FP64
-    const double tolIR = 0.1 * tolMhat;
+    // refine to refineTarget*tolCG: at 1 the reference's pcg rule (relres <= tolCG); the
+    // FP32 corrections leave no FP64-PCG overshoot below it, so the default of 0.1 keeps
+    // the Lanczos eigenvalues within tolCG of the FP64 form's before any Rayleigh-Ritz step
+    const double tolIR = K->o.refineTarget * tolMhat;
     while (rn2 > tolIR * tolIR * bn2 && bn2 > 0) {
       if (refine >= K->o.maxRefine) break;
       ++refine;
+      // a round needs only the reduction that takes the residual to the target: the FP32
+      // solve is asked for half of it, never for less than tolInner32 (its accuracy floor)
+      const double need = tolIR * std::sqrt(bn2 / rn2);
+      const double tau = std::min(1e-2, std::max(K->o.tolInner32, 0.5 * need));
       k_pcg_init<float, double><<<vec_blocks(NF), 256, 0, s>>>(B.r, F.r, F.x, NF, st32,
-                                                              K->o.tolInner32, K->o.maxitCG,
+                                                              tau, K->o.maxitCG,
                                                               partials32, K->counter);
       ::fame::count_launch();
       PcgState h32{};
@@ -266,6 +271,7 @@ int fame_krinv_default_opts(fame_krinv_opts* o) {
   o->useGraphs = 1;
   o->mhatPreconditioner = 1;
   o->passColumns = 0;
+  o->refineTarget = 0.1;
   return FAME_OK;
 }
 
@@ -283,6 +289,10 @@ int fame_krinv_create(fame_basis* b, fame_mass* m, const fame_krinv_opts* o, fam
   if (K->o.prec_mode != FAME_PREC_FP64 && K->o.prec_mode != FAME_PREC_MIXED) {
     delete K;
     return fail(FAME_ERR_INVALID, "unknown precision mode");
+  }
+  if (!(K->o.refineTarget > 0.0 && K->o.refineTarget <= 1.0)) {
+    delete K;
+    return fail(FAME_ERR_INVALID, "refineTarget must lie in (0, 1]");
   }
   K->b = b;
   K->m = m;

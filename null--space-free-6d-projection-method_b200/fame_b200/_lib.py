@@ -39,7 +39,8 @@ class fame_krinv_opts(C.Structure):
                 ("maxitKr", C.c_int), ("maxitM", C.c_int), ("epsC", C.c_double),
                 ("useKrPreconditioner", C.c_int), ("tolInner32", C.c_double),
                 ("maxRefine", C.c_int), ("checkEvery", C.c_int), ("verifyTrueResidual", C.c_int),
-                ("useGraphs", C.c_int), ("mhatPreconditioner", C.c_int), ("passColumns", C.c_int)]
+                ("useGraphs", C.c_int), ("mhatPreconditioner", C.c_int), ("passColumns", C.c_int),
+                ("refineTarget", C.c_double)]
 
 
 class fame_krinv_stats(C.Structure):

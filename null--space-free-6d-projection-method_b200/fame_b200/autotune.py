@@ -29,10 +29,11 @@ COLUMN_CANDIDATES = {6: (0, 4, 6), 8: (0, 2, 4), 10: (0, 2, 4)}
 
 
 def tune_krinv_schedule(sys: QSystem, precision="mixed", tolCG=1e-10, maxitCG=3000, candidates=DEFAULT_CANDIDATES,
-                        reps=4, seed=7, columns=None, rtol=1e-7):
+                        reps=4, seed=7, columns=None, rtol=1e-7, **opts):
     """Return ``(best, table)``: ``best`` = {"checkEvery", "useGraphs", "passColumns"} of the
     fastest candidate (pass it as keyword arguments to make_explicit_krinv_compact) and
-    ``table`` the seconds per K_r^{-1} action of every candidate."""
+    ``table`` the seconds per K_r^{-1} action of every candidate.  ``opts``: further K_r^{-1}
+    options held fixed over the candidates (e.g. ``refineTarget``)."""
     if columns is None:
         columns = COLUMN_CANDIDATES.get(2 * sys.N, (0,))
     v = start_vector(seed, sys.nr).reshape(-1, 1)
@@ -40,7 +41,7 @@ def tune_krinv_schedule(sys: QSystem, precision="mixed", tolCG=1e-10, maxitCG=30
     for cols in columns:
         for every, graphs in candidates:
             op, _ = make_explicit_krinv_compact(sys, tolCG, maxitCG, precision=precision, checkEvery=int(every),
-                                                useGraphs=int(graphs), passColumns=int(cols))
+                                                useGraphs=int(graphs), passColumns=int(cols), **opts)
             y = op(v)  # warm-up (graph capture, workspaces)
             torch.cuda.synchronize()
             t0 = time.perf_counter()

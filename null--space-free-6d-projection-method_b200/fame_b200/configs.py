@@ -30,6 +30,10 @@ GAMMA_SHIFT = np.array([1e-3, 0.0, 0.0])
 # Solver settings of the 10-eigenpair workloads (shift 0, Krylov block 40, outer tol 1e-8,
 # inner Mhat PCG tol 1e-10).
 SOLVE = dict(nev=10, p=40, tol=1e-8, maxRestart=30, tolCG=1e-10, maxitCG=3000)
+# Options of the mixed form in these workloads: the FP64 refinement of each Mhat solve stops
+# at the reference pcg rule relres <= tolCG (exp1/make_explicit_krinv_compact.m:43), as the
+# FP64 form does; the eigenvalues are then refined by Rayleigh-Ritz on the exact K_r.
+MIXED_OPTS = dict(refineTarget=1.0)
 
 
 def _coords(N, device):

@@ -510,13 +510,14 @@ def rayleigh_ritz(sys: QSystem, Y):
 
 
 def solve_batch(Ns, materials, qs, P, nev=10, tol=1e-8, maxiter=30, p=40, tolCG=1e-10,
-                precision="mixed", seed=None, device=None, tuned=None):
+                precision="mixed", seed=None, device=None, tuned=None, **kw):
     """Solve independent Bloch points of uneven size concurrently (one call).
 
     ``materials[i]`` is the float64 device eps grid of instance i.  ``tuned`` maps a grid
     size N to K_r^{-1} options (``checkEvery``, ``useGraphs``, ``passColumns``, e.g. from
     ``tune_batch``) applied to every instance of that N; other instances use the
-    defaults.  Returns ``(lam, infos)`` with lam (count x nev) ascending eigenvalues
+    defaults.  Other keyword arguments are K_r^{-1} options of every instance (e.g.
+    ``refineTarget``).  Returns ``(lam, infos)`` with lam (count x nev) ascending eigenvalues
     lambda = 1/theta.
     """
     from . import configs
@@ -528,7 +529,7 @@ def solve_batch(Ns, materials, qs, P, nev=10, tol=1e-8, maxiter=30, p=40, tolCG=
     qarr = (C.c_double * (3 * count))(*np.asarray(qs, dtype=np.float64).reshape(-1))
     Parr = (C.c_double * 18)(*np.asarray(P, dtype=np.float64).reshape(6, 3).reshape(-1, order="F"))
     base = dict(kind=L.FAME_KRINV_EXPLICIT, tolCG=tolCG, maxitCG=3000,
-                prec_mode=L.FAME_PREC_MIXED if precision == "mixed" else L.FAME_PREC_FP64)
+                prec_mode=L.FAME_PREC_MIXED if precision == "mixed" else L.FAME_PREC_FP64, **kw)
     opts = (L.fame_krinv_opts * count)(*[_opts(**base, **((tuned or {}).get(int(n), {}))) for n in Ns])
     theta = (C.c_double * (count * nev))()
     infos = (L.fame_lanczos_info * count)()

@@ -189,6 +189,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     opts.epsC = field_or(o, "epsC", opts.epsC);
     opts.useKrPreconditioner = (int)field_or(o, "useKrPreconditioner", opts.useKrPreconditioner);
     opts.mhatPreconditioner = (int)field_or(o, "mhatPreconditioner", opts.mhatPreconditioner);
+    opts.refineTarget = field_or(o, "refineTarget", opts.refineTarget);
     check(fame_krinv_create((fame_basis*)b->p, (fame_mass*)m->p, &opts, &k));
     plhs[0] = wrap(H_KRINV, k);
   } else if (!strcmp(cmd, "krinv_apply")) { /* KrInvOp(q) */

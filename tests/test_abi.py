@@ -40,6 +40,7 @@ def test_status_strings_and_default_opts():
     assert L.fame_krinv_default_opts(C.byref(o)) == 0
     assert o.tolCG == 1e-10 and o.maxitCG == 1200 and o.tolM == 1e-12 and o.maxitKr == 600
     assert o.epsC == 4.0 and o.useKrPreconditioner == 1 and o.mhatPreconditioner == 1
+    assert o.tolInner32 == 3e-6 and o.refineTarget == 0.1
     assert L.fame_version() >= 100
 
 

@@ -160,6 +160,42 @@ def test_lanczos_n3_benchmark_system_fp64_and_mixed(cuda_device):
     assert d < 2e-9, d
 
 
+def test_mixed_refinement_target(cuda_device):
+    """The mixed form's refinement target: at refineTarget = 1 each Mhat solve stops at the
+    reference's pcg rule relres <= tolCG (exp1/make_explicit_krinv_compact.m:43) with fewer
+    FP32 iterations than the default decade below it; both reach the oracle's action within
+    the accuracy of that rule, the N=3 benchmark eigenvalues after Rayleigh-Ritz equal the
+    oracle's refined ones, and targets outside (0, 1] are rejected."""
+    import fame_b200 as F
+    N = 3
+    S, sg = _systems(N, "golden", F.configs.Q_PHYS, "cos", cuda_device)
+    rng = np.random.default_rng(11)
+    b = rng.standard_normal(S.nr) + 1j * rng.standard_normal(S.nr)
+    y_ref = O.make_explicit_krinv_compact(S, 1e-13, 3000)[0](b)
+    bd = torch.as_tensor(b, device=cuda_device)
+    its = {}
+    for target, bound in ((0.1, 1e-11), (1.0, 1e-10)):
+        op, stats = F.make_explicit_krinv_compact(sg, 1e-10, 3000, precision="mixed", refineTarget=target)
+        y = op(bd).cpu().numpy()
+        st = stats()
+        assert st.maxRelativeResidual <= bound, (target, st.maxRelativeResidual)
+        assert _rel(y, y_ref) < 1e-8, (target, _rel(y, y_ref))
+        its[target] = st.fp32Iterations
+    assert its[1.0] <= its[0.1], its
+    sol = O.solve_modes(S, nev=10, p=40, tol=1e-10, maxRestart=30, tolCG=1e-12)
+    lam_rr_oracle = O.rayleigh_ritz_Kr(sol["Y"], S)[0]
+    op, _ = F.make_explicit_krinv_compact(sg, 1e-10, 3000, precision="mixed", **F.configs.MIXED_OPTS)
+    Y, theta, _, info = F.Lanczos(op, None, None, sg.nr, 10, 1e-8, 30, 40, F.start_vector(F.configs.SEED, sg.nr))
+    assert info["converged"]
+    lam = np.sort(1.0 / theta)
+    assert np.max(np.abs(lam - sol["lam"]) / sol["lam"]) < 2e-9
+    lam_rr, _ = F.rayleigh_ritz(sg, Y)
+    assert np.max(np.abs(lam_rr - lam_rr_oracle) / lam_rr_oracle) < 1e-10
+    for bad in (0.0, -1.0, 1.5):
+        with pytest.raises(F.FameError):
+            F.make_explicit_krinv_compact(sg, 1e-10, 3000, precision="mixed", refineTarget=bad)
+
+
 def test_pivoted_split_when_v1_is_singular(cuda_device):
     """q_3 = 0 makes the reference's V1 block singular for xi = 0; the basis pivots and
     the explicit K_r^{-1} then agrees with the nested one (which never inverts V1)."""
