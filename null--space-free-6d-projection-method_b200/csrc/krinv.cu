@@ -138,11 +138,12 @@ int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
                                               " relres=" + std::to_string(relres) +
                                               " iter=" + std::to_string(h.iter));
   } else {
-    // FP64 iterative refinement: u (=B.x, zero) ; r64 (=B.r) = bhat
-    FAME_TRY(read_back(K->ctx, st, &h, sizeof(PcgState)));
-    if (h.flag == -1) return fail(FAME_ERR_NONFINITE, "Mhat right-hand side contains NaN/Inf");
-    const double bn2 = h.bnorm2;
-    double rn2 = h.rho;
+    // FP64 iterative refinement: u (=B.x, zero) ; r64 (=B.r) = bhat.  The first round
+    // always runs, so ||bhat||^2 is read with the first refinement residual instead of
+    // here (a zero bhat gives a converged FP32 solve and a zero residual; NaN/Inf in
+    // bhat reaches the FP32 solve's initial norm).
+    double bn2 = 1.0, rn2 = 1.0;
+    bool first = true;
     PcgBuf<float>& F = K->b32;
     PcgState* st32 = K->st32;
     float* partials32 = reinterpret_cast<float*>(K->partials);
@@ -152,12 +153,15 @@ int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
     // FP32 corrections leave no FP64-PCG overshoot below it, so the default of 0.1 keeps
     // the Lanczos eigenvalues within tolCG of the FP64 form's before any Rayleigh-Ritz step
     const double tolIR = K->o.refineTarget * tolMhat;
-    while (rn2 > tolIR * tolIR * bn2 && bn2 > 0) {
+    while (first || (rn2 > tolIR * tolIR * bn2 && bn2 > 0)) {
       if (refine >= K->o.maxRefine) break;
       ++refine;
+      first = false;
       // a round needs only the reduction that takes the residual to the target: the FP32
       // solve is asked for half of it, never for less than tolInner32 (its accuracy floor)
-      const double need = tolIR * std::sqrt(bn2 / rn2);
+      const double need = refine == 1 ? tolIR : tolIR * std::sqrt(bn2 / rn2);
+      // the first chunk of queued iterations is sized from this round of the previous call
+      int& hint = K->lastIt32Round[std::min(refine, kRoundHints) - 1];
       const double tau = std::min(1e-2, std::max(K->o.tolInner32, 0.5 * need));
       k_pcg_init<float, double><<<vec_blocks(NF), 256, 0, s>>>(B.r, F.r, F.x, NF, st32,
                                                               tau, K->o.maxitCG,
@@ -166,13 +170,13 @@ int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
       PcgState h32{};
       if (K->o.mhatPreconditioner) {
         FAME_TRY(pcg_iterate<float>(K, OpMhatPre<float>{coef_line_of<float>(bs), es_of<float>(K->m), K->m->EtInv32},
-                                    F, st32, K->lastIt32, h32, false, nullptr));
+                                    F, st32, hint, h32, false, nullptr));
       } else {
         FAME_TRY(pcg_iterate<float>(K, OpMhat<float>{coef_line_of<float>(bs), es_of<float>(K->m)}, F, st32,
-                                    K->lastIt32, h32, false, nullptr));
+                                    hint, h32, false, nullptr));
       }
-      if (h32.flag == -1 || h32.flag == 4)
-        return fail(FAME_ERR_NOT_CONVERGED, "FP32 correction solve broke down");
+      if (h32.flag == -1) return fail(FAME_ERR_NONFINITE, "Mhat right-hand side contains NaN/Inf");
+      if (h32.flag == 4) return fail(FAME_ERR_NOT_CONVERGED, "FP32 correction solve broke down");
       K->stats.fp32Iterations += h32.iter;
       iters += h32.iter;
       // u += dx ; r64 = bhat - Mhat u  (FP64 residual)
@@ -181,6 +185,10 @@ int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
       FAME_TRY((run_chain_lin<double, 3>(K->n, pro, epi, B.work, K->m->Et64, NF, s)));
       K->stats.massApplies += 3;
       FAME_TRY(read_back(K->ctx, st, &h, sizeof(PcgState)));
+      if (refine == 1) {
+        if (h.flag == -1) return fail(FAME_ERR_NONFINITE, "Mhat right-hand side contains NaN/Inf");
+        bn2 = h.bnorm2;
+      }
       rn2 = h.rho;
       if (!std::isfinite(rn2)) return fail(FAME_ERR_NONFINITE, "refinement residual is NaN/Inf");
     }

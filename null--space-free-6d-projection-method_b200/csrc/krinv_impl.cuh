@@ -22,6 +22,10 @@ struct OuterState {
 
 }  // namespace fame
 
+// refinement rounds of the mixed explicit K_r^{-1} that keep their own chunk hint (later
+// rounds share the last one)
+constexpr int kRoundHints = 4;
+
 struct fame_krinv {
   fame_basis* b = nullptr;
   fame_mass* m = nullptr;
@@ -37,6 +41,7 @@ struct fame_krinv {
   unsigned* counter = nullptr;
   fame::PcgState *st64 = nullptr, *st32 = nullptr;
   int lastIt64 = 0, lastIt32 = 0;
+  int lastIt32Round[kRoundHints] = {};  // explicit mixed: FP32 iterations of each refinement round
   // nested (method B) outer vectors, 2NF each
   double2 *ox = nullptr, *orr = nullptr, *oz = nullptr, *op = nullptr, *oq = nullptr;
   double* sigma = nullptr;  // |q|^2 (NF), sigma_r = [sigma; sigma]
