@@ -47,8 +47,9 @@ struct fame_krinv {
   double* sigma = nullptr;  // |q|^2 (NF), sigma_r = [sigma; sigma]
   fame::OuterState* ost = nullptr;
   void* lanczos_ws = nullptr;  // Lanczos basis workspace reused across solves
-  // CUDA graphs of kGraphIters PCG iterations, one per (precision, operator)
-  cudaGraphExec_t graphs[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  // CUDA graphs of PCG iterations per (precision, operator): [slot] holds kGraphIters
+  // iterations, [6 + slot] one iteration (the remainder of a chunk)
+  cudaGraphExec_t graphs[12] = {};
 };
 
 namespace fame {
@@ -130,7 +131,11 @@ template <typename T> struct OpMhatPre {
   }
 };
 
-// PCG iterations per captured graph.
+// PCG iterations per captured graph.  A chunk of c iterations replays the graph of
+// kGraphIters iterations c / kGraphIters times and a one-iteration graph for the rest,
+// so it queues exactly the iterations asked for: surplus iterations are gated off on
+// the device but still cost their launches (~15 us per iteration at 2N = 10), and
+// every graph launch adds a few microseconds on the device.
 constexpr int kGraphIters = 4;
 
 template <typename T, class Op> constexpr int graph_slot() {
@@ -152,56 +157,70 @@ int enqueue_iterations(fame_krinv* K, const Op& op, PcgBuf<T>& B, PcgState* st, 
   return FAME_OK;
 }
 
-// Queue `count` gated PCG iterations: as replays of a captured graph of
-// kGraphIters iterations (count rounded up; surplus iterations are gated
-// off by the device state), or as plain launches before the graph exists.
+// Capture `iters` PCG iterations as a graph (on a capture stream, so that the work
+// already queued on the context stream is not part of it).
+template <typename T, class Op>
+int capture_iterations(fame_krinv* K, const Op& op, PcgBuf<T>& B, PcgState* st, int iters, cudaGraphExec_t& ge) {
+  cudaStream_t cs = K->ctx->own;
+  if (cs == K->ctx->stream) {
+    if (!K->ctx->capture) FAME_CUDA_TRY(cudaStreamCreateWithFlags(&K->ctx->capture, cudaStreamNonBlocking));
+    cs = K->ctx->capture;
+  }
+  cudaGraph_t g = nullptr;
+  FAME_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+  const int st_enq = enqueue_iterations<T>(K, op, B, st, cs, iters);
+  const cudaError_t e_end = cudaStreamEndCapture(cs, &g);
+  if (st_enq != FAME_OK) {
+    if (g) cudaGraphDestroy(g);
+    return st_enq;
+  }
+  if (e_end != cudaSuccess) return fail(FAME_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e_end));
+  const cudaError_t e_inst = cudaGraphInstantiate(&ge, g, 0);
+  cudaGraphDestroy(g);
+  if (e_inst != cudaSuccess) {
+    ge = nullptr;
+    return fail(FAME_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e_inst));
+  }
+  return FAME_OK;
+}
+
+// Queue `count` gated PCG iterations: replays of the captured graphs of kGraphIters
+// and of one iteration, or plain launches before the graphs exist (the first
+// iterations run eagerly, so that kernel attributes are set and modules loaded
+// before the capture).
 template <typename T, class Op>
 int queue_iterations(fame_krinv* K, const Op& op, PcgBuf<T>& B, PcgState* st, int count) {
   cudaStream_t s = K->ctx->stream;
-  cudaGraphExec_t& ge = K->graphs[graph_slot<T, Op>()];
   if (!K->o.useGraphs) return enqueue_iterations<T>(K, op, B, st, s, count);
+  cudaGraphExec_t& ge = K->graphs[graph_slot<T, Op>()];
+  cudaGraphExec_t& ge1 = K->graphs[6 + graph_slot<T, Op>()];
   if (!ge) {
-    // the first iterations run eagerly (kernel attributes set, modules loaded), then capture
-    FAME_TRY(enqueue_iterations<T>(K, op, B, st, s, kGraphIters));
-    count -= kGraphIters;
-    cudaStream_t cs = K->ctx->own;
-    if (cs == s) {
-      if (!K->ctx->capture) FAME_CUDA_TRY(cudaStreamCreateWithFlags(&K->ctx->capture, cudaStreamNonBlocking));
-      cs = K->ctx->capture;
-    }
-    cudaGraph_t g = nullptr;
-    FAME_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    const int st_enq = enqueue_iterations<T>(K, op, B, st, cs, kGraphIters);
-    const cudaError_t e_end = cudaStreamEndCapture(cs, &g);
-    if (st_enq != FAME_OK) {
-      if (g) cudaGraphDestroy(g);
-      return st_enq;
-    }
-    if (e_end != cudaSuccess) return fail(FAME_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e_end));
-    const cudaError_t e_inst = cudaGraphInstantiate(&ge, g, 0);
-    cudaGraphDestroy(g);
-    if (e_inst != cudaSuccess) {
-      ge = nullptr;
-      return fail(FAME_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e_inst));
-    }
+    const int eager = std::min(count, kGraphIters);
+    FAME_TRY(enqueue_iterations<T>(K, op, B, st, s, eager));
+    count -= eager;
+    FAME_TRY(capture_iterations<T>(K, op, B, st, kGraphIters, ge));
   }
-  for (int done = 0; done < count; done += kGraphIters) {
+  for (; count >= kGraphIters; count -= kGraphIters) {
     FAME_CUDA_TRY(cudaGraphLaunch(ge, s));
     ::fame::count_launch((long long)Op::launches_per_iter * kGraphIters);
+  }
+  if (count > 0 && !ge1) FAME_TRY(capture_iterations<T>(K, op, B, st, 1, ge1));
+  for (; count > 0; --count) {
+    FAME_CUDA_TRY(cudaGraphLaunch(ge1, s));
+    ::fame::count_launch((long long)Op::launches_per_iter);
   }
   return FAME_OK;
 }
 
 // Queue PCG iterations until the device state stops them; the host reads the
-// state once per chunk (the first chunk is sized from the previous solve's
-// iteration count).  With verify, convergence is confirmed on the true
+// state once per chunk (the first chunk is the previous solve's iteration count).  With verify, convergence is confirmed on the true
 // residual as MATLAB pcg does, continuing up to three times if it fails.
 template <typename T, class Op>
 int pcg_iterate(fame_krinv* K, const Op& op, PcgBuf<T>& B, PcgState* st, int& lastIt, PcgState& h,
                 bool verify, const C<T>* b) {
   cudaStream_t s = K->ctx->stream;
   const int every = std::max(1, K->o.checkEvery);
-  int chunk = lastIt > 4 ? lastIt - 2 : every;
+  int chunk = lastIt > 0 ? lastIt : every;  // iteration counts repeat from call to call
   int queued = 0, moresteps = 0;
   for (;;) {
     FAME_TRY((queue_iterations<T, Op>(K, op, B, st, chunk)));
