@@ -108,11 +108,25 @@ __global__ void __launch_bounds__(256) k_gemv_n_sub(const double2* __restrict__ 
   for (long long row = blockIdx.x * (long long)blockDim.x + threadIdx.x; row < n;
        row += (long long)gridDim.x * blockDim.x) {
     double2 v = w[row];
-    for (int j = 0; j < m; ++j) {
-      const double2 q = Q[row + ldq * j];
-      v.x -= q.x * c[j].x - q.y * c[j].y;
-      v.y -= q.x * c[j].y + q.y * c[j].x;
+    // Q(row, :) c in four partial sums (j = 4t + u): the column loads and the FP64
+    // chains of consecutive columns overlap
+    double sr[4] = {0.0, 0.0, 0.0, 0.0}, si[4] = {0.0, 0.0, 0.0, 0.0};
+    int j = 0;
+    for (; j + 4 <= m; j += 4) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const double2 q = Q[row + ldq * (j + u)], cj = c[j + u];
+        sr[u] += q.x * cj.x - q.y * cj.y;
+        si[u] += q.x * cj.y + q.y * cj.x;
+      }
     }
+    for (; j < m; ++j) {
+      const double2 q = Q[row + ldq * j], cj = c[j];
+      sr[0] += q.x * cj.x - q.y * cj.y;
+      si[0] += q.x * cj.y + q.y * cj.x;
+    }
+    v.x -= (sr[0] + sr[1]) + (sr[2] + sr[3]);
+    v.y -= (si[0] + si[1]) + (si[2] + si[3]);
     w[row] = v;
     acc.v[0] += v.x * v.x + v.y * v.y;
   }
@@ -120,80 +134,90 @@ __global__ void __launch_bounds__(256) k_gemv_n_sub(const double2* __restrict__ 
 }
 
 // Between two Gram-Schmidt passes: w -= Q c (c = the previous pass's coefficients),
-// then this block's share of the next pass's Q^H w, both from one read of Q.  Each
-// warp stages the 32 x m tile of its 32 rows in shared memory (cp.async; row stride
-// m|1, so the sweep along a row and the sweep along a column are both free of bank
-// conflicts), subtracts along its rows, and accumulates the inner products along the
-// columns: lane l owns columns l and l + 32 (m <= 64).  partial[b*m + j] as k_gemv_h.
-constexpr int kFuseWarps = 4;
+// then this block's share of the next pass's Q^H w, both from one read of Q in HBM.
+// The block walks blocks of kFuseRows rows: each thread first updates one row of w
+// (reading that row of Q from HBM), then the warps form the inner products of the
+// block's rows with the updated w, re-reading those rows of Q while they are still in
+// L1/L2 (kFuseRows x m x 16 bytes per block; at most ~1 MB per SM in flight).  Warp
+// k owns columns k, k + kFuseWarps, ... and keeps their sums in registers across the
+// row blocks; lane l takes rows l, l + 32, ... of a row block.  partial[b*m + j] as
+// k_gemv_h.
+constexpr int kFuseWarps = 8;
+constexpr int kFuseRows = kFuseWarps * 32;
 constexpr int kFuseMaxCols = 64;
-constexpr size_t kFuseSmemMax = (size_t)kFuseWarps * 32 * (kFuseMaxCols + 1) * sizeof(double2);
+constexpr int kFuseColsPerWarp = kFuseMaxCols / kFuseWarps;
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
-__global__ void __launch_bounds__(kFuseWarps * 32) k_cgs_sub_dot(const double2* __restrict__ Q, long long ldq, int m,
-                                                                 const double2* __restrict__ coef,
-                                                                 double2* __restrict__ w, long long n,
-                                                                 double2* __restrict__ partial) {
-  extern __shared__ double2 tiles[];  // [kFuseWarps][32][m|1]
+__global__ void __launch_bounds__(kFuseRows) k_cgs_sub_dot(const double2* __restrict__ Q, long long ldq, int m,
+                                                           const double2* __restrict__ coef,
+                                                           double2* __restrict__ w, long long n,
+                                                           double2* __restrict__ partial) {
   __shared__ double2 c[kFuseMaxCols];
-  __shared__ double2 red[kFuseWarps][kFuseMaxCols];
-  const int ms = m | 1;
+  __shared__ double2 vs[kFuseRows];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  double2* tile = tiles + (size_t)wid * 32 * ms;
-  double2* mine = tile + lane * ms;
   for (int j = threadIdx.x; j < m; j += blockDim.x) c[j] = coef[j];
+  double ar[kFuseColsPerWarp], ai[kFuseColsPerWarp];
+#pragma unroll
+  for (int k = 0; k < kFuseColsPerWarp; ++k) ar[k] = ai[k] = 0.0;
   __syncthreads();
-  double a0r = 0.0, a0i = 0.0, a1r = 0.0, a1i = 0.0;
-  const long long groups = (n + 31) >> 5;
-  for (long long g = (long long)blockIdx.x * kFuseWarps + wid; g < groups; g += (long long)gridDim.x * kFuseWarps) {
-    const long long row = (g << 5) + lane;
-    const bool live = row < n;
-    __syncwarp();  // the previous group's column sweep is done with the tile
-    if (live) {
-      const double2* src = Q + row;
-      for (int j = 0; j < m; ++j) cp_async16(mine + j, src + ldq * j);
-    } else {
-      for (int j = 0; j < m; ++j) mine[j] = make_double2(0.0, 0.0);
-    }
-    double2 v = live ? w[row] : make_double2(0.0, 0.0);
-    cp_async_wait_all();
-    __syncwarp();
-    for (int j = 0; j < m; ++j) {
-      const double2 q = mine[j], cj = c[j];
-      v.x -= q.x * cj.x - q.y * cj.y;
-      v.y -= q.x * cj.y + q.y * cj.x;
-    }
-    if (live) w[row] = v;
-    for (int r = 0; r < 32; ++r) {
-      const double vx = __shfl_sync(0xffffffffu, v.x, r), vy = __shfl_sync(0xffffffffu, v.y, r);
-      const double2* tr = tile + r * ms;
-      if (lane < m) {
-        const double2 q = tr[lane];
-        a0r += q.x * vx + q.y * vy;
-        a0i += q.x * vy - q.y * vx;
+  const long long blocks = (n + kFuseRows - 1) / kFuseRows;
+  for (long long b = blockIdx.x; b < blocks; b += gridDim.x) {
+    const long long r0 = b * kFuseRows;
+    {  // w(row) -= Q(row, :) c, in four partial sums (j = 4t + u)
+      const long long row = r0 + threadIdx.x;
+      double2 v = make_double2(0.0, 0.0);
+      if (row < n) {
+        double sr[4] = {0.0, 0.0, 0.0, 0.0}, si[4] = {0.0, 0.0, 0.0, 0.0};
+        int j = 0;
+        for (; j + 4 <= m; j += 4) {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const double2 q = Q[row + ldq * (j + u)], cj = c[j + u];
+            sr[u] += q.x * cj.x - q.y * cj.y;
+            si[u] += q.x * cj.y + q.y * cj.x;
+          }
+        }
+        for (; j < m; ++j) {
+          const double2 q = Q[row + ldq * j], cj = c[j];
+          sr[0] += q.x * cj.x - q.y * cj.y;
+          si[0] += q.x * cj.y + q.y * cj.x;
+        }
+        v = w[row];
+        v.x -= (sr[0] + sr[1]) + (sr[2] + sr[3]);
+        v.y -= (si[0] + si[1]) + (si[2] + si[3]);
+        w[row] = v;
       }
-      if (lane + 32 < m) {
-        const double2 q = tr[lane + 32];
-        a1r += q.x * vx + q.y * vy;
-        a1i += q.x * vy - q.y * vx;
+      vs[threadIdx.x] = v;  // zero past the end
+    }
+    __syncthreads();
+    // inner products of this row block with the owned columns
+#pragma unroll
+    for (int k = 0; k < kFuseColsPerWarp; ++k) {
+      const int j = wid + kFuseWarps * k;
+      if (j < m) {
+        const double2* qj = Q + ldq * j + r0;
+#pragma unroll
+        for (int i = 0; i < kFuseRows / 32; ++i) {
+          const int r = lane + 32 * i;
+          if (r0 + r < n) {
+            const double2 q = qj[r], v = vs[r];
+            ar[k] += q.x * v.x + q.y * v.y;
+            ai[k] += q.x * v.y - q.y * v.x;
+          }
+        }
       }
     }
+    __syncthreads();  // vs is rewritten by the next row block
   }
-  if (lane < m) red[wid][lane] = make_double2(a0r, a0i);
-  if (lane + 32 < m) red[wid][lane + 32] = make_double2(a1r, a1i);
-  __syncthreads();
-  for (int j = threadIdx.x; j < m; j += blockDim.x) {
-    double sr = 0.0, si = 0.0;
-    for (int k = 0; k < kFuseWarps; ++k) {
-      sr += red[k][j].x;
-      si += red[k][j].y;
+#pragma unroll
+  for (int k = 0; k < kFuseColsPerWarp; ++k) {
+    const int j = wid + kFuseWarps * k;
+    double sr = ar[k], si = ai[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sr += __shfl_xor_sync(0xffffffffu, sr, o);
+      si += __shfl_xor_sync(0xffffffffu, si, o);
     }
-    partial[(long long)blockIdx.x * m + j] = make_double2(sr, si);
+    if (j < m && lane == 0) partial[(long long)blockIdx.x * m + j] = make_double2(sr, si);
   }
 }
 
@@ -369,7 +393,6 @@ struct LanczosWs {
     FAME_TRY(dalloc((void**)&v, n * sizeof(double2)));
     FAME_TRY(dalloc((void**)&coef, kMaxCols * sizeof(double2)));
     FAME_TRY(dalloc((void**)&partial, (size_t)nblk * p * sizeof(double2)));
-    FAME_CUDA_TRY(cudaFuncSetAttribute(k_cgs_sub_dot, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFuseSmemMax));
     FAME_TRY(dalloc((void**)&scal, 8 * sizeof(double)));
     FAME_TRY(dalloc((void**)&partials, 4 * kVecBlocksMax * sizeof(double)));
     FAME_TRY(dalloc((void**)&counter, sizeof(unsigned)));
@@ -399,12 +422,16 @@ struct LanczosWs {
     std::memcpy(h, hbuf, bytes);
     return FAME_OK;
   }
-  // blocks of k_cgs_sub_dot: persistent over the row groups, as many as fit at once,
-  // and no more than the partial buffer's nblk rows
-  int fuse_blocks(int m) const {
-    const size_t smem = (size_t)kFuseWarps * 32 * (m | 1) * sizeof(double2) + 6 * 1024;
-    const long long per_sm = std::max<long long>(1, std::min<long long>(16, (227 * 1024) / (long long)smem));
-    const long long need = ((n + 31) / 32 + kFuseWarps - 1) / kFuseWarps;
+  // blocks of k_cgs_sub_dot: persistent over the row blocks, as many as are resident at
+  // once, and no more than the partial buffer's nblk rows
+  int fuse_blocks() const {
+    int resident = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_cgs_sub_dot, kFuseRows, 0) != cudaSuccess) {
+      cudaGetLastError();
+      resident = 4;
+    }
+    const long long per_sm = std::max(1, resident);
+    const long long need = (n + kFuseRows - 1) / kFuseRows;
     return (int)std::max<long long>(1, std::min<long long>({need, 148 * per_sm, (long long)nblk}));
   }
   // `passes` classical Gram-Schmidt passes against Q(:,0:m): alpha = Re of the first
@@ -419,9 +446,8 @@ struct LanczosWs {
     ::fame::count_launch();
     for (int pass = 1; pass < passes; ++pass) {
       if (m <= kFuseMaxCols) {
-        const int g = fuse_blocks(m);
-        const size_t smem = (size_t)kFuseWarps * 32 * (m | 1) * sizeof(double2);
-        k_cgs_sub_dot<<<g, kFuseWarps * 32, smem, s>>>(Q, n, m, coef, w, n, partial);
+        const int g = fuse_blocks();
+        k_cgs_sub_dot<<<g, kFuseRows, 0, s>>>(Q, n, m, coef, w, n, partial);
         ::fame::count_launch();
         k_gemv_h_reduce<<<m, 256, 0, s>>>(partial, g, m, coef, scal, 0);
         ::fame::count_launch();
