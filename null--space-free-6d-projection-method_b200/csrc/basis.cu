@@ -17,10 +17,6 @@ struct BasisReduce {
   unsigned int nsingular;
 };
 
-__device__ __forceinline__ void atomic_min_pos_double(unsigned long long* a, double v) {
-  atomicMin(a, (unsigned long long)__double_as_longlong(v));
-}
-
 struct BasisArgs {
   int N, n;
   int piv;  // physical component used as the third block row (V3); V1 = the other two
@@ -41,6 +37,9 @@ struct BasisArgs {
 
 __global__ void k_build_basis(BasisArgs a) {
   const double tol = 1e-13;
+  // min |q|^2 and min |det V1| as bit patterns of non-negative doubles (their integer
+  // order is their numeric order), reduced per thread and per warp: one atomic per warp
+  unsigned long long mq = ~0ull, md = ~0ull;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.NF;
        i += (long long)gridDim.x * blockDim.x) {
     double q[3] = {0.0, 0.0, 0.0};
@@ -127,8 +126,20 @@ __global__ void k_build_basis(BasisArgs a) {
       a.W2f_l[il] = make_float2((float)W2, 0.f);
       a.invCf_l[il] = (float)invC;
     }
-    atomic_min_pos_double(&a.red->minQq, Qq);
-    atomic_min_pos_double(&a.red->minAbsDet, fabs(det));
+    const unsigned long long bq = (unsigned long long)__double_as_longlong(Qq);
+    const unsigned long long bd = (unsigned long long)__double_as_longlong(fabs(det));
+    mq = bq < mq ? bq : mq;
+    md = bd < md ? bd : md;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long oq = __shfl_xor_sync(0xffffffffu, mq, o), od = __shfl_xor_sync(0xffffffffu, md, o);
+    mq = oq < mq ? oq : mq;
+    md = od < md ? od : md;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&a.red->minQq, mq);
+    atomicMin(&a.red->minAbsDet, md);
   }
 }
 
