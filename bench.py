@@ -214,6 +214,9 @@ def run_fame(args):
         times, launches = [], 0
         res = None
         for _ in range(steps):
+            # the previous step's eigenvectors go back to the allocator first, so that every
+            # step reuses one cached output block instead of one step mapping a second one
+            res = None
             flush.zero_()
             barrier()
             l0 = F.kernel_launches()
