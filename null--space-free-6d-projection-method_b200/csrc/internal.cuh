@@ -122,6 +122,9 @@ struct LanczosOperator {
   void** ws;
   int (*apply)(void* self, const double2* x, double2* y);
   void* self;
+  // optional: reports an error of the last apply that was left for Lanczos to detect
+  // (called when the step's Lanczos coefficients come back NaN/Inf)
+  int (*check)(void* self) = nullptr;
 };
 int lanczos_run(const LanczosOperator& op, int nev, double tol, int maxiter, int p, const void* v0, double* theta,
                 void* Y, fame_lanczos_info* info);

@@ -102,6 +102,15 @@ template <> MhatCoef<float> coef_line_of<float>(fame_basis* b) { return MhatCoef
 template <> const double* es_of<double>(fame_mass* m) { return m->Et64; }
 template <> const float* es_of<float>(fame_mass* m) { return m->Et32; }
 
+// NaN/Inf test of the last explicit K_r^{-1} output (the post chain's count in aux).
+int krinv_output_check(fame_krinv* K) {
+  if (K->o.kind != FAME_KRINV_EXPLICIT) return FAME_OK;
+  PcgState h{};
+  FAME_TRY(read_back(K->ctx, K->st64, &h, sizeof(PcgState)));
+  if (h.aux != 0.0) return fail(FAME_ERR_NONFINITE, "Explicit K_r^{-1} output contains NaN/Inf");
+  return FAME_OK;
+}
+
 int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
   fame_basis* bs = K->b;
   cudaStream_t s = K->ctx->stream;
@@ -206,8 +215,7 @@ int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
     FAME_TRY((run_chain<double, 2>(K->n, pro, epi, B.work, K->m->Et64, NF, s)));
     K->stats.massApplies += 2;
   }
-  FAME_TRY(read_back(K->ctx, st, &h, sizeof(PcgState)));
-  if (h.aux != 0.0) return fail(FAME_ERR_NONFINITE, "Explicit K_r^{-1} output contains NaN/Inf");
+  if (!K->deferOutputCheck) FAME_TRY(krinv_output_check(K));
   K->stats.inverseCalls += 1;
   K->stats.totalIterations += iters;
   K->stats.maxIterations = std::max<long long>(K->stats.maxIterations, iters);

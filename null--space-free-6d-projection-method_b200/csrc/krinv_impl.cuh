@@ -47,6 +47,10 @@ struct fame_krinv {
   double* sigma = nullptr;  // |q|^2 (NF), sigma_r = [sigma; sigma]
   fame::OuterState* ost = nullptr;
   void* lanczos_ws = nullptr;  // Lanczos basis workspace reused across solves
+  // set while Lanczos applies the explicit operator: the NaN/Inf test of each output is
+  // left to Lanczos, whose own read of the step's coefficients would see it, instead of
+  // costing a host synchronisation per call (krinv_output_check runs it on demand)
+  bool deferOutputCheck = false;
   // CUDA graphs of PCG iterations per (precision, operator): [slot] holds kGraphIters
   // iterations, [6 + slot] one iteration (the remainder of a chunk)
   cudaGraphExec_t graphs[12] = {};
@@ -56,6 +60,7 @@ namespace fame {
 int nested_alloc(fame_krinv* K);
 void nested_free(fame_krinv* K);
 int krinv_nested_apply_one(fame_krinv* K, const double2* b, double2* x);
+int krinv_output_check(fame_krinv* K);
 void lanczos_ws_free(fame_krinv* K);
 int recover_one(fame_krinv* K, const double2* y, double2* X, double2* MX, int* iters, double* relres);
 template <typename T> MhatCoef<T> coef_of(fame_basis* b);       // natural order

@@ -554,6 +554,10 @@ int lanczos_run(const LanczosOperator& op, int nev, double tol, int maxiter, int
       double sc[2];
       FAME_TRY(L.sync_read(L.scal, sc, 2 * sizeof(double)));
       const double alpha = sc[1], beta2 = sc[0];
+      if (op.check && !(std::isfinite(alpha) && std::isfinite(beta2))) {
+        FAME_TRY(op.check(op.self));  // the operator's own error first
+        return fail(FAME_ERR_NONFINITE, "Lanczos coefficients are NaN/Inf");
+      }
       if (!(beta2 > 0.0) || std::sqrt(beta2) < 1e-14) {  // exp2/Lanczos.m:75-79
         beta = std::sqrt(std::max(beta2, 0.0));
         break;
@@ -651,13 +655,19 @@ using namespace fame;
 
 namespace {
 int krinv_lanczos_apply(void* self, const double2* x, double2* y) {
-  return fame_krinv_apply(static_cast<fame_krinv*>(self), x, y, 1);
+  fame_krinv* K = static_cast<fame_krinv*>(self);
+  K->deferOutputCheck = true;
+  const int st = fame_krinv_apply(K, x, y, 1);
+  K->deferOutputCheck = false;
+  return st;
 }
+int krinv_lanczos_check(void* self) { return krinv_output_check(static_cast<fame_krinv*>(self)); }
 }  // namespace
 
 extern "C" int fame_lanczos(fame_krinv* K, int nev, double tol, int maxiter, int p, const void* v0,
                             double* theta, void* Y, fame_lanczos_info* info) {
   if (!K) return fail(FAME_ERR_INVALID, "fame_lanczos: K is NULL");
   LanczosOperator op{K->ctx, 2 * K->NF, &K->lanczos_ws, krinv_lanczos_apply, K};
+  op.check = krinv_lanczos_check;
   return lanczos_run(op, nev, tol, maxiter, p, v0, theta, Y, info);
 }
