@@ -167,14 +167,13 @@ int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
       ++refine;
       first = false;
       // a round needs only the reduction that takes the residual to the target: the FP32
-      // solve is asked for half of it, never for less than tolInner32 (its accuracy floor)
-      const double need = refine == 1 ? tolIR : tolIR * std::sqrt(bn2 / rn2);
+      // solve is asked for half of it, never for less than tolInner32 (its accuracy floor);
+      // k_pcg_init takes it on the device from the FP64 state (residual and ||bhat||)
       // the first chunk of queued iterations is sized from this round of the previous call
       int& hint = K->lastIt32Round[std::min(refine, kRoundHints) - 1];
-      const double tau = std::min(1e-2, std::max(K->o.tolInner32, 0.5 * need));
       k_pcg_init<float, double><<<vec_blocks(NF), 256, 0, s>>>(B.r, F.r, F.x, NF, st32,
-                                                              tau, K->o.maxitCG,
-                                                              partials32, K->counter);
+                                                              K->o.tolInner32, K->o.maxitCG,
+                                                              partials32, K->counter, st, tolIR);
       ::fame::count_launch();
       PcgState h32{};
       if (K->o.mhatPreconditioner) {
@@ -193,11 +192,15 @@ int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
       EpiResidMhat<double> epi{c, K->bhat, B.r, &st->rho, K->partials, K->counter};
       FAME_TRY((run_chain_lin<double, 3>(K->n, pro, epi, B.work, K->m->Et64, NF, s)));
       K->stats.massApplies += 3;
-      FAME_TRY(read_back(K->ctx, st, &h, sizeof(PcgState)));
-      if (refine == 1) {
-        if (h.flag == -1) return fail(FAME_ERR_NONFINITE, "Mhat right-hand side contains NaN/Inf");
-        bn2 = h.bnorm2;
+      // a second round always follows the first (one FP32 round reaches ~3e-6), and it
+      // takes its tolerance on the device, so the host reads the residual from then on
+      if (refine == 1 && K->o.maxRefine > 1) {
+        first = true;
+        continue;
       }
+      FAME_TRY(read_back(K->ctx, st, &h, sizeof(PcgState)));
+      if (h.flag == -1) return fail(FAME_ERR_NONFINITE, "Mhat right-hand side contains NaN/Inf");
+      bn2 = h.bnorm2;
       rn2 = h.rho;
       if (!std::isfinite(rn2)) return fail(FAME_ERR_NONFINITE, "refinement residual is NaN/Inf");
     }

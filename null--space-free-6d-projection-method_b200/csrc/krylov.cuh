@@ -507,11 +507,16 @@ __global__ void __launch_bounds__(256) k_pcg_finish(C<T>* x, C<T>* r, const C<T>
   }
 }
 
-// PCG start with x0 = 0: r = (T) b, x = 0, rho = ||r||^2.
+// PCG start with x0 = 0: r = (T) b, x = 0, rho = ||r||^2.  With ref (a correction
+// solve of FP64 iterative refinement, b the refinement residual whose squared norm and
+// right-hand side norm ref holds): the relative tolerance is half the reduction that
+// takes ||b|| to tolIR ||bhat||, at least tol and at most 1e-2, and a residual already at
+// the target starts converged (no iterations).
 template <typename T, typename TB>
 __global__ void __launch_bounds__(256) k_pcg_init(const C<TB>* b, C<T>* r, C<T>* x, long long n,
                                                  PcgState* st, double tol, int maxit, T* partials,
-                                                 unsigned* counter) {
+                                                 unsigned* counter, const PcgState* ref = nullptr,
+                                                 double tolIR = 0.0) {
   Red<T, 1> acc;
   acc.v[0] = 0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -522,7 +527,18 @@ __global__ void __launch_bounds__(256) k_pcg_init(const C<TB>* b, C<T>* r, C<T>*
     acc.v[0] += cabs2<T>(ri);
   }
   grid_sum_finalize<T, 1>(acc, partials, counter, [&](const Red<T, 1>& tot) {
-    pcg_init_state(st, (double)tot.v[0], tol, maxit);
+    double tau = tol;
+    bool at_target = false;
+    if (ref) {
+      const double bn2 = ref->bnorm2, rn2 = ref->rho;
+      at_target = rn2 <= tolIR * tolIR * bn2 || !(bn2 > 0.0);
+      if (!at_target) tau = fmin(1e-2, fmax(tol, 0.5 * tolIR * sqrt(bn2 / rn2)));
+    }
+    pcg_init_state(st, (double)tot.v[0], tau, maxit);
+    if (at_target && st->flag == 0) {
+      st->active = 0;
+      st->conv = 1;
+    }
   });
 }
 
