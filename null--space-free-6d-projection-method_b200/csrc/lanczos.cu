@@ -229,11 +229,15 @@ __global__ void k_nrm2(const double2* x, long long n, double* scal, double* part
   grid_sum_finalize<double, 1>(acc, partials, counter, [&](const Red<double, 1>& t) { scal[0] = t.v[0]; });
 }
 
-// y = x / sqrt(scal[0])
-__global__ void k_scale_inv_sqrt(const double2* x, double2* y, long long n, const double* scal) {
+// y = x / sqrt(scal[0]), also into y2 when given (the next column of the Krylov basis)
+__global__ void k_scale_inv_sqrt(const double2* x, double2* y, long long n, const double* scal,
+                                 double2* y2 = nullptr) {
   const double s = 1.0 / sqrt(scal[0]);
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    y[i] = cscale<double>(x[i], s);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double2 v = cscale<double>(x[i], s);
+    y[i] = v;
+    if (y2) y2[i] = v;
+  }
 }
 
 // out(:, c0:c0+CT) = Q(:, 0:m) * U(0:m, c0:c0+CT)  (U real, column-major ldU = m)
@@ -535,6 +539,7 @@ int lanczos_run(const LanczosOperator& op, int nev, double tol, int maxiter, int
   std::vector<double> Alpha, Beta, d, c;
   double beta = 0.0;
   bool justRestarted = false;
+  bool vInQ = false;  // v already stored in the basis column the next step starts from
   int sizeV = 1, kk = 0;
   std::vector<double> ev, Us;
   std::vector<int> ind;
@@ -546,7 +551,9 @@ int lanczos_run(const LanczosOperator& op, int nev, double tol, int maxiter, int
     for (int jj = sizeV; jj <= p; ++jj) {
       const int j = jj - 1;
       double2* qj = L.Q + (size_t)n * j;
-      FAME_CUDA_TRY(cudaMemcpyAsync(qj, L.v, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+      // Q(:,jj) = v, unless the previous step's normalisation already wrote it there
+      if (!vInQ) FAME_CUDA_TRY(cudaMemcpyAsync(qj, L.v, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+      vInQ = false;
       FAME_TRY(op.apply(op.self, qj, L.w));  // Aq = fncA(Q(:,jj))
       // alpha = Re(Aq' Q(:,jj)) from the first pass; passes: 2, or 3 after a restart
       FAME_TRY(L.cgs(jj, justRestarted ? 3 : 2));
@@ -563,7 +570,8 @@ int lanczos_run(const LanczosOperator& op, int nev, double tol, int maxiter, int
         break;
       }
       beta = std::sqrt(beta2);
-      k_scale_inv_sqrt<<<vec_blocks(n), 256, 0, s>>>(L.w, L.v, n, L.scal);
+      vInQ = jj < p;  // the next step of this cycle stores v in column jj
+      k_scale_inv_sqrt<<<vec_blocks(n), 256, 0, s>>>(L.w, L.v, n, L.scal, vInQ ? L.Q + (size_t)n * jj : nullptr);
       ::fame::count_launch();
       Alpha.push_back(alpha);
       Beta.push_back(beta);
