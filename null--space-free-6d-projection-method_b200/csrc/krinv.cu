@@ -147,9 +147,9 @@ int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
                                               " relres=" + std::to_string(relres) +
                                               " iter=" + std::to_string(h.iter));
   } else {
-    // FP64 iterative refinement: u (=B.x, zero) ; r64 (=B.r) = bhat.  The first round
-    // always runs, so ||bhat||^2 is read with the first refinement residual instead of
-    // here (a zero bhat gives a converged FP32 solve and a zero residual; NaN/Inf in
+    // FP64 iterative refinement: u (=B.x, zero) ; r64 (=B.r) = bhat.  The first two
+    // rounds always run, so ||bhat||^2 is read with the second round's residual instead
+    // of here (a zero bhat gives converged FP32 solves and a zero residual; NaN/Inf in
     // bhat reaches the FP32 solve's initial norm).
     double bn2 = 1.0, rn2 = 1.0;
     bool first = true;
