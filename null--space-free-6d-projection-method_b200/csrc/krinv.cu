@@ -178,17 +178,18 @@ int krinv_explicit_apply_one(fame_krinv* K, const double2* q, double2* y) {
       PcgState h32{};
       if (K->o.mhatPreconditioner) {
         FAME_TRY(pcg_iterate<float>(K, OpMhatPre<float>{coef_line_of<float>(bs), es_of<float>(K->m), K->m->EtInv32},
-                                    F, st32, hint, h32, false, nullptr));
+                                    F, st32, hint, h32, false, nullptr, true));
       } else {
         FAME_TRY(pcg_iterate<float>(K, OpMhat<float>{coef_line_of<float>(bs), es_of<float>(K->m)}, F, st32,
-                                    hint, h32, false, nullptr));
+                                    hint, h32, false, nullptr, true));
       }
       if (h32.flag == -1) return fail(FAME_ERR_NONFINITE, "Mhat right-hand side contains NaN/Inf");
       if (h32.flag == 4) return fail(FAME_ERR_NOT_CONVERGED, "FP32 correction solve broke down");
       K->stats.fp32Iterations += h32.iter;
       iters += h32.iter;
-      // u += dx ; r64 = bhat - Mhat u  (FP64 residual)
-      ProResidMhat<double, float, true> pro{c, B.x, F.x};
+      // u += dx ; r64 = bhat - Mhat u  (FP64 residual); the FP32 solve's last update of
+      // dx is still pending and is applied here (the FP32 residual is not needed again)
+      ProResidMhat<double, float, true> pro{c, B.x, F.x, F.p, st32};
       EpiResidMhat<double> epi{c, K->bhat, B.r, &st->rho, K->partials, K->counter};
       FAME_TRY((run_chain_lin<double, 3>(K->n, pro, epi, B.work, K->m->Et64, NF, s)));
       K->stats.massApplies += 3;

@@ -222,7 +222,7 @@ int queue_iterations(fame_krinv* K, const Op& op, PcgBuf<T>& B, PcgState* st, in
 // residual as MATLAB pcg does, continuing up to three times if it fails.
 template <typename T, class Op>
 int pcg_iterate(fame_krinv* K, const Op& op, PcgBuf<T>& B, PcgState* st, int& lastIt, PcgState& h,
-                bool verify, const C<T>* b) {
+                bool verify, const C<T>* b, bool keepPending = false) {
   cudaStream_t s = K->ctx->stream;
   const int every = std::max(1, K->o.checkEvery);
   int chunk = lastIt > 0 ? lastIt : every;  // iteration counts repeat from call to call
@@ -236,7 +236,9 @@ int pcg_iterate(fame_krinv* K, const Op& op, PcgBuf<T>& B, PcgState* st, int& la
       chunk = every;
       continue;
     }
-    if (Op::fused_update && h.pend) {  // apply the last iteration's x/r update
+    // apply the last iteration's x/r update (keepPending: the caller's next kernel applies
+    // it to x, and r is not needed)
+    if (Op::fused_update && h.pend && !keepPending) {
       const long long nlen = (long long)Op::nvec * K->NF;
       k_pcg_finish<T><<<vec_blocks(nlen), 256, 0, s>>>(B.x, B.r, B.p, B.Ap, nlen, st);
       ::fame::count_launch();

@@ -315,16 +315,24 @@ template <typename T> struct ProPcgDir {
 };
 
 // r = b - Mhat x with ||r||^2 into *out (true residual / refinement residual).
-// With ADDX, the prologue first forms x = x + dx (dx in lower precision).
+// With ADDX, the prologue first forms x = x + dx (dx in lower precision); with dst,
+// dx is the solution of a PCG whose last update is still pending (dst->pend), and
+// dx + alpha p is formed first, in dx's precision as k_pcg_finish would.
 template <typename T, typename TD, bool ADDX> struct ProResidMhat {
   using Ext = C<T>;
   static constexpr bool unit0 = true;
   MhatCoef<T> c;
   C<T>* x;
   const C<TD>* dx;
+  const C<TD>* dp = nullptr;
+  const PcgState* dst = nullptr;
   __device__ __forceinline__ C<T> load(long long i, long long, Ext& e) const {
     C<T> xi = x[i];
-    if (ADDX) xi = cadd<T>(xi, ccast<T, TD>(ldc<TD>(dx + i)));
+    if (ADDX) {
+      C<TD> d = ldc<TD>(dx + i);
+      if (dst && dst->pend) d = cadd<TD>(d, cmul<TD>(mk<TD>((TD)dst->alpha_re, (TD)dst->alpha_im), ldc<TD>(dp + i)));
+      xi = cadd<T>(xi, ccast<T, TD>(d));
+    }
     e = xi;
     return cscale<T>(xi, ldr<T>(c.invC + i));
   }
